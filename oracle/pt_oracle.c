@@ -1,0 +1,821 @@
+/*
+ * pt_oracle.c -- CPU oracle for ParaTreeT's Barnes-Hut gravity path.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for the CUDA path and the "port"
+ * CPU baseline.  The product never links, loads or calls this file.
+ *
+ * A plain-C, structure-of-arrays restatement of the reference path, FP64
+ * throughout, compiled with -ffp-contract=off so that every expression is
+ * evaluated exactly as the reference (built -DUSE_DOUBLE_FP) evaluates it.
+ * Arithmetic expressions that decide bit-exact parity keep the reference's
+ * association order; each block cites the reference lines it restates.
+ */
+#include "pt_oracle.h"
+#include "pt_sfc.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define PTO_MAX_DEPTH 21 /* 63 key bits / 3 */
+
+typedef struct {
+  double mass, cm[3], soft, radius;
+  double xx, xy, xz, yy, yz, zz;
+  double lo[3], hi[3];
+  int count;
+} pto_mom;
+
+struct pto_sim {
+  int n, bucket, threads;
+  double theta, dt_max, last_dt;
+  /* particles, current (key-sorted after a build) order */
+  double *x, *y, *z, *vx, *vy, *vz, *m, *soft;
+  double *ax, *ay, *az, *pot, *potf;
+  int* order;
+  uint64_t* key;
+  double ulo[3], uhi[3];
+  /* tree */
+  long nnodes, cap;
+  uint64_t* nkey;
+  int *ntype, *ndepth, *npstart, *nnp, *nparent, *nchild, *nwait;
+  pto_mom* mom;
+  int *leaves, *empties;
+  long nleaves, nempties, leafcap, emptycap;
+  /* interaction lists of the last evaluation */
+  long *list_off;
+  uint64_t* list_key;
+  int* list_kind;
+  long list_total, list_cap;
+  unsigned long long n_pp, n_pc, n_open;
+  double t_build, t_trav;
+};
+
+static double wall(void) {
+#ifdef _OPENMP
+  return omp_get_wtime();
+#else
+  return 0.0;
+#endif
+}
+
+/* ---------------------------------------------------------------- universe
+ * src/Driver.h:67-80 (remakeUniverse): cube centred on the bbox centre with
+ * half-side (1 + 1.91e-6) * 0.5 * longest side. */
+static void remake_universe(pto_sim* s, const double blo[3], const double bhi[3]) {
+  double sx = bhi[0] - blo[0], sy = bhi[1] - blo[1], sz = bhi[2] - blo[2];
+  double mx = (sx > sy) ? sx : sy;
+  mx = (mx > sz) ? mx : sz;
+  double c[3];
+  for (int d = 0; d < 3; d++) c[d] = (blo[d] + bhi[d]) / 2.0;
+  const double fEps = 1.0 + 1.91e-6;
+  double h = fEps * 0.5 * mx;
+  for (int d = 0; d < 3; d++) {
+    s->ulo[d] = c[d] - h;
+    s->uhi[d] = c[d] + h;
+  }
+}
+
+static void particle_bbox(const pto_sim* s, double lo[3], double hi[3]) {
+  lo[0] = lo[1] = lo[2] = 1.7976931348623157e308;
+  hi[0] = hi[1] = hi[2] = -1.7976931348623157e308;
+  for (int i = 0; i < s->n; i++) {
+    double p[3] = {s->x[i], s->y[i], s->z[i]};
+    for (int d = 0; d < 3; d++) {
+      if (p[d] < lo[d]) lo[d] = p[d];
+      if (p[d] > hi[d]) hi[d] = p[d];
+    }
+  }
+}
+
+/* src/Decomposition.C:58-64: key = SFC key | placeholder bit 63. */
+static void assign_keys(pto_sim* s) {
+  for (int i = 0; i < s->n; i++)
+    s->key[i] = pt_morton_key(s->x[i], s->y[i], s->z[i], s->ulo, s->uhi) | PT_KEY_PLACEHOLDER;
+}
+
+/* ---------------------------------------------------------------- sort
+ * src/Subtree.h:281 sorts the particles by key (Particle::operator<,
+ * src/Particle.C:61-79).  Stable LSD radix sort here: equal keys keep their
+ * current order. */
+static void permute_d(double* a, const int* perm, double* tmp, int n) {
+  for (int i = 0; i < n; i++) tmp[i] = a[perm[i]];
+  memcpy(a, tmp, sizeof(double) * (size_t)n);
+}
+
+static void sort_particles(pto_sim* s) {
+  int n = s->n;
+  int* idx = (int*)malloc(sizeof(int) * (size_t)n);
+  int* idx2 = (int*)malloc(sizeof(int) * (size_t)n);
+  uint64_t* k2 = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)n);
+  uint64_t* k1 = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)n);
+  for (int i = 0; i < n; i++) { idx[i] = i; k1[i] = s->key[i]; }
+  for (int pass = 0; pass < 8; pass++) {
+    int shift = pass * 8;
+    long cnt[257];
+    memset(cnt, 0, sizeof(cnt));
+    for (int i = 0; i < n; i++) cnt[((k1[i] >> shift) & 0xff) + 1]++;
+    for (int b = 0; b < 256; b++) cnt[b + 1] += cnt[b];
+    for (int i = 0; i < n; i++) {
+      long d = cnt[(k1[i] >> shift) & 0xff]++;
+      k2[d] = k1[i];
+      idx2[d] = idx[i];
+    }
+    uint64_t* tk = k1; k1 = k2; k2 = tk;
+    int* ti = idx; idx = idx2; idx2 = ti;
+  }
+  double* tmp = (double*)malloc(sizeof(double) * (size_t)n);
+  permute_d(s->x, idx, tmp, n);
+  permute_d(s->y, idx, tmp, n);
+  permute_d(s->z, idx, tmp, n);
+  permute_d(s->vx, idx, tmp, n);
+  permute_d(s->vy, idx, tmp, n);
+  permute_d(s->vz, idx, tmp, n);
+  permute_d(s->m, idx, tmp, n);
+  permute_d(s->soft, idx, tmp, n);
+  for (int i = 0; i < n; i++) idx2[i] = s->order[idx[i]];
+  memcpy(s->order, idx2, sizeof(int) * (size_t)n);
+  memcpy(s->key, k1, sizeof(uint64_t) * (size_t)n);
+  free(tmp); free(idx); free(idx2); free(k1); free(k2);
+}
+
+/* ---------------------------------------------------------------- moments
+ * Leaf data: CentroidData(particles, n, depth), examples/CentroidData.h:41-59,
+ * accumulating MultipoleMoments::operator+=(Particle) in particle order,
+ * examples/MultipoleMoments.h:274-353 (non-HEXADECAPOLE branch), then
+ * calculateRadiusBox (:473-482) or radius 1.0 for count <= 1. */
+static void mom_clear(pto_mom* q) {
+  memset(q, 0, sizeof(*q));
+  for (int d = 0; d < 3; d++) {
+    q->lo[d] = 1.7976931348623157e308;
+    q->hi[d] = -1.7976931348623157e308;
+  }
+}
+
+static void mom_add_particle(pto_mom* q, double px, double py, double pz, double pm, double ps) {
+  double m1 = q->mass;
+  q->mass += pm;
+  if (q->mass == 0.0) {
+    q->soft = 0.5 * (q->soft + ps);
+    q->cm[0] = 0.5 * (q->cm[0] + px);
+    q->cm[1] = 0.5 * (q->cm[1] + py);
+    q->cm[2] = 0.5 * (q->cm[2] + pz);
+    return;
+  }
+  q->soft = (m1 * q->soft + pm * ps) / q->mass;
+  double c1[3] = {q->cm[0], q->cm[1], q->cm[2]};
+  q->cm[0] = (m1 * q->cm[0] + pm * px) / q->mass;
+  q->cm[1] = (m1 * q->cm[1] + pm * py) / q->mass;
+  q->cm[2] = (m1 * q->cm[2] + pm * pz) / q->mass;
+  double d0 = c1[0] - q->cm[0], d1 = c1[1] - q->cm[1], d2 = c1[2] - q->cm[2];
+  q->xx += m1 * d0 * d0;
+  q->yy += m1 * d1 * d1;
+  q->zz += m1 * d2 * d2;
+  q->xy += m1 * d0 * d1;
+  q->xz += m1 * d0 * d2;
+  q->yz += m1 * d1 * d2;
+  d0 = px - q->cm[0];
+  d1 = py - q->cm[1];
+  d2 = pz - q->cm[2];
+  q->xx += pm * d0 * d0;
+  q->yy += pm * d1 * d1;
+  q->zz += pm * d2 * d2;
+  q->xy += pm * d0 * d1;
+  q->xz += pm * d0 * d2;
+  q->yz += pm * d1 * d2;
+}
+
+static void box_grow_pt(double lo[3], double hi[3], const double p[3]) {
+  for (int d = 0; d < 3; d++) {
+    if (p[d] < lo[d]) lo[d] = p[d];
+    if (p[d] > hi[d]) hi[d] = p[d];
+  }
+}
+
+static void leaf_moments(pto_sim* s, pto_mom* q, int start, int cnt) {
+  mom_clear(q);
+  for (int i = start; i < start + cnt; i++) {
+    mom_add_particle(q, s->x[i], s->y[i], s->z[i], s->m[i], s->soft[i]);
+    double p[3] = {s->x[i], s->y[i], s->z[i]};
+    box_grow_pt(q->lo, q->hi, p);
+  }
+  q->count = cnt;
+  if (q->count > 1) {
+    double dx = q->hi[0] - q->lo[0], dy = q->hi[1] - q->lo[1], dz = q->hi[2] - q->lo[2];
+    q->radius = 0.5 * sqrt(dx * dx + dy * dy + dz * dz);
+  } else {
+    q->radius = 1.0;
+  }
+}
+
+/* Upward combine: CentroidData::operator+=, examples/CentroidData.h:61-73,
+ * with MultipoleMoments::operator+=(MultipoleMoments) (parallel axis),
+ * examples/MultipoleMoments.h:204-221 and :253-271, and
+ * calculateRadiusFarthestCorner, :458-469. */
+static void mom_combine(pto_mom* q, const pto_mom* c) {
+  for (int d = 0; d < 3; d++) {
+    if (c->lo[d] < q->lo[d]) q->lo[d] = c->lo[d];
+    if (c->hi[d] > q->hi[d]) q->hi[d] = c->hi[d];
+  }
+  double m1 = q->mass;
+  q->mass += c->mass;
+  if (q->mass == 0.0) {
+    q->soft = 0.5 * (q->soft + c->soft);
+    for (int d = 0; d < 3; d++) q->cm[d] = 0.5 * (q->cm[d] + c->cm[d]);
+  } else if (m1 == 0.0) {
+    double lo[3], hi[3];
+    int cnt = q->count;
+    memcpy(lo, q->lo, sizeof(lo));
+    memcpy(hi, q->hi, sizeof(hi));
+    *q = *c;
+    q->count = cnt;
+    memcpy(q->lo, lo, sizeof(lo));
+    memcpy(q->hi, hi, sizeof(hi));
+  } else if (c->mass != 0.0) {
+    q->soft = (m1 * q->soft + c->mass * c->soft) / q->mass;
+    double c1[3] = {q->cm[0], q->cm[1], q->cm[2]};
+    for (int d = 0; d < 3; d++) q->cm[d] = (m1 * q->cm[d] + c->mass * c->cm[d]) / q->mass;
+    double d0 = c1[0] - q->cm[0], d1 = c1[1] - q->cm[1], d2 = c1[2] - q->cm[2];
+    q->xx += m1 * d0 * d0;
+    q->yy += m1 * d1 * d1;
+    q->zz += m1 * d2 * d2;
+    q->xy += m1 * d0 * d1;
+    q->xz += m1 * d0 * d2;
+    q->yz += m1 * d1 * d2;
+    d0 = c->cm[0] - q->cm[0];
+    d1 = c->cm[1] - q->cm[1];
+    d2 = c->cm[2] - q->cm[2];
+    q->xx += c->xx + c->mass * d0 * d0;
+    q->yy += c->yy + c->mass * d1 * d1;
+    q->zz += c->zz + c->mass * d2 * d2;
+    q->xy += c->xy + c->mass * d0 * d1;
+    q->xz += c->xz + c->mass * d0 * d2;
+    q->yz += c->yz + c->mass * d1 * d2;
+  }
+  q->count += c->count;
+  if (q->count > 1) {
+    double e[3];
+    for (int d = 0; d < 3; d++) {
+      double a = q->cm[d] - q->lo[d], b = q->hi[d] - q->cm[d];
+      e[d] = (a > b) ? a : b;
+    }
+    q->radius = sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+  } else {
+    q->radius = 1.0;
+  }
+}
+
+/* ---------------------------------------------------------------- build */
+static long new_node(pto_sim* s) {
+  if (s->nnodes == s->cap) {
+    long nc = s->cap ? 2 * s->cap : 1024;
+    s->nkey = (uint64_t*)realloc(s->nkey, sizeof(uint64_t) * nc);
+    s->ntype = (int*)realloc(s->ntype, sizeof(int) * nc);
+    s->ndepth = (int*)realloc(s->ndepth, sizeof(int) * nc);
+    s->npstart = (int*)realloc(s->npstart, sizeof(int) * nc);
+    s->nnp = (int*)realloc(s->nnp, sizeof(int) * nc);
+    s->nparent = (int*)realloc(s->nparent, sizeof(int) * nc);
+    s->nchild = (int*)realloc(s->nchild, sizeof(int) * nc);
+    s->nwait = (int*)realloc(s->nwait, sizeof(int) * nc);
+    s->mom = (pto_mom*)realloc(s->mom, sizeof(pto_mom) * nc);
+    s->cap = nc;
+  }
+  return s->nnodes++;
+}
+
+static void push_int(int** a, long* len, long* cap, int v) {
+  if (*len == *cap) {
+    *cap = *cap ? 2 * *cap : 1024;
+    *a = (int*)realloc(*a, sizeof(int) * (*cap));
+  }
+  (*a)[(*len)++] = v;
+}
+
+/* src/Subtree.h:263-267 (getType), with depth 21 forced to Leaf. */
+static int node_type(long n, int bucket, int depth) {
+  if (n == 0) return PTO_EMPTY;
+  if (n <= bucket || depth >= PTO_MAX_DEPTH) return PTO_LEAF;
+  return PTO_INTERNAL;
+}
+
+static int key_depth(uint64_t k) {
+  int pos = 63 - __builtin_clzll(k);
+  return pos / 3;
+}
+
+/* Utility::removeLeadingZeros, src/Utility.h:127-130 with :91-93. */
+static uint64_t left_align(uint64_t k) { return k << (63 - 3 * key_depth(k)); }
+
+/* first index in [lo, hi) whose key >= v (Utility::binarySearchComp,
+ * src/Utility.h:33-50 with OctTree::findChildsLastParticle,
+ * src/Modularization.C:60-65). */
+static int first_ge(const uint64_t* keys, int lo, int hi, uint64_t v) {
+  while (lo < hi) {
+    int mid = lo + ((hi - lo) >> 1);
+    if (keys[mid] >= v) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo;
+}
+
+static void make_node(pto_sim* s, long id, uint64_t key, int type, int depth, int pstart, int np, int parent) {
+  s->nkey[id] = key;
+  s->ntype[id] = type;
+  s->ndepth[id] = depth;
+  s->npstart[id] = pstart;
+  s->nnp[id] = np;
+  s->nparent[id] = parent;
+  s->nchild[id] = -1;
+  s->nwait[id] = (type == PTO_INTERNAL) ? 8 : 0;
+  if (type == PTO_LEAF) {
+    leaf_moments(s, &s->mom[id], pstart, np);
+    push_int(&s->leaves, &s->nleaves, &s->leafcap, (int)id);
+  } else {
+    mom_clear(&s->mom[id]);
+    s->mom[id].radius = 0.0;
+    if (type == PTO_EMPTY) push_int(&s->empties, &s->nempties, &s->emptycap, (int)id);
+  }
+}
+
+/* src/Subtree.h:314-349 (recursiveBuild); children of a node are allocated
+ * as one contiguous group of 8. */
+static void recursive_build(pto_sim* s, long node) {
+  uint64_t ck = s->nkey[node] << 3;
+  int start = s->npstart[node];
+  int finish = start + s->nnp[node];
+  long first = -1;
+  for (int i = 0; i < 8; i++) {
+    long c = new_node(s);
+    if (i == 0) first = c;
+  }
+  s->nchild[node] = (int)first;
+  int depth = s->ndepth[node] + 1;
+  for (int i = 0; i < 8; i++) {
+    int fge = finish;
+    if (i < 7) fge = first_ge(s->key, start, finish, left_align(ck + 1));
+    int cn = fge - start;
+    long c = first + i;
+    make_node(s, c, ck, node_type(cn, s->bucket, depth), depth, start, cn, (int)node);
+    if (s->ntype[c] == PTO_INTERNAL) recursive_build(s, c);
+    start = fge;
+    ck++;
+  }
+}
+
+/* src/Subtree.h:352-384 (populateTree): leaves (DFS order), then empty
+ * leaves, through a FIFO; a parent joins the queue when its last child is
+ * popped, and combines its children in pop order. */
+static void populate(pto_sim* s) {
+  long total = s->nleaves + s->nempties;
+  long qcap = s->nnodes + 1, head = 0, tail = 0;
+  int* q = (int*)malloc(sizeof(int) * qcap);
+  for (long i = 0; i < s->nleaves; i++) q[tail++] = s->leaves[i];
+  for (long i = 0; i < s->nempties; i++) q[tail++] = s->empties[i];
+  (void)total;
+  while (head < tail) {
+    int nd = q[head++];
+    if (nd == 0) continue; /* the root */
+    int p = s->nparent[nd];
+    mom_combine(&s->mom[p], &s->mom[nd]);
+    if (--s->nwait[p] == 0) q[tail++] = p;
+  }
+  free(q);
+}
+
+static void build_tree(pto_sim* s) {
+  sort_particles(s);
+  s->nnodes = 0;
+  s->nleaves = s->nempties = 0;
+  long root = new_node(s);
+  make_node(s, root, 1, node_type(s->n, s->bucket, 0), 0, 0, s->n, -1);
+  if (s->ntype[root] == PTO_INTERNAL) recursive_build(s, root);
+  populate(s);
+}
+
+/* ---------------------------------------------------------------- visitor
+ * examples/GravityVisitor.h.  Offsets are zero (no periodic replicas). */
+static const double kOpenGeom = 4.0 / 3.0; /* :14 */
+
+/* SPLINE, GravityVisitor.h:87-120 (a: potential term, b: force term) */
+static void spline(double r2, double twoh, double* a, double* b) {
+  double r = sqrt(r2);
+  if (r < twoh) {
+    double dih = 2.0 / twoh;
+    double u = r * dih;
+    if (u < 1.0) {
+      *a = dih * (7.0 / 5.0 - 2.0 / 3.0 * u * u + 3.0 / 10.0 * u * u * u * u - 1.0 / 10.0 * u * u * u * u * u);
+      *b = dih * dih * dih * (4.0 / 3.0 - 6.0 / 5.0 * u * u + 1.0 / 2.0 * u * u * u);
+    } else {
+      double dir = 1.0 / r;
+      *a = -1.0 / 15.0 * dir +
+           dih * (8.0 / 5.0 - 4.0 / 3.0 * u * u + u * u * u - 3.0 / 10.0 * u * u * u * u + 1.0 / 30.0 * u * u * u * u * u);
+      *b = -1.0 / 15.0 * dir * dir * dir + dih * dih * dih * (8.0 / 3.0 - 3.0 * u + 6.0 / 5.0 * u * u - 1.0 / 6.0 * u * u * u);
+    }
+  } else {
+    *a = 1.0 / r;
+    *b = *a * *a * *a;
+  }
+}
+
+/* SPLINEQ, GravityVisitor.h:37-80, kept exactly as the reference evaluates
+ * it (including its softened-branch grouping). */
+static void splineq(double invr, double r2, double twoh, double* a, double* b, double* c, double* d) {
+  double dir = invr;
+  if (r2 < twoh * twoh) {
+    double dih = 2.0 / twoh;
+    double u = dih / dir;
+    if (u < 1.0) {
+      *a = dih * (7.0) / 5.0 - 2.0 / 3.0 * u * u + 3.0 / 10.0 * u * u * u * u - 1.0 / 10.0 * u * u * u * u * u;
+      *b = dih * dih * dih * (4.0) / 3.0 - 6.0 / 5.0 * u * u + 1.0 / 2.0 * u * u * u;
+      *c = dih * dih * dih * dih * dih * (12.0) / 5.0 - 3.0 / 2.0 * u;
+      *d = 3.0 / 2.0 * dih * dih * dih * dih * dih * dih * dir;
+    } else {
+      *a = -1.0 / 15.0 * dir + dih * (8.0 / 5.0) - 4.0 / 3.0 * u * u + u * u * u - 3.0 / 10.0 * u * u * u * u +
+           1.0 / 30.0 * u * u * u * u * u;
+      *b = -1.0 / 15.0 * dir * dir * dir + dih * dih * dih * (8.0) / 3.0 - 3.0 * u + 6.0 / 5.0 * u * u -
+           1.0 / 6.0 * u * u * u;
+      *c = -1.0 / 5.0 * dir * dir * dir * dir * dir + 3.0 * dih * dih * dih * dih * dir +
+           dih * dih * dih * dih * dih * (-12.0) / 5.0 + 1.0 / 2.0 * u;
+      *d = -dir * dir * dir * dir * dir * dir * dir + 3.0 * dih * dih * dih * dih * dir * dir * dir -
+           1.0 / 2.0 * dih * dih * dih * dih * dih * dih * dir;
+    }
+  } else {
+    *a = dir;
+    *b = *a * *a * *a;
+    *c = 3.0 * *b * *a * *a;
+    *d = 5.0 * *c * *a * *a;
+  }
+}
+
+/* box/sphere test of the stand-in Space::intersect (x, y, z order; <=). */
+static int box_sphere(const double lo[3], const double hi[3], const double c[3], double rsq) {
+  double dsq = 0.0, d;
+  for (int k = 0; k < 3; k++) {
+    if ((d = lo[k] - c[k]) > 0) dsq += d * d;
+    else if ((d = c[k] - hi[k]) > 0) dsq += d * d;
+  }
+  return dsq <= rsq;
+}
+
+/* GravityVisitor::open, :162-182 (non-HEXADECAPOLE :180). */
+static int visit_open(const pto_sim* s, const pto_mom* src, const pto_mom* tgt, double gfac) {
+  if (src->count <= 6) return 1;
+  double rsq = src->radius * src->radius * gfac;
+  return box_sphere(tgt->lo, tgt->hi, src->cm, rsq);
+  (void)s;
+}
+
+/* GravityVisitor::openSoftening, :122-128. */
+static int open_softening(const pto_mom* src, const pto_mom* tgt) {
+  double r1 = 2.0 * src->soft, r2 = 2.0 * tgt->soft;
+  double dx = src->cm[0] - tgt->cm[0], dy = src->cm[1] - tgt->cm[1], dz = src->cm[2] - tgt->cm[2];
+  double rs = r1 + r2;
+  if (dx * dx + dy * dy + dz * dz <= rs * rs) return 1;
+  return box_sphere(tgt->lo, tgt->hi, src->cm, r1 * r1);
+}
+
+/* GravityVisitor::leaf, :144-160 -- P2P; the per-source-leaf sum is formed
+ * first and then added (applyAcceleration).  pot_full additionally sums
+ * -m_j * a (the reference's leaf() does not touch the potential). */
+static void visit_leaf(pto_sim* s, int src, int tgt) {
+  int s0 = s->npstart[src], sn = s->nnp[src];
+  int t0 = s->npstart[tgt], tn = s->nnp[tgt];
+  for (int i = t0; i < t0 + tn; i++) {
+    double ax = 0.0, ay = 0.0, az = 0.0, pf = 0.0;
+    for (int j = s0; j < s0 + sn; j++) {
+      double dx = (s->x[j] + 0.0) - s->x[i];
+      double dy = (s->y[j] + 0.0) - s->y[i];
+      double dz = (s->z[j] + 0.0) - s->z[i];
+      double rsq = dx * dx + dy * dy + dz * dz;
+      double twoh = s->soft[j] + s->soft[i];
+      if (rsq != 0) {
+        double a, b;
+        spline(rsq, twoh, &a, &b);
+        double bm = b * s->m[j];
+        ax += dx * bm;
+        ay += dy * bm;
+        az += dz * bm;
+        pf += -s->m[j] * a;
+      }
+    }
+    s->ax[i] += ax;
+    s->ay[i] += ay;
+    s->az[i] += az;
+    s->potf[i] += pf;
+  }
+}
+
+/* GravityVisitor::node, :184-224 (non-HEXADECAPOLE :207-221), with the
+ * unsoftened monopole fallback addGravity, :130-139. */
+static void visit_node(pto_sim* s, int src, int tgt) {
+  const pto_mom* q = &s->mom[src];
+  const pto_mom* t = &s->mom[tgt];
+  if (q->count == 0) return;
+  int t0 = s->npstart[tgt], tn = s->nnp[tgt];
+  if (open_softening(q, t)) {
+    for (int i = t0; i < t0 + tn; i++) {
+      double dx = (q->cm[0] + 0.0) - s->x[i];
+      double dy = (q->cm[1] + 0.0) - s->y[i];
+      double dz = (q->cm[2] + 0.0) - s->z[i];
+      double rsq = dx * dx + dy * dy + dz * dz;
+      if (rsq != 0) {
+        double f = q->mass / (rsq * sqrt(rsq));
+        s->ax[i] += dx * f;
+        s->ay[i] += dy * f;
+        s->az[i] += dz * f;
+        s->potf[i] += -q->mass / sqrt(rsq);
+      }
+    }
+    return;
+  }
+  for (int i = t0; i < t0 + tn; i++) {
+    double rx = (s->x[i] - q->cm[0]) - 0.0;
+    double ry = (s->y[i] - q->cm[1]) - 0.0;
+    double rz = (s->z[i] - q->cm[2]) - 0.0;
+    double rsq = rx * rx + ry * ry + rz * rz;
+    double dir = 1.0 / sqrt(rsq);
+    double twoh = q->soft + s->soft[i];
+    double a, b, c, d;
+    splineq(dir, rsq, twoh, &a, &b, &c, &d);
+    double qx = q->xx * rx + q->xy * ry + q->xz * rz;
+    double qy = q->xy * rx + q->yy * ry + q->yz * rz;
+    double qz = q->xz * rx + q->yz * ry + q->zz * rz;
+    double qir = 0.5 * (qx * rx + qy * ry + qz * rz);
+    double tr = 0.5 * (q->xx + q->yy + q->zz);
+    double qir3 = b * q->mass + d * qir - c * tr;
+    double p = -q->mass * a - c * qir + b * tr;
+    s->pot[i] += p;
+    s->potf[i] += p;
+    s->ax[i] += -qir3 * rx + c * qx;
+    s->ay[i] += -qir3 * ry + c * qy;
+    s->az[i] += -qir3 * rz + c * qz;
+  }
+}
+
+static void list_push(pto_sim* s, uint64_t key, int kind) {
+  if (s->list_total == s->list_cap) {
+    s->list_cap = s->list_cap ? 2 * s->list_cap : 4096;
+    s->list_key = (uint64_t*)realloc(s->list_key, sizeof(uint64_t) * s->list_cap);
+    s->list_kind = (int*)realloc(s->list_kind, sizeof(int) * s->list_cap);
+  }
+  s->list_key[s->list_total] = key;
+  s->list_kind[s->list_total] = kind;
+  s->list_total++;
+}
+
+/* src/Traverser.h:154-217 for one bucket: pre-order DFS; Leaf -> leaf()
+ * (self included, CallSelfLeaf), Internal -> open() ? children : node(),
+ * EmptyLeaf -> nothing. */
+static void walk(pto_sim* s, int tgt, double gfac, int record, unsigned long long* cnt) {
+  int stack[8 * (PTO_MAX_DEPTH + 2)];
+  int sp = 0;
+  stack[sp++] = 0;
+  while (sp) {
+    int nd = stack[--sp];
+    int ty = s->ntype[nd];
+    if (ty == PTO_LEAF) {
+      visit_leaf(s, nd, tgt);
+      cnt[0] += (unsigned long long)s->nnp[nd] * (unsigned long long)s->nnp[tgt];
+      if (record) list_push(s, s->nkey[nd], 0);
+    } else if (ty == PTO_INTERNAL) {
+      cnt[2]++;
+      if (visit_open(s, &s->mom[nd], &s->mom[tgt], gfac)) {
+        int c0 = s->nchild[nd];
+        for (int c = 7; c >= 0; c--) stack[sp++] = c0 + c;
+      } else {
+        visit_node(s, nd, tgt);
+        cnt[1] += (unsigned long long)s->nnp[tgt];
+        if (record) list_push(s, s->nkey[nd], 1);
+      }
+    }
+  }
+}
+
+static void traverse(pto_sim* s, int record) {
+  double gfac = kOpenGeom / (s->theta * s->theta);
+  memset(s->ax, 0, sizeof(double) * s->n);
+  memset(s->ay, 0, sizeof(double) * s->n);
+  memset(s->az, 0, sizeof(double) * s->n);
+  memset(s->pot, 0, sizeof(double) * s->n);
+  memset(s->potf, 0, sizeof(double) * s->n);
+  unsigned long long pp = 0, pc = 0, op = 0;
+  if (record) {
+    free(s->list_off);
+    s->list_off = (long*)malloc(sizeof(long) * (s->nleaves + 1));
+    s->list_total = 0;
+    for (long b = 0; b < s->nleaves; b++) {
+      unsigned long long c[3] = {0, 0, 0};
+      s->list_off[b] = s->list_total;
+      walk(s, s->leaves[b], gfac, 1, c);
+      pp += c[0]; pc += c[1]; op += c[2];
+    }
+    s->list_off[s->nleaves] = s->list_total;
+  } else {
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : pp, pc, op) num_threads(s->threads)
+#endif
+    for (long b = 0; b < s->nleaves; b++) {
+      unsigned long long c[3] = {0, 0, 0};
+      walk(s, s->leaves[b], gfac, 0, c);
+      pp += c[0]; pc += c[1]; op += c[2];
+    }
+  }
+  s->n_pp = pp;
+  s->n_pc = pc;
+  s->n_open = op;
+}
+
+/* ---------------------------------------------------------------- API */
+static double* dup_d(const double* a, int n) {
+  double* p = (double*)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+  if (n > 0) memcpy(p, a, sizeof(double) * (size_t)n);
+  return p;
+}
+
+pto_sim* pto_create(int n, const double* x, const double* y, const double* z, const double* vx,
+                    const double* vy, const double* vz, const double* m, const double* soft, int bucket,
+                    double theta, double dt_max, int threads) {
+  pto_sim* s = (pto_sim*)calloc(1, sizeof(pto_sim));
+  s->n = n;
+  s->bucket = bucket;
+  s->theta = theta;
+  s->dt_max = dt_max;
+  s->threads = threads > 0 ? threads : 1;
+  s->x = dup_d(x, n); s->y = dup_d(y, n); s->z = dup_d(z, n);
+  s->vx = dup_d(vx, n); s->vy = dup_d(vy, n); s->vz = dup_d(vz, n);
+  s->m = dup_d(m, n); s->soft = dup_d(soft, n);
+  s->ax = (double*)calloc((size_t)n + 1, sizeof(double));
+  s->ay = (double*)calloc((size_t)n + 1, sizeof(double));
+  s->az = (double*)calloc((size_t)n + 1, sizeof(double));
+  s->pot = (double*)calloc((size_t)n + 1, sizeof(double));
+  s->potf = (double*)calloc((size_t)n + 1, sizeof(double));
+  s->order = (int*)malloc(sizeof(int) * ((size_t)n + 1));
+  s->key = (uint64_t*)malloc(sizeof(uint64_t) * ((size_t)n + 1));
+  for (int i = 0; i < n; i++) s->order[i] = i;
+  double lo[3], hi[3];
+  particle_bbox(s, lo, hi);
+  remake_universe(s, lo, hi);
+  assign_keys(s);
+  return s;
+}
+
+void pto_destroy(pto_sim* s) {
+  if (!s) return;
+  free(s->x); free(s->y); free(s->z); free(s->vx); free(s->vy); free(s->vz); free(s->m); free(s->soft);
+  free(s->ax); free(s->ay); free(s->az); free(s->pot); free(s->potf); free(s->order); free(s->key);
+  free(s->nkey); free(s->ntype); free(s->ndepth); free(s->npstart); free(s->nnp); free(s->nparent);
+  free(s->nchild); free(s->nwait); free(s->mom); free(s->leaves); free(s->empties);
+  free(s->list_off); free(s->list_key); free(s->list_kind);
+  free(s);
+}
+
+int pto_forces(pto_sim* s, int record_lists) {
+  double t0 = wall();
+  build_tree(s);
+  double t1 = wall();
+  traverse(s, record_lists);
+  double t2 = wall();
+  s->t_build = t1 - t0;
+  s->t_trav = t2 - t1;
+  return 0;
+}
+
+/* examples/Gravity.C:63-67 with v_max from src/Subtree.h:164-170. */
+static double timestep(const pto_sim* s) {
+  double v2 = 0.0;
+  for (int i = 0; i < s->n; i++) {
+    double w = s->vx[i] * s->vx[i] + s->vy[i] * s->vy[i] + s->vz[i] * s->vz[i];
+    if (w > v2) v2 = w;
+  }
+  double vmax = sqrt(v2);
+  double len = s->uhi[0] - s->ulo[0];
+  double t = len / vmax / cbrt((double)s->n);
+  return t < s->dt_max ? t : s->dt_max;
+}
+
+/* src/Driver.h:183-251 iteration: forces, Particle::kick (src/Particle.C:7-9)
+ * for all particles, then Particle::perturb (:11-21) with the new bbox,
+ * remakeUniverse and rekey (src/Partition.h:382-387). */
+int pto_run(pto_sim* s, int nsteps) {
+  if (nsteps <= 0) return pto_forces(s, 0);
+  for (int it = 0; it < nsteps; it++) {
+    pto_forces(s, 0);
+    double dt = timestep(s);
+    s->last_dt = dt;
+    for (int i = 0; i < s->n; i++) {
+      s->vx[i] += s->ax[i] * dt / 2;
+      s->vy[i] += s->ay[i] * dt / 2;
+      s->vz[i] += s->az[i] * dt / 2;
+    }
+    for (int i = 0; i < s->n; i++) {
+      s->vx[i] += (s->ax[i] * dt / 2);
+      s->vy[i] += (s->ay[i] * dt / 2);
+      s->vz[i] += (s->az[i] * dt / 2);
+      s->x[i] += (s->vx[i] * dt);
+      s->y[i] += (s->vy[i] * dt);
+      s->z[i] += (s->vz[i] * dt);
+    }
+    double lo[3], hi[3];
+    particle_bbox(s, lo, hi);
+    remake_universe(s, lo, hi);
+    assign_keys(s);
+  }
+  return 0;
+}
+
+void pto_get_acc(const pto_sim* s, double* ax, double* ay, double* az, double* pot, double* pot_full) {
+  for (int i = 0; i < s->n; i++) {
+    int o = s->order[i];
+    if (ax) ax[o] = s->ax[i];
+    if (ay) ay[o] = s->ay[i];
+    if (az) az[o] = s->az[i];
+    if (pot) pot[o] = s->pot[i];
+    if (pot_full) pot_full[o] = s->potf[i];
+  }
+}
+
+void pto_get_keys(const pto_sim* s, uint64_t* keys) {
+  for (int i = 0; i < s->n; i++) keys[s->order[i]] = s->key[i];
+}
+
+void pto_get_state(const pto_sim* s, double* x, double* y, double* z, double* vx, double* vy, double* vz) {
+  for (int i = 0; i < s->n; i++) {
+    int o = s->order[i];
+    x[o] = s->x[i]; y[o] = s->y[i]; z[o] = s->z[i];
+    vx[o] = s->vx[i]; vy[o] = s->vy[i]; vz[o] = s->vz[i];
+  }
+}
+
+void pto_get_universe(const pto_sim* s, double* lo3, double* hi3) {
+  for (int d = 0; d < 3; d++) { lo3[d] = s->ulo[d]; hi3[d] = s->uhi[d]; }
+}
+
+void pto_get_counters(const pto_sim* s, unsigned long long* out4, double* times2, double* last_dt) {
+  out4[0] = s->n_pp; out4[1] = s->n_pc; out4[2] = s->n_open; out4[3] = (unsigned long long)s->nleaves;
+  times2[0] = s->t_build; times2[1] = s->t_trav;
+  *last_dt = s->last_dt;
+}
+
+long pto_num_nodes(const pto_sim* s) { return s->nnodes; }
+
+void pto_get_nodes(const pto_sim* s, uint64_t* keys, int* ints4, double* d18) {
+  for (long i = 0; i < s->nnodes; i++) {
+    const pto_mom* q = &s->mom[i];
+    keys[i] = s->nkey[i];
+    ints4[4 * i + 0] = s->ntype[i];
+    ints4[4 * i + 1] = s->ndepth[i];
+    ints4[4 * i + 2] = q->count;
+    ints4[4 * i + 3] = s->ntype[i] == PTO_INTERNAL ? 8 : 0;
+    double* d = d18 + 18 * i;
+    d[0] = q->mass; d[1] = q->cm[0]; d[2] = q->cm[1]; d[3] = q->cm[2]; d[4] = q->soft; d[5] = q->radius;
+    d[6] = q->xx; d[7] = q->xy; d[8] = q->xz; d[9] = q->yy; d[10] = q->yz; d[11] = q->zz;
+    d[12] = q->lo[0]; d[13] = q->lo[1]; d[14] = q->lo[2];
+    d[15] = q->hi[0]; d[16] = q->hi[1]; d[17] = q->hi[2];
+  }
+}
+
+long pto_num_buckets(const pto_sim* s) { return s->nleaves; }
+
+void pto_get_bucket_keys(const pto_sim* s, uint64_t* keys) {
+  for (long b = 0; b < s->nleaves; b++) keys[b] = s->nkey[s->leaves[b]];
+}
+
+long pto_list_total(const pto_sim* s) { return s->list_off ? s->list_total : 0; }
+
+void pto_get_lists(const pto_sim* s, long* offsets, uint64_t* keys, int* kinds) {
+  if (!s->list_off) return;
+  for (long b = 0; b <= s->nleaves; b++) offsets[b] = s->list_off[b];
+  memcpy(keys, s->list_key, sizeof(uint64_t) * s->list_total);
+  memcpy(kinds, s->list_kind, sizeof(int) * s->list_total);
+}
+
+/* FP64 isolated direct sum with the reference's spline kernel. */
+void pto_direct(int n, const double* x, const double* y, const double* z, const double* m,
+                const double* soft, int nt, const int* targets, double* ax, double* ay, double* az,
+                double* pot, int threads) {
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 4) num_threads(threads > 0 ? threads : 1)
+#endif
+  for (int t = 0; t < nt; t++) {
+    int i = targets[t];
+    double sx = 0.0, sy = 0.0, sz = 0.0, sp = 0.0;
+    for (int j = 0; j < n; j++) {
+      double dx = x[j] - x[i], dy = y[j] - y[i], dz = z[j] - z[i];
+      double rsq = dx * dx + dy * dy + dz * dz;
+      if (rsq != 0) {
+        double a, b;
+        spline(rsq, soft[j] + soft[i], &a, &b);
+        double bm = b * m[j];
+        sx += dx * bm;
+        sy += dy * bm;
+        sz += dz * bm;
+        sp += -m[j] * a;
+      }
+    }
+    ax[t] = sx; ay[t] = sy; az[t] = sz; pot[t] = sp;
+  }
+  (void)threads;
+}

@@ -1,0 +1,59 @@
+/*
+ * pt_oracle.h -- CPU oracle for the Barnes-Hut gravity path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is a plain-C restatement of ParaTreeT's
+ * gravity path (keys, sort, octree build, FIFO upward pass, transposed
+ * traversal with GravityVisitor, kick/perturb) used as the checker for the
+ * CUDA path and as the timed CPU baseline.  Nothing in the product links or
+ * calls it.  Each function in pt_oracle.c cites the reference lines it follows.
+ */
+#ifndef PT_ORACLE_H_
+#define PT_ORACLE_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pto_sim pto_sim;
+
+/* Node types, numbered as Node<Data>::Type in src/Node.h:82-95. */
+enum { PTO_LEAF = 1, PTO_EMPTY = 2, PTO_INTERNAL = 6 };
+
+pto_sim* pto_create(int n, const double* x, const double* y, const double* z, const double* vx,
+                    const double* vy, const double* vz, const double* m, const double* soft, int bucket,
+                    double theta, double dt_max, int threads);
+void pto_destroy(pto_sim* s);
+/* One force evaluation (keys -> traversal); record_lists keeps the per-bucket
+ * interaction lists of this evaluation. */
+int pto_forces(pto_sim* s, int record_lists);
+/* nsteps iterations of forces -> kick -> perturb -> new universe -> rekey. */
+int pto_run(pto_sim* s, int nsteps);
+
+void pto_get_acc(const pto_sim* s, double* ax, double* ay, double* az, double* pot, double* pot_full);
+void pto_get_keys(const pto_sim* s, uint64_t* keys);
+void pto_get_state(const pto_sim* s, double* x, double* y, double* z, double* vx, double* vy, double* vz);
+void pto_get_universe(const pto_sim* s, double* lo3, double* hi3);
+/* counters: n_pp, n_pc, n_open, n_buckets; times: build, traverse seconds */
+void pto_get_counters(const pto_sim* s, unsigned long long* out4, double* times2, double* last_dt);
+long pto_num_nodes(const pto_sim* s);
+/* Same layout as the reference-side dump: ints [type, depth, count, n_children],
+ * 18 doubles [mass, cm3, soft, radius, xx, xy, xz, yy, yz, zz, lo3, hi3]. */
+void pto_get_nodes(const pto_sim* s, uint64_t* keys, int* ints4, double* dbls18);
+long pto_num_buckets(const pto_sim* s);
+void pto_get_bucket_keys(const pto_sim* s, uint64_t* keys);
+long pto_list_total(const pto_sim* s);
+void pto_get_lists(const pto_sim* s, long* offsets, uint64_t* keys, int* kinds);
+
+/* FP64 direct sum (spline softening, twoh = soft_i + soft_j, G = 1) over
+ * all n sources for nt target indices; isolated (no periodic images). */
+void pto_direct(int n, const double* x, const double* y, const double* z, const double* m,
+                const double* soft, int nt, const int* targets, double* ax, double* ay, double* az,
+                double* pot, int threads);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,475 @@
+/*
+ * ref_driver.cpp -- TEST INFRASTRUCTURE (oracle).  Never linked into the
+ * product.
+ *
+ * Compiles the reference's OWN gravity sources from where they lie (see
+ * oracle/Makefile): examples/GravityVisitor.h, examples/CentroidData.h,
+ * examples/MultipoleMoments.h, src/Node.h, src/Particle.{h,C}, src/Utility.h,
+ * src/common.h -- built with -DUSE_DOUBLE_FP and without -DHEXADECAPOLE
+ * (the monopole+quadrupole branch) and with -ffp-contract=off.  Around them
+ * this file restates the Charm++-bound driver pieces, each following the
+ * cited reference lines:
+ *
+ *   universe          src/Driver.h:67-80 (remakeUniverse), bbox from
+ *                     src/Reader.C:92 / src/Partition.h:368-378
+ *   keys              src/Decomposition.C:58-64
+ *   sort              src/Subtree.h:281 (std::sort; stable here, so that
+ *                     equal keys keep input order -- the reference's tie
+ *                     order is unspecified)
+ *   node allocation   src/CacheManager.h:38-43 (FullNodePool::alloc)
+ *   tree build        src/Subtree.h:263-267, :293-298, :314-349,
+ *                     src/Modularization.C:60-65
+ *   upward pass       src/Subtree.h:352-384 (FIFO order)
+ *   traversal         src/Traverser.h:154-217 (TransposedDownTraverser::
+ *                     recurse) over contiguous groups of buckets, one group
+ *                     per Partition (src/Partition.h:129-134)
+ *   step              src/Driver.h:183-251: forces -> kick -> perturb ->
+ *                     new universe -> rekey; dt from examples/Gravity.C:63-67
+ *
+ * Deviation for degenerate input only: a node at depth 21 (all 63 key bits
+ * used) is made a Leaf even when it holds more than `bucket` particles (the
+ * reference would shift its key out of range).
+ */
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <deque>
+#include <functional>
+#include <queue>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "common.h"
+#include "Particle.h"
+#include "Utility.h"
+#include "CentroidData.h"
+#include "Node.h"
+#include "GravityVisitor.h"
+
+namespace {
+
+using RNode = Node<CentroidData>;
+using RFull = FullNode<CentroidData, 8>;
+
+constexpr int kLogBranch = 3;
+constexpr int kMaxDepth = 21;
+
+struct ListEntry {
+  uint64_t key;
+  int kind;  // 0 = leaf (P2P), 1 = node (P2C)
+};
+
+struct RefSim {
+  // configuration
+  int bucket = 16;
+  double theta = 0.7;
+  double dt_max = 0.01;
+  int group = 64;
+  int record_lists = 0;
+  int threads = 1;
+  // state
+  std::vector<Particle> particles;  // sorted by key after each build
+  OrientedBox<Real> universe;
+  std::deque<RFull> pool;
+  std::vector<RNode*> leaves, empty_leaves;
+  RNode* root = nullptr;
+  // outputs of the last force evaluation
+  std::vector<double> acc, pot;  // original order, 3N and N
+  std::vector<uint64_t> keys;    // original order
+  std::vector<std::vector<ListEntry>> lists;  // per bucket (DFS leaf order)
+  unsigned long long n_pp = 0, n_pc = 0, n_open = 0;
+  double last_dt = 0.0;
+  double t_build = 0.0, t_traverse = 0.0;
+};
+
+Node<CentroidData>::Type getType(size_t n, size_t B, int depth) {
+  if (n == 0) return RNode::Type::EmptyLeaf;
+  if (n <= B || depth >= kMaxDepth) return RNode::Type::Leaf;
+  return RNode::Type::Internal;
+}
+
+RNode* makeNode(RefSim& s, Key key, RNode::Type type, int depth, int n, Particle* p, RNode* parent) {
+  if (type == RNode::Type::Leaf) {
+    s.pool.emplace_back(key, type, depth, n, p, parent, 0, 0);
+  } else {
+    s.pool.emplace_back(key, type, depth, parent, 0, 0);
+  }
+  return &s.pool.back();
+}
+
+void handlePossibleLeaf(RefSim& s, RNode* node) {
+  if (node->type == RNode::Type::EmptyLeaf) s.empty_leaves.push_back(node);
+  else if (node->type == RNode::Type::Leaf) s.leaves.push_back(node);
+}
+
+void recursiveBuild(RefSim& s, RNode* node, Particle* np, size_t n) {
+  Key child_key = node->key << kLogBranch;
+  int start = 0;
+  int finish = (int)n;
+  std::function<bool(const Particle&, Key)> compGE = [](const Particle& a, Key b) { return a.key >= b; };
+  for (int i = 0; i < node->n_children; i++) {
+    int first_ge = finish;
+    if (i < node->n_children - 1) {
+      Key sib = Utility::removeLeadingZeros(child_key + 1, kLogBranch);
+      first_ge = Utility::binarySearchComp(sib, np, start, finish, compGE);
+    }
+    int cn = first_ge - start;
+    RNode* child = makeNode(s, child_key, getType(cn, s.bucket, node->depth + 1), node->depth + 1, cn,
+                            np + start, node);
+    node->exchangeChild(i, child);
+    if (child->isLeaf()) handlePossibleLeaf(s, child);
+    else recursiveBuild(s, child, np + start, cn);
+    start = first_ge;
+    child_key++;
+  }
+}
+
+void populateTree(RefSim& s) {
+  std::queue<RNode*> going_up;
+  for (auto* l : s.leaves) going_up.push(l);
+  for (auto* e : s.empty_leaves) going_up.push(e);
+  while (!going_up.empty()) {
+    RNode* node = going_up.front();
+    going_up.pop();
+    if (node == s.root) continue;  // tp_key == root key; no canopy above it
+    RNode* parent = node->parent;
+    parent->data += node->data;
+    parent->wait_count--;
+    if (parent->wait_count == 0) going_up.push(parent);
+  }
+}
+
+void remakeUniverse(RefSim& s, const OrientedBox<Real>& box) {
+  Vector3D<Real> bsize = box.size();
+  Real mx = (bsize.x > bsize.y) ? bsize.x : bsize.y;
+  mx = (mx > bsize.z) ? mx : bsize.z;
+  Vector3D<Real> bcenter = box.center();
+  const Real fEps = 1.0 + 1.91e-6;
+  bsize = Vector3D<Real>(fEps * 0.5 * mx);
+  s.universe = OrientedBox<Real>(bcenter - bsize, bcenter + bsize);
+}
+
+void assignKeys(RefSim& s) {
+  for (auto& p : s.particles) {
+    p.key = SFC::generateKey(p.position, s.universe);
+    p.key |= (Key)1 << (KEY_BITS - 1);
+  }
+}
+
+void buildTree(RefSim& s) {
+  std::stable_sort(s.particles.begin(), s.particles.end());
+  s.pool.clear();
+  s.leaves.clear();
+  s.empty_leaves.clear();
+  size_t n = s.particles.size();
+  Key root_key = 1;
+  s.root = makeNode(s, root_key, getType(n, s.bucket, 0), Utility::getDepthFromKey(root_key, kLogBranch),
+                    (int)n, s.particles.data(), nullptr);
+  if (s.root->isLeaf()) handlePossibleLeaf(s, s.root);
+  else recursiveBuild(s, s.root, s.particles.data(), n);
+  populateTree(s);
+}
+
+// One Partition's worth of TransposedDownTraverser::recurse.
+struct GroupTrav {
+  RefSim& s;
+  GravityVisitor v;
+  size_t b0, nb;
+  unsigned long long pp = 0, pc = 0, op = 0;
+  GroupTrav(RefSim& sim, size_t b0_, size_t nb_)
+      : s(sim), v(Vector3D<Real>(0, 0, 0), sim.theta), b0(b0_), nb(nb_) {}
+
+  void recurse(RNode* node, const std::vector<char>& active) {
+    std::vector<char> next(nb, 0);
+    bool cont = false;
+    switch (node->type) {
+      case RNode::Type::Leaf:
+        for (size_t b = 0; b < nb; b++) {
+          if (!active[b]) continue;
+          RNode* tgt = s.leaves[b0 + b];
+          v.leaf(*node, *tgt);
+          pp += (unsigned long long)node->n_particles * tgt->n_particles;
+          if (s.record_lists) s.lists[b0 + b].push_back({node->key, 0});
+        }
+        break;
+      case RNode::Type::Internal:
+        for (size_t b = 0; b < nb; b++) {
+          if (!active[b]) continue;
+          RNode* tgt = s.leaves[b0 + b];
+          bool open = v.open(*node, *tgt);
+          op++;
+          next[b] = open;
+          if (open) {
+            cont = true;
+          } else {
+            v.node(*node, *tgt);
+            pc += (unsigned long long)tgt->n_particles;
+            if (s.record_lists) s.lists[b0 + b].push_back({node->key, 1});
+          }
+        }
+        break;
+      default:
+        break;
+    }
+    if (cont) {
+      for (int c = 0; c < node->n_children; c++) recurse(node->getChild(c), next);
+    }
+  }
+};
+
+void traverse(RefSim& s) {
+  size_t nb = s.leaves.size();
+  if (s.record_lists) {
+    s.lists.assign(nb, {});
+  }
+  size_t ngroups = (nb + s.group - 1) / s.group;
+  unsigned long long pp = 0, pc = 0, op = 0;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : pp, pc, op) num_threads(s.threads)
+#endif
+  for (long g = 0; g < (long)ngroups; g++) {
+    size_t b0 = (size_t)g * s.group;
+    size_t n = std::min((size_t)s.group, nb - b0);
+    GroupTrav t(s, b0, n);
+    std::vector<char> all(n, 1);
+    t.recurse(s.root, all);
+    pp += t.pp;
+    pc += t.pc;
+    op += t.op;
+  }
+  s.n_pp = pp;
+  s.n_pc = pc;
+  s.n_open = op;
+}
+
+double now() {
+#ifdef _OPENMP
+  return omp_get_wtime();
+#else
+  return 0.0;
+#endif
+}
+
+void forces(RefSim& s) {
+  double t0 = now();
+  buildTree(s);
+  double t1 = now();
+  for (auto& p : s.particles) {
+    p.acceleration = Vector3D<Real>(0.0);
+    p.potential = 0.0;
+  }
+  traverse(s);
+  double t2 = now();
+  s.t_build = t1 - t0;
+  s.t_traverse = t2 - t1;
+  size_t n = s.particles.size();
+  s.acc.assign(3 * n, 0.0);
+  s.pot.assign(n, 0.0);
+  s.keys.assign(n, 0);
+  for (auto& p : s.particles) {
+    s.acc[3 * p.order + 0] = p.acceleration.x;
+    s.acc[3 * p.order + 1] = p.acceleration.y;
+    s.acc[3 * p.order + 2] = p.acceleration.z;
+    s.pot[p.order] = p.potential;
+    s.keys[p.order] = p.key;
+  }
+}
+
+// examples/Gravity.C:63-67 with max velocity from src/Subtree.h:164-170.
+double timestep(const RefSim& s) {
+  Real vmax2 = 0.0;
+  for (auto& p : s.particles) {
+    if (p.velocity.lengthSquared() > vmax2) vmax2 = p.velocity.lengthSquared();
+  }
+  Real vmax = std::sqrt(vmax2);
+  Real len = s.universe.greater_corner.x - s.universe.lesser_corner.x;
+  Real t = len / vmax / std::cbrt((Real)s.particles.size());
+  return std::min(t, (Real)s.dt_max);
+}
+
+}  // namespace
+
+extern "C" {
+
+void* ptref_create(int n, const double* x, const double* y, const double* z, const double* vx,
+                   const double* vy, const double* vz, const double* m, const double* soft, int bucket,
+                   double theta, double dt_max, int group, int threads) {
+  RefSim* s = new RefSim();
+  s->bucket = bucket;
+  s->theta = theta;
+  s->dt_max = dt_max;
+  s->group = group > 0 ? group : 64;
+  s->threads = threads > 0 ? threads : 1;
+  s->particles.resize(n);
+  OrientedBox<Real> box;
+  for (int i = 0; i < n; i++) {
+    Particle& p = s->particles[i];
+    p.order = i;
+    p.mass = m[i];
+    p.soft = soft[i];
+    p.position = Vector3D<Real>(x[i], y[i], z[i]);
+    p.velocity = Vector3D<Real>(vx[i], vy[i], vz[i]);
+    p.velocity_predicted = p.velocity;
+    p.potential = 0.0;
+    p.u = 0.0;
+    p.u_predicted = 0.0;
+    p.type = Particle::Type::eDark;
+    box.grow(p.position);
+  }
+  remakeUniverse(*s, box);
+  assignKeys(*s);
+  return s;
+}
+
+void ptref_destroy(void* h) { delete (RefSim*)h; }
+
+void ptref_set_record_lists(void* h, int on) { ((RefSim*)h)->record_lists = on; }
+
+/* nsteps == 0: one force evaluation.  Otherwise nsteps iterations of
+ * src/Driver.h:183-251; outputs describe the LAST force evaluation, and the
+ * particle state is the state after the last drift. */
+int ptref_run(void* hp, int nsteps) {
+  RefSim& s = *(RefSim*)hp;
+  if (nsteps <= 0) {
+    forces(s);
+    return 0;
+  }
+  for (int it = 0; it < nsteps; it++) {
+    forces(s);
+    double dt = timestep(s);
+    s.last_dt = dt;
+    for (auto& p : s.particles) p.kick(dt);
+    OrientedBox<Real> box;
+    for (auto& p : s.particles) {
+      p.perturb(dt);
+      box.grow(p.position);
+    }
+    remakeUniverse(s, box);
+    assignKeys(s);
+  }
+  return 0;
+}
+
+void ptref_get_acc(void* h, double* ax, double* ay, double* az, double* pot) {
+  RefSim& s = *(RefSim*)h;
+  size_t n = s.particles.size();
+  for (size_t i = 0; i < n; i++) {
+    ax[i] = s.acc[3 * i];
+    ay[i] = s.acc[3 * i + 1];
+    az[i] = s.acc[3 * i + 2];
+    pot[i] = s.pot[i];
+  }
+}
+
+void ptref_get_keys(void* h, uint64_t* keys) {
+  RefSim& s = *(RefSim*)h;
+  std::memcpy(keys, s.keys.data(), s.keys.size() * sizeof(uint64_t));
+}
+
+void ptref_get_state(void* h, double* x, double* y, double* z, double* vx, double* vy, double* vz) {
+  RefSim& s = *(RefSim*)h;
+  for (auto& p : s.particles) {
+    x[p.order] = p.position.x;
+    y[p.order] = p.position.y;
+    z[p.order] = p.position.z;
+    vx[p.order] = p.velocity.x;
+    vy[p.order] = p.velocity.y;
+    vz[p.order] = p.velocity.z;
+  }
+}
+
+void ptref_get_universe(void* h, double* lo3, double* hi3) {
+  RefSim& s = *(RefSim*)h;
+  lo3[0] = s.universe.lesser_corner.x;
+  lo3[1] = s.universe.lesser_corner.y;
+  lo3[2] = s.universe.lesser_corner.z;
+  hi3[0] = s.universe.greater_corner.x;
+  hi3[1] = s.universe.greater_corner.y;
+  hi3[2] = s.universe.greater_corner.z;
+}
+
+void ptref_get_counters(void* h, unsigned long long* out4, double* times2, double* last_dt) {
+  RefSim& s = *(RefSim*)h;
+  out4[0] = s.n_pp;
+  out4[1] = s.n_pc;
+  out4[2] = s.n_open;
+  out4[3] = s.leaves.size();
+  times2[0] = s.t_build;
+  times2[1] = s.t_traverse;
+  *last_dt = s.last_dt;
+}
+
+long ptref_num_nodes(void* h) { return (long)((RefSim*)h)->pool.size(); }
+
+/* Node dump of the last build, in allocation (pre-order) order.
+ * ints:    [type, depth, count(n_particles or data.count), n_children]
+ * dbls:    [mass, cmx, cmy, cmz, soft, radius, xx, xy, xz, yy, yz, zz,
+ *           lox, loy, loz, hix, hiy, hiz]  (18 per node) */
+void ptref_get_nodes(void* h, uint64_t* keys, int* ints4, double* dbls18) {
+  RefSim& s = *(RefSim*)h;
+  size_t i = 0;
+  for (auto& nd : s.pool) {
+    keys[i] = nd.key;
+    ints4[4 * i + 0] = (int)nd.type;
+    ints4[4 * i + 1] = nd.depth;
+    ints4[4 * i + 2] = nd.data.count;
+    ints4[4 * i + 3] = nd.n_children;
+    const auto& mm = nd.data.multipoles;
+    double* d = dbls18 + 18 * i;
+    d[0] = mm.totalMass;
+    d[1] = mm.cm.x;
+    d[2] = mm.cm.y;
+    d[3] = mm.cm.z;
+    d[4] = mm.soft;
+    d[5] = mm.radius;
+    d[6] = mm.xx;
+    d[7] = mm.xy;
+    d[8] = mm.xz;
+    d[9] = mm.yy;
+    d[10] = mm.yz;
+    d[11] = mm.zz;
+    d[12] = nd.data.box.lesser_corner.x;
+    d[13] = nd.data.box.lesser_corner.y;
+    d[14] = nd.data.box.lesser_corner.z;
+    d[15] = nd.data.box.greater_corner.x;
+    d[16] = nd.data.box.greater_corner.y;
+    d[17] = nd.data.box.greater_corner.z;
+    i++;
+  }
+}
+
+long ptref_num_buckets(void* h) { return (long)((RefSim*)h)->leaves.size(); }
+
+void ptref_get_bucket_keys(void* h, uint64_t* keys) {
+  RefSim& s = *(RefSim*)h;
+  for (size_t i = 0; i < s.leaves.size(); i++) keys[i] = s.leaves[i]->key;
+}
+
+/* Interaction lists (CSR over buckets in DFS order): offsets has
+ * nbuckets+1 entries; entries hold node keys, kinds 0 = P2P leaf, 1 = P2C. */
+long ptref_list_total(void* h) {
+  RefSim& s = *(RefSim*)h;
+  long t = 0;
+  for (auto& l : s.lists) t += (long)l.size();
+  return t;
+}
+
+void ptref_get_lists(void* h, long* offsets, uint64_t* keys, int* kinds) {
+  RefSim& s = *(RefSim*)h;
+  long o = 0;
+  for (size_t b = 0; b < s.lists.size(); b++) {
+    offsets[b] = o;
+    for (auto& e : s.lists[b]) {
+      keys[o] = e.key;
+      kinds[o] = e.kind;
+      o++;
+    }
+  }
+  offsets[s.lists.size()] = o;
+}
+
+}  // extern "C"

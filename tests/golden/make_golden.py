@@ -1,0 +1,159 @@
+"""Generate the committed golden fixtures under tests/golden/.
+
+Run in a container where the reference tree is mounted and the
+reference-sources oracle (oracle/_ref/libptref.so, ``make -C oracle``) is
+built:
+
+    python tests/golden/make_golden.py [--reference /root/reference]
+
+Outputs
+-------
+lambs_kat.npz
+    The reference's own force-accuracy fixture (tests/gravity/
+    lambs.00200_subsamp_30K, big-endian Tipsy, 30000 dark particles, eps
+    2.5e-4) as FP32 positions, plus the accelerations that the reference's
+    tests/gravity/direct.acc holds for 2000 seeded target particles.  It is
+    the known-answer test of the FP64 spline direct sum.
+ref_<case>.json
+    SHA-256 digests (and a few sample values) of every output of the
+    reference's own gravity sources, compiled where they lie, on a seeded
+    workload: particle keys, the node dump (canonical key order), the
+    per-bucket interaction lists, accelerations, partial potentials, and the
+    state after the configured number of kick/perturb steps.  The C oracle
+    and the CUDA path must reproduce these bit for bit.
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import os
+import struct
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from paratreet_b200 import ics  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+# name -> (generator, kwargs, bucket, theta, dt_max, steps)
+CASES = {
+    "plummer_10k": (ics.plummer, dict(n=10000, seed=42, soft=0.01), 16, 0.7, 0.01, 1),
+    "mixture_16k": (ics.mixture, dict(n=16384, seed=7, soft=1e-4), 16, 0.7, 1e-4, 3),
+    "plummer_4k_b32_t05": (ics.plummer, dict(n=4096, seed=5, soft=1e-3), 32, 0.5, 0.01, 1),
+    "hernquist_8k_t10": (ics.hernquist, dict(n=8192, seed=3, soft=0.01), 32, 1.0, 0.005, 2),
+}
+
+
+def digest(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def run_case(name):
+    gen, kw, bucket, theta, dt_max, steps = CASES[name]
+    p = gen(**kw)
+    r = O.RefSim(p, bucket=bucket, theta=theta, dt_max=dt_max, threads=1)
+    r.forces(record_lists=True)
+    ax, ay, az, pot = r.acc()
+    tree = O.sort_tree(r.tree())
+    lists = r.lists()
+    cnt = r.counters()
+    out = {
+        "case": name,
+        "generator": gen.__name__,
+        "kwargs": kw,
+        "bucket": bucket,
+        "theta": theta,
+        "dt_max": dt_max,
+        "steps": steps,
+        "n_nodes": int(tree.keys.size),
+        "n_buckets": int(lists.bucket_keys.size),
+        "n_pp": cnt["n_pp"],
+        "n_pc": cnt["n_pc"],
+        "sha256": {
+            "keys": digest(r.keys()),
+            "node_keys": digest(tree.keys),
+            "node_types": digest(tree.types.astype(np.int32)),
+            "node_counts": digest(tree.count.astype(np.int32)),
+            "node_moments": digest(tree.moments),
+            "bucket_keys": digest(lists.bucket_keys),
+            "list_offsets": digest(lists.offsets.astype(np.int64)),
+            "list_keys": digest(lists.keys),
+            "list_kinds": digest(lists.kinds.astype(np.int32)),
+            "ax": digest(ax), "ay": digest(ay), "az": digest(az), "pot": digest(pot),
+        },
+        "samples": {
+            "idx": [0, 1, 2, int(p["x"].size // 2), int(p["x"].size - 1)],
+        },
+    }
+    idx = out["samples"]["idx"]
+    out["samples"]["ax"] = [float(ax[i]) for i in idx]
+    out["samples"]["pot"] = [float(pot[i]) for i in idx]
+    r.close()
+    r = O.RefSim(p, bucket=bucket, theta=theta, dt_max=dt_max, threads=1)
+    r.run(steps)
+    st = r.state()
+    a2 = r.acc()
+    out["after_steps"] = {
+        "last_dt": r.counters()["last_dt"],
+        "sha256": {k: digest(v) for k, v in zip(("x", "y", "z", "vx", "vy", "vz"), st)},
+        "acc_sha256": {k: digest(v) for k, v in zip(("ax", "ay", "az", "pot"), a2)},
+    }
+    with open(os.path.join(OUT, f"ref_{name}.json"), "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+    print(name, out["n_nodes"], out["n_buckets"], out["n_pp"], out["n_pc"])
+
+
+def read_tipsy_dark(path):
+    with open(path, "rb") as f:
+        buf = f.read()
+    t, n, ndim, nsph, ndark, nstar = struct.unpack(">diiiii", buf[:28])
+    assert nsph == 0 and nstar == 0 and n == ndark
+    d = np.frombuffer(buf[32:32 + 36 * ndark], dtype=">f4").reshape(ndark, 9)
+    return d
+
+
+def read_acc(path):
+    v = np.loadtxt(path)
+    n = int(v[0])
+    a = v[1:].reshape(3, n)
+    return a
+
+
+def make_kat(reference):
+    g = os.path.join(reference, "tests", "gravity")
+    d = read_tipsy_dark(os.path.join(g, "lambs.00200_subsamp_30K"))
+    acc = read_acc(os.path.join(g, "direct.acc"))
+    n = d.shape[0]
+    rng = np.random.default_rng(2024)
+    tgt = np.sort(rng.choice(n, 2000, replace=False)).astype(np.int32)
+    np.savez_compressed(
+        os.path.join(OUT, "lambs_kat.npz"),
+        pos=d[:, 1:4].astype(np.float32),
+        mass=d[:, 0].astype(np.float32),
+        eps=d[:, 7].astype(np.float32),
+        targets=tgt,
+        acc=acc[:, tgt].T.copy(),
+    )
+    print("kat", n, tgt.size)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--cases", nargs="*", default=list(CASES))
+    a = ap.parse_args()
+    if not O.ref_available():
+        sys.exit("oracle/_ref/libptref.so is missing: run `make -C oracle` with the reference mounted")
+    make_kat(a.reference)
+    for c in a.cases:
+        run_case(c)
+
+
+if __name__ == "__main__":
+    main()
