@@ -1,0 +1,393 @@
+"""Benchmark of the B200 Barnes-Hut gravity path.
+
+Headline: force evaluations / s of one force pass (universe, keys, sort,
+octree build, upward pass, traversal) at N = 16,777,216 (Plummer sphere, seed
+42, eps 1e-3, bucket 32, theta 0.7) in the mixed-precision form, with inputs
+resident in HBM.  A "step" is one force pass.  Also reported: the same pass
+end to end through the C ABI with host buffers (e2e), the FP64 form, force
+errors of both against the FP64 direct sum on 4096 seeded targets, the
+traversal kernel's roofline, and the reference CPU path on the host cores.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Multi-GPU (torchrun): every rank holds the whole system, builds the whole
+tree and traverses its contiguous share of the DFS-ordered buckets (strong
+scaling of one force pass); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "force_evals_per_s"
+UNIT = "force evaluations/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=1 << 24)
+    ap.add_argument("--workload", default="plummer")
+    ap.add_argument("--theta", type=float, default=0.7)
+    ap.add_argument("--bucket", type=int, default=32)
+    ap.add_argument("--soft", type=float, default=1e-3)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--targets", type=int, default=4096)
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--no-extras", action="store_true", help="skip e2e, fp64 comparison, errors, cpu baseline")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    return ap.parse_args()
+
+
+def make_ics(a):
+    from paratreet_b200 import ics
+    if a.workload == "plummer":
+        return ics.plummer(a.n, seed=42, soft=a.soft)
+    if a.workload == "mixture":
+        return ics.mixture(a.n, seed=7, soft=a.soft)
+    if a.workload == "hernquist":
+        return ics.hernquist(a.n, seed=3, soft=a.soft)
+    raise SystemExit(f"unknown workload {a.workload}")
+
+
+def workload_config(a, world):
+    return {"workload": f"{a.workload} N={a.n} eps={a.soft} bucket={a.bucket} theta={a.theta}",
+            "n_particles": a.n, "bucket": a.bucket, "theta": a.theta, "precision": a.precision,
+            "parallelism": f"buckets sharded over {world} GPU(s)" if world > 1 else "1 GPU",
+            "l2": "inputs (>=1 GiB particle SoA, >=128 MiB node records) exceed the 126 MB L2"}
+
+
+class ClockSampler:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def dist_init(a):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def max_over_ranks(v: float, world: int) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def rel_errors(a, ref):
+    num = np.sqrt((a[0] - ref[0]) ** 2 + (a[1] - ref[1]) ** 2 + (a[2] - ref[2]) ** 2)
+    den = np.sqrt(ref[0] ** 2 + ref[1] ** 2 + ref[2] ** 2)
+    e = num / den
+    return {"rms": float(np.sqrt(np.mean(e * e))), "p99": float(np.percentile(e, 99)), "max": float(e.max())}
+
+
+# ----------------------------------------------------------------- reference arm
+def run_reference(a):
+    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    cfg = workload_config(a, 1)
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "metric": METRIC,
+                          "unavailable": "reference-sources oracle (oracle/_ref) was not built"}))
+        return 0
+    p = make_ics(a)
+    threads = os.cpu_count() or 1
+    vals = []
+    sample_desc = None
+    for s in range(a.warmup + a.steps):
+        v, sample_desc = reference_sample(p, a, threads, seconds=a.cpu_seconds / 2)
+        if s >= a.warmup:
+            vals.append(v)
+    value = float(np.mean(vals))
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
+           "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "data": "synthetic",
+           "dtype": "f64", "config": cfg, "vs_baseline": None,
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                            "sample": sample_desc},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+def reference_sample(p, a, threads, seconds=10.0):
+    """Reference CPU path (the reference's own gravity sources): full tree
+    build at N, traversal of a strided sample of bucket groups, scaled to N."""
+    from oracle import oracle as O
+    r = O.RefSim(p, bucket=a.bucket, theta=a.theta, dt_max=0.01, group=16, threads=threads)
+    t_build, t_trav, frac = r.forces_sample(stride=0, budget_s=seconds)
+    r.close()
+    t_est = t_build + t_trav / max(frac, 1e-12)
+    desc = (f"reference gravity sources (oracle/_ref, -O2 FP64) on {threads} threads: full tree build at "
+            f"N={a.n} ({t_build:.2f} s) + traversal of {100 * frac:.3f}% of the particles' buckets "
+            f"({t_trav:.2f} s), traversal scaled to all buckets")
+    return a.n / t_est, desc
+
+
+# ----------------------------------------------------------------- our arm
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference(a)
+    world, rank, local = dist_init(a)
+    import torch
+    torch.cuda.set_device(local)
+    from paratreet_b200.gravity import GravitySimulation
+
+    p = make_ics(a)
+    n = a.n
+    sim = GravitySimulation(max_particles_per_leaf=a.bucket, theta=a.theta, max_timestep=0.01,
+                            precision=a.precision, device=local)
+    stream = torch.cuda.current_stream()
+    sim.set_stream(stream.cuda_stream)
+    sim.set_particles(p)
+
+    def pass_range():
+        if world == 1:
+            sim.start_down()
+        else:
+            nb = sim.counters()["n_buckets"] or 1
+            b0, b1 = rank * nb // world, (rank + 1) * nb // world
+            sim.start_down(buckets=(b0, b1))
+
+    sim.start_down()  # establishes bucket count for sharding
+    for _ in range(a.warmup):
+        pass_range()
+    torch.cuda.synchronize()
+    barrier(world)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    trav_ms, cnts = [], None
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        barrier(world)
+        for k in range(a.steps):
+            ev[k][0].record(stream)
+            pass_range()
+            ev[k][1].record(stream)
+            c = sim.counters()
+            trav_ms.append(c["ms_traverse"])
+            cnts = c
+        torch.cuda.synchronize()
+    step_ms = [s.elapsed_time(e) for s, e in ev]
+    t_local = sum(step_ms) / 1e3
+    t = max_over_ranks(t_local, world)
+    barrier(world)
+    value = n * a.steps / t
+    launches = gpu_launches(cnts)
+
+    # roofline of the traversal (dominant kernel)
+    flops = 20.0 * cnts["n_pp"] + 66.0 * cnts["n_pc"]
+    t_trav = float(np.mean(trav_ms)) / 1e3
+    peaks = measured_peaks()
+    clocks = clk.summary()
+    sm_max = (peaks.get("sm_max_mhz") or clocks.get("sm_max_mhz") or 1965.0)
+    import torch.cuda as tc
+    nsm = tc.get_device_properties(local).multi_processor_count
+    lanes = 128 if a.precision == "mixed" else 64
+    peak_tf = nsm * lanes * 2 * sm_max * 1e6 / 1e12
+    achieved = flops / t_trav / 1e12
+    roofline = {"bound": "fp32" if a.precision == "mixed" else "fp64", "achieved": achieved,
+                "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf, "traffic": None,
+                "kernel": f"traverse_{a.precision}", "flops_per_launch": flops,
+                "flop_model": "20 per P2P pair + 66 per P2C evaluation",
+                "peak_source": f"nominal: {nsm} SMs x {lanes} {'FP32' if lanes == 128 else 'FP64'} lanes x 2 x "
+                               f"{sm_max:.0f} MHz (no measured FP32/FP64 figure in MEASURED_PEAKS.json)"}
+
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+           "warmup": a.warmup, "ms_per_step": t * 1e3 / a.steps, "higher_is_better": True,
+           "scaling": "strong", "vs_baseline": None, "dtype": "f32 interactions / f64 tree"
+           if a.precision == "mixed" else "f64", "data": "synthetic (seeded Plummer sphere)",
+           "config": workload_config(a, world), "gpu_launches": launches * a.steps,
+           "roofline": roofline, "clocks": clocks,
+           "phases_ms": {k: cnts[k] for k in ("ms_keys", "ms_sort", "ms_build", "ms_upward", "ms_traverse",
+                                              "ms_total")},
+           "interactions": {"n_pp": cnts["n_pp"], "n_pc": cnts["n_pc"], "n_open": cnts["n_open"],
+                            "n_nodes": cnts["n_nodes"], "n_buckets": cnts["n_buckets"]},
+           "interactions_per_s": (cnts["n_pp"] + cnts["n_pc"]) / t_trav}
+
+    if not a.no_extras:
+        out.update(extras(a, sim, p, world, rank, stream, value))
+    sim.close()
+    if rank == 0:
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def gpu_launches(c):
+    """Kernels of our library launched by one force pass (counted from the
+    pass structure: keys 3, sort 8x(3 + scan) + 9 gathers, build per level,
+    upward per level, traversal 1)."""
+    levels = int(c["depth"]) + 2
+    scan_kernels = 3
+    n = 3 + 8 * (2 + scan_kernels + 1) + 9 + 1 + levels * (1 + scan_kernels + 1) + 2 * levels + 1 + 1 + levels + 1 + 1
+    return n
+
+
+def extras(a, sim, p, world, rank, stream, value):
+    import torch
+    n = a.n
+    res = {}
+    # e2e through the C ABI with pinned host buffers
+    fields = ("x", "y", "z", "vx", "vy", "vz", "m", "soft")
+    pinned = {k: torch.from_numpy(np.ascontiguousarray(p[k])).pin_memory() for k in fields}
+    outs = {k: torch.empty(n, dtype=torch.float64).pin_memory() for k in ("ax", "ay", "az", "pot_full")}
+    host = {k: pinned[k].numpy() for k in fields}
+    hout = {k: outs[k].numpy() for k in outs}
+    torch.cuda.synchronize()
+    steps = max(1, min(a.steps, 3))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    e0.record(stream)
+    for _ in range(steps):
+        sim.set_particles(host)
+        if world == 1:
+            sim.start_down()
+        else:
+            nb = sim.counters()["n_buckets"] or 1
+            sim.start_down(buckets=(rank * nb // world, (rank + 1) * nb // world))
+        sim.accelerations({"ax": hout["ax"], "ay": hout["ay"], "az": hout["az"], "pot": None,
+                           "pot_full": hout["pot_full"]})
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
+    res["e2e"] = {"value": n * steps / t, "unit": UNIT, "h2d_bytes_per_step": 8 * 8 * n,
+                  "d2h_bytes_per_step": 4 * 8 * n, "steps": steps,
+                  "path": "pt_set_particles (pinned H2D) + pt_compute_forces + pt_get_accel (D2H)"}
+    if rank != 0:
+        return res
+    # force errors vs the FP64 direct sum on seeded targets, mixed and FP64
+    rng = np.random.default_rng(43)
+    tgt = np.sort(rng.choice(n, size=min(a.targets, n), replace=False)).astype(np.int32)
+    dax, day, daz, _ = sim.direct_sum(tgt)
+    sim.start_down()
+    am = sim.accelerations()
+    err_m = rel_errors((am["ax"][tgt], am["ay"][tgt], am["az"][tgt]), (dax, day, daz))
+    other = "fp64" if a.precision == "mixed" else "mixed"
+    sim.set_precision(other)
+    sim.start_down()
+    t64 = []
+    for _ in range(a.fp64_steps):
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        sim.start_down()
+        s1.record(stream)
+        torch.cuda.synchronize()
+        t64.append(s0.elapsed_time(s1) / 1e3)
+    a64 = sim.accelerations()
+    c64 = sim.counters()
+    err_o = rel_errors((a64["ax"][tgt], a64["ay"][tgt], a64["az"][tgt]), (dax, day, daz))
+    diff = rel_errors((am["ax"], am["ay"], am["az"]), (a64["ax"], a64["ay"], a64["az"]))
+    sim.set_precision(a.precision)
+    v_other = n / float(np.mean(t64))
+    res["precision_comparison"] = {
+        f"{a.precision}_force_evals_per_s": value, f"{other}_force_evals_per_s": v_other,
+        "ratio_mixed_over_fp64": (value / v_other) if a.precision == "mixed" else (v_other / value),
+        f"{a.precision}_err_vs_direct": err_m, f"{other}_err_vs_direct": err_o,
+        "mixed_vs_fp64_all_particles": diff, "targets": int(tgt.size), "target_seed": 43,
+        f"{other}_ms_traverse": c64["ms_traverse"]}
+    # CPU baseline: the reference's gravity sources on the host cores
+    try:
+        threads = os.cpu_count() or 1
+        v, desc = reference_sample(p, a, threads, seconds=a.cpu_seconds)
+        res["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "reference", "sample": desc}
+    except Exception as e:  # reported, not fatal
+        res["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                               "sample": f"failed: {e}"}
+    return res
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,180 @@
+/*
+ * pt_gravity.h -- C ABI of the B200 Barnes-Hut gravity path.
+ *
+ * Drop-in replacement for the path ParaTreeT's Gravity example runs once per
+ * iteration: universe + SFC keys, key sort, octree build, upward pass of
+ * CentroidData / MultipoleMoments, the TransposedDownTraverser walk with
+ * GravityVisitor (open / node / leaf), and the kick / perturb integrator.
+ *
+ * Conventions
+ *   - Every function returns an int status: PT_OK (0) or a negative PT_E*
+ *     code; pt_last_error() gives the text.  Nothing throws across the ABI.
+ *   - Host arrays are FP64 structure-of-arrays in the caller's particle order
+ *     (the reference's Particle::order, src/Reader.C:89).  Outputs are always
+ *     returned in that order.
+ *   - Device memory is owned by the handle.  One host thread per handle.
+ *     Work is issued on the handle's stream (pt_set_stream) and every call
+ *     that returns host data synchronises that stream.
+ *   - Nodes and buckets are reported in the layouts documented at each
+ *     getter; node keys are the reference's (root 1, child = key<<3 | c;
+ *     src/Subtree.h:325, src/Utility.h:105-108).
+ */
+#ifndef PT_GRAVITY_H_
+#define PT_GRAVITY_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PT_ABI_VERSION 1
+
+enum {
+  PT_OK = 0,
+  PT_E_ARG = -1,        /* bad argument */
+  PT_E_CUDA = -2,       /* CUDA runtime error */
+  PT_E_NOMEM = -3,      /* device allocation failed */
+  PT_E_STATE = -4,      /* call out of order (e.g. no particles) */
+  PT_E_DEVICE = -5,     /* a kernel reported an error status */
+  PT_E_NONFINITE = -6,  /* NaN/Inf in particle positions */
+  PT_E_UNSUPPORTED = -7 /* feature not built in this library */
+};
+
+/* Arithmetic of the traversal. */
+enum {
+  PT_FP64 = 0,  /* reference-exact FP64 (bit-identical to the reference built
+                   with -DUSE_DOUBLE_FP) */
+  PT_MIXED = 1  /* FP64 positions, tree and opening tests; FP32 P2P / P2C
+                   interactions on bucket-relative offsets with compensated
+                   FP32 accumulation */
+};
+
+/* Integrator of pt_step. */
+enum {
+  PT_KKD = 0,  /* the reference's iteration (src/Driver.h:218-250,
+                  src/Particle.C:7-21): forces(x_n); v += a dt/2; v += a dt/2;
+                  x += v dt */
+  PT_KDK = 1   /* textbook leapfrog: v += a(x_n) dt/2; x += v dt; forces(x_{n+1});
+                  v += a dt/2 */
+};
+
+typedef struct pt_config {
+  double theta;      /* opening angle: GravityVisitor(offset, theta),
+                        examples/GravityVisitor.h:16-20, examples/Main.C:55 */
+  int bucket;        /* max particles per leaf: Configuration::
+                        max_particles_per_leaf (-l), examples/Main.C:29 */
+  int precision;     /* PT_FP64 or PT_MIXED */
+  int integrator;    /* PT_KKD or PT_KDK */
+  double dt_max;     /* max_timestep (-j), examples/Main.C:57,77; the step is
+                        min(L / v_max / cbrt(N), dt_max), examples/Gravity.C:63-67 */
+  int device;        /* CUDA device ordinal */
+  int record_lists;  /* keep per-bucket interaction lists of every force pass */
+  int reserved[8];
+} pt_config;
+
+typedef struct pt_handle pt_handle;
+
+typedef struct pt_counters {
+  uint64_t n_pp;       /* P2P pairs, n_src * n_tgt per leaf() (src/Traverser.h:27) */
+  uint64_t n_pc;       /* P2C evaluations, n_tgt per node() (src/Traverser.h:35) */
+  uint64_t n_open;     /* open() tests */
+  int64_t n_nodes;
+  int64_t n_buckets;
+  int32_t depth;       /* deepest level */
+  int32_t reserved;
+  /* device milliseconds of the last force pass, by phase */
+  float ms_keys;       /* bbox + universe + keys */
+  float ms_sort;       /* radix sort + permute */
+  float ms_build;      /* octree build + bucket order */
+  float ms_upward;     /* leaf moments + upward pass */
+  float ms_traverse;   /* traversal (the dominant kernel) */
+  float ms_total;
+} pt_counters;
+
+/* Library / handle ------------------------------------------------------- */
+int pt_abi_version(void);
+/* Fills the reference's defaults for the Gravity example with the octree:
+ * theta 0.7, bucket 16, FP64, KKD, dt_max 1e-5, device 0. */
+int pt_config_default(pt_config* cfg);
+/* Replaces paratreet::initialize<CentroidData> (src/Paratreet.h:220-239) for
+ * this path: allocates the device state of one simulation. */
+int pt_create(const pt_config* cfg, pt_handle** out);
+int pt_destroy(pt_handle* h);
+const char* pt_last_error(const pt_handle* h);
+/* cudaStream_t as void*; NULL = the handle's own stream. */
+int pt_set_stream(pt_handle* h, void* stream);
+int pt_set_theta(pt_handle* h, double theta);
+int pt_set_precision(pt_handle* h, int precision);
+
+/* Particles -------------------------------------------------------------- */
+/* Replaces Reader::load + the universe reduction (src/Reader.C:11-107,
+ * src/Driver.h:96-107): copies FP64 host SoA to the device.  soft is the
+ * per-particle softening (Particle::soft, the Tipsy eps). */
+int pt_set_particles(pt_handle* h, int64_t n, const double* x, const double* y, const double* z,
+                     const double* vx, const double* vy, const double* vz, const double* m,
+                     const double* soft);
+/* Same from device pointers (FP64, n elements each); copied device-to-device. */
+int pt_set_particles_device(pt_handle* h, int64_t n, const double* x, const double* y,
+                            const double* z, const double* vx, const double* vy, const double* vz,
+                            const double* m, const double* soft);
+int64_t pt_num_particles(const pt_handle* h);
+
+/* Force pass ------------------------------------------------------------- */
+/* One force evaluation: universe (src/Driver.h:67-80), keys
+ * (src/Decomposition.C:58-64), sort + build + upward (src/Subtree.h:276-384),
+ * and Partition::startDown<GravityVisitor> over every bucket
+ * (src/Partition.h:129-134, src/Traverser.h:154-217,
+ * examples/Gravity.C:29-33). */
+int pt_compute_forces(pt_handle* h);
+/* Only the buckets [b0, b1) of the DFS-ordered bucket list are traversed
+ * (multi-GPU sharding of one system); the tree is still built in full. */
+int pt_compute_forces_range(pt_handle* h, int64_t b0, int64_t b1);
+/* Accelerations and potentials of the last force pass, caller order.
+ * pot: the reference's potential (quadrupole node() terms only,
+ * examples/GravityVisitor.h:218); pot_full: every interaction's potential
+ * (P2P spline, quadrupole, monopole).  Any pointer may be NULL. */
+int pt_get_accel(pt_handle* h, double* ax, double* ay, double* az, double* pot, double* pot_full);
+/* Device pointers (sorted order, FP64) of the last force pass, and the
+ * sorted-to-caller permutation (int32 order[i] = caller index of sorted i). */
+int pt_device_accel(pt_handle* h, const double** ax, const double** ay, const double** az,
+                    const int32_t** order);
+
+/* Integration ------------------------------------------------------------ */
+/* nsteps iterations of src/Driver.h:183-251 (PT_KKD) or leapfrog (PT_KDK).
+ * dt = min(L / v_max / cbrt(N), dt_max) per step. */
+int pt_step(pt_handle* h, int nsteps);
+int pt_get_state(pt_handle* h, double* x, double* y, double* z, double* vx, double* vy, double* vz);
+int pt_last_dt(const pt_handle* h, double* dt);
+
+/* Parity / inspection ---------------------------------------------------- */
+/* SFC keys of the last pass with the placeholder bit (caller order). */
+int pt_get_keys(pt_handle* h, uint64_t* keys);
+int pt_get_universe(pt_handle* h, double* lo3, double* hi3);
+int pt_get_tree_size(pt_handle* h, int64_t* n_nodes, int64_t* n_buckets);
+/* Node dump, breadth-first order.  ints4: [type (1 Leaf, 2 EmptyLeaf,
+ * 6 Internal; src/Node.h:82-95), depth, count, n_children]; dbls18:
+ * [mass, cm x/y/z, soft, radius, xx, xy, xz, yy, yz, zz, box lo x/y/z,
+ * box hi x/y/z] (CentroidData + MultipoleMoments,
+ * examples/CentroidData.h:24-38, examples/MultipoleMoments.h:161-184). */
+int pt_get_tree(pt_handle* h, uint64_t* keys, int32_t* ints4, double* dbls18);
+/* Keys of the buckets (leaves) in DFS order (Subtree::leaves). */
+int pt_get_bucket_keys(pt_handle* h, uint64_t* keys);
+/* Interaction lists of the last pass (needs record_lists): CSR over buckets
+ * in DFS order; entries are node keys in traversal order, kinds 0 = leaf()
+ * P2P, 1 = node() P2C. */
+int pt_get_lists_size(pt_handle* h, int64_t* total);
+int pt_get_lists(pt_handle* h, int64_t* offsets, uint64_t* keys, int32_t* kinds);
+int pt_get_counters(pt_handle* h, pt_counters* c);
+
+/* FP64 direct sum (the force-error yardstick) ------------------------------
+ * Isolated spline-softened sum over all particles for nt caller indices,
+ * the kernel of examples/GravityVisitor.h:87-120 with twoh = soft_i + soft_j. */
+int pt_direct_sum(pt_handle* h, int64_t nt, const int32_t* targets, double* ax, double* ay,
+                  double* az, double* pot);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PT_GRAVITY_H_ */

@@ -81,6 +81,7 @@ def _ref_lib():
         lib.ptref_create.argtypes = [C.c_int] + [_dp] * 8 + [C.c_int, C.c_double, C.c_double, C.c_int, C.c_int]
         lib.ptref_run.argtypes = [C.c_void_p, C.c_int]
         lib.ptref_set_record_lists.argtypes = [C.c_void_p, C.c_int]
+        lib.ptref_forces_sample.argtypes = [C.c_void_p, C.c_double] + [C.POINTER(C.c_double)] * 3
         _ref = lib
     return _ref
 
@@ -214,6 +215,13 @@ class RefSim(_Sim):
         a = [np.zeros(self.n) for _ in range(4)]
         self._lib.ptref_get_acc(self._h, *a)
         return a  # ax, ay, az, pot (partial potential)
+
+    def forces_sample(self, stride=0, budget_s=10.0):
+        """Timed bounded sample: full build, then bucket groups until budget_s.
+        Returns (build seconds, traversal seconds, traversed particle share)."""
+        tb, tt, fr = C.c_double(), C.c_double(), C.c_double()
+        self._lib.ptref_forces_sample(self._h, budget_s, C.byref(tb), C.byref(tt), C.byref(fr))
+        return tb.value, tt.value, fr.value
 
 
 def direct_sum(p: dict, targets: np.ndarray, threads: int = 1):

@@ -291,9 +291,66 @@ double timestep(const RefSim& s) {
   return std::min(t, (Real)s.dt_max);
 }
 
+
+// Bounded CPU sample of one force pass: the full tree build, then bucket
+// groups in a fixed pseudo-random order on all threads until budget_s of
+// traversal time is spent.  frac = share of the particles whose buckets were
+// traversed.
+void forces_sample(RefSim& s, double budget_s, double* t_build, double* t_trav, double* frac) {
+  double t0 = now();
+  buildTree(s);
+  double t1 = now();
+  for (auto& p : s.particles) {
+    p.acceleration = Vector3D<Real>(0.0);
+    p.potential = 0.0;
+  }
+  s.record_lists = 0;
+  size_t nb = s.leaves.size();
+  size_t ngroups = (nb + s.group - 1) / s.group;
+  std::vector<size_t> order(ngroups);
+  for (size_t g = 0; g < ngroups; g++) order[g] = g;
+  uint64_t st = 0x9E3779B97F4A7C15ull;
+  for (size_t g = ngroups; g > 1; g--) {
+    st ^= st << 13; st ^= st >> 7; st ^= st << 17;
+    std::swap(order[g - 1], order[st % g]);
+  }
+  std::atomic<size_t> next(0);
+  std::atomic<long> done_particles(0);
+  double tstart = now();
+#ifdef _OPENMP
+#pragma omp parallel num_threads(s.threads)
+#endif
+  {
+    while (true) {
+      if (now() - tstart > budget_s) break;
+      size_t k = next.fetch_add(1);
+      if (k >= ngroups) break;
+      size_t g = order[k];
+      size_t b0 = g * s.group;
+      size_t n = std::min((size_t)s.group, nb - b0);
+      GroupTrav t(s, b0, n);
+      std::vector<char> all(n, 1);
+      t.recurse(s.root, all);
+      long cnt = 0;
+      for (size_t b = 0; b < n; b++) cnt += s.leaves[b0 + b]->n_particles;
+      done_particles += cnt;
+    }
+  }
+  double t2 = now();
+  *t_build = t1 - t0;
+  *t_trav = t2 - tstart;
+  *frac = (double)done_particles.load() / (double)std::max<size_t>(1, s.particles.size());
+}
+
 }  // namespace
 
 extern "C" {
+
+int ptref_forces_sample(void* h, double budget_s, double* t_build, double* t_trav, double* frac) {
+  forces_sample(*(RefSim*)h, budget_s, t_build, t_trav, frac);
+  return 0;
+}
+
 
 void* ptref_create(int n, const double* x, const double* y, const double* z, const double* vx,
                    const double* vy, const double* vz, const double* m, const double* soft, int bucket,

@@ -1,0 +1,813 @@
+// pt_api.cu -- the C ABI (include/pt_gravity.h): handle, device buffers and the
+// per-pass orchestration of the kernels.
+//
+// One force pass (pt_compute_forces) runs, on the handle's stream:
+//   K1 bbox + universe -> K2 keys -> K3 radix sort -> K4 permute
+//   -> K5 level-synchronous octree build (+ bucket DFS order)
+//   -> K6 leaf moments + upward pass + traversal records
+//   -> K7 traversal (FP64 or mixed), optionally with interaction lists.
+// The host reads back one 4-byte count per tree level (to size the next
+// level) and the status word at the end; everything else stays on the device.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/pt_gravity.h"
+#include "pt_launch.h"
+
+using namespace pt;
+
+struct pt_handle {
+  pt_config cfg{};
+  std::string err;
+  int sms = 148;
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+
+  int64_t n = 0, cap_n = 0;
+  Particles p{};
+  double* tmp_d = nullptr;
+  int32_t* tmp_i = nullptr;
+  uint64_t* key_alt = nullptr;
+  uint32_t *idx = nullptr, *idx_alt = nullptr;
+  uint32_t* sort_hist = nullptr;
+  uint32_t* scan_scratch = nullptr;
+  size_t scan_scratch_elems = 0;
+  uint32_t* d_total = nullptr;
+  double* bbox_partial = nullptr;
+  int bbox_blocks = 0;
+  double* d_uni = nullptr;  // 12 doubles
+  unsigned* d_status = nullptr;
+  unsigned long long* d_counters = nullptr;  // 3
+  unsigned* d_work = nullptr;
+  unsigned long long* d_vmax2 = nullptr;
+  float4* srcf = nullptr;
+  float* softf = nullptr;
+  int64_t cap_srcf = 0;
+
+  Nodes nd{};
+  int64_t node_cap = 0, nnodes = 0;
+  uint32_t* flags = nullptr;
+  std::vector<int64_t> lev;
+  int32_t* buckets = nullptr;
+  int64_t nbuckets = 0, cap_buckets = 0;
+
+  int64_t* list_count = nullptr;
+  int64_t* list_off = nullptr;
+  int32_t* list_node = nullptr;
+  int8_t* list_kind = nullptr;
+  int64_t list_total = 0, list_cap = 0, list_nb = 0;
+  bool lists_valid = false;
+
+  double* dsum = nullptr;  // direct-sum scratch (caller-order copies + partials)
+  int64_t dsum_cap = 0;
+
+  cudaEvent_t ev[7]{};
+  pt_counters last{};
+  double last_dt = 0.0;
+  bool have_forces = false;
+  bool trav_range_partial = false;
+};
+
+namespace {
+
+int fail(pt_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+#define CK(call)                                                                               \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess)                                                                     \
+      return fail(h, (e_ == cudaErrorMemoryAllocation) ? PT_E_NOMEM : PT_E_CUDA,               \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                         \
+  } while (0)
+
+#define CKR(expr)              \
+  do {                         \
+    int r_ = (expr);           \
+    if (r_ != PT_OK) return r_; \
+  } while (0)
+
+template <typename T>
+int dalloc(pt_handle* h, T** ptr, size_t count) {
+  if (*ptr) {
+    cudaFree(*ptr);
+    *ptr = nullptr;
+  }
+  if (count == 0) count = 1;
+  CK(cudaMalloc((void**)ptr, count * sizeof(T)));
+  return PT_OK;
+}
+
+template <typename T>
+void dfree(T*& ptr) {
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+}
+
+int grid_for(const pt_handle* h, int64_t n) {
+  int64_t g = (n + 255) / 256;
+  int64_t cap = (int64_t)h->sms * 8;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+int ensure_particles(pt_handle* h, int64_t n) {
+  if (n <= h->cap_n && h->p.x) return PT_OK;
+  int64_t c = std::max<int64_t>(n, 1);
+  double** dbl[] = {&h->p.x, &h->p.y, &h->p.z, &h->p.vx, &h->p.vy, &h->p.vz, &h->p.m, &h->p.soft,
+                    &h->p.ax, &h->p.ay, &h->p.az, &h->p.pot, &h->p.potf, &h->tmp_d};
+  for (auto pp : dbl) CKR(dalloc(h, pp, c));
+  CKR(dalloc(h, &h->p.order, c));
+  CKR(dalloc(h, &h->tmp_i, c));
+  CKR(dalloc(h, &h->p.key, c));
+  CKR(dalloc(h, &h->key_alt, c));
+  CKR(dalloc(h, &h->idx, c));
+  CKR(dalloc(h, &h->idx_alt, c));
+  CKR(dalloc(h, &h->sort_hist, sort_hist_elems(c)));
+  size_t ss = std::max(scan_scratch_bytes((int64_t)sort_hist_elems(c)), scan_scratch_bytes(8 * c + 64));
+  h->scan_scratch_elems = ss / sizeof(uint32_t) + 1;
+  CKR(dalloc(h, &h->scan_scratch, h->scan_scratch_elems));
+  h->cap_n = c;
+  return PT_OK;
+}
+
+int grow_nodes(pt_handle* h, int64_t need) {
+  if (need <= h->node_cap) return PT_OK;
+  int64_t nc = std::max<int64_t>(need + need / 2, 1024);
+  Nodes o = h->nd;
+  Nodes nn{};
+  int64_t keep = h->nnodes;
+  // build arrays are copied, the rest are (re)computed after the build
+  CKR(dalloc(h, &nn.key, nc));
+  CKR(dalloc(h, &nn.type, nc));
+  CKR(dalloc(h, &nn.depth, nc));
+  CKR(dalloc(h, &nn.pstart, nc));
+  CKR(dalloc(h, &nn.pcount, nc));
+  CKR(dalloc(h, &nn.parent, nc));
+  CKR(dalloc(h, &nn.first_child, nc));
+  CKR(dalloc(h, &nn.count, nc));
+  CKR(dalloc(h, &nn.mom, nc));
+  CKR(dalloc(h, &nn.walk, nc));
+  CKR(dalloc(h, &nn.quad, nc));
+  CKR(dalloc(h, &nn.quadf, nc));
+  CKR(dalloc(h, &nn.fifo, nc));
+  CKR(dalloc(h, &nn.nleaf_sub, nc));
+  CKR(dalloc(h, &nn.nempty_sub, nc));
+  CKR(dalloc(h, &nn.leaf_base, nc));
+  CKR(dalloc(h, &nn.empty_base, nc));
+  if (keep > 0 && o.key) {
+    cudaStream_t st = h->stream;
+    CK(cudaMemcpyAsync(nn.key, o.key, keep * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(nn.type, o.type, keep * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(nn.depth, o.depth, keep * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(nn.pstart, o.pstart, keep * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(nn.pcount, o.pcount, keep * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(nn.parent, o.parent, keep * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(nn.first_child, o.first_child, keep * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(nn.leaf_base, o.leaf_base, keep * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(nn.empty_base, o.empty_base, keep * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+    CK(cudaStreamSynchronize(st));
+  }
+  dfree(o.key); dfree(o.type); dfree(o.depth); dfree(o.pstart); dfree(o.pcount); dfree(o.parent);
+  dfree(o.first_child); dfree(o.count); dfree(o.mom); dfree(o.walk); dfree(o.quad); dfree(o.quadf);
+  dfree(o.fifo); dfree(o.nleaf_sub); dfree(o.nempty_sub); dfree(o.leaf_base); dfree(o.empty_base);
+  h->nd = nn;
+  CKR(dalloc(h, &h->flags, nc));
+  h->node_cap = nc;
+  return PT_OK;
+}
+
+int read_status(pt_handle* h) {
+  unsigned st = 0;
+  CK(cudaMemcpyAsync(&st, h->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (st) {
+    CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned), h->stream));
+    std::string m = "device status:";
+    if (st & kErrNonFinite) m += " non-finite particle position;";
+    if (st & kErrStack) m += " traversal stack overflow;";
+    if (st & kErrBucketTooBig) m += " bucket larger than 32;";
+    if (st & kErrListOverflow) m += " interaction list overflow;";
+    if (st & kErrCapacity) m += " capacity exceeded;";
+    return fail(h, (st & kErrNonFinite) ? PT_E_NONFINITE : PT_E_DEVICE, m);
+  }
+  return PT_OK;
+}
+
+// K1..K4: universe, keys, sort, permute.
+int keys_and_sort(pt_handle* h) {
+  cudaStream_t st = h->stream;
+  const int64_t n = h->n;
+  const int g = grid_for(h, n);
+  launch_bbox(h->p.x, h->p.y, h->p.z, n, h->bbox_partial, h->bbox_blocks, h->d_uni, h->d_status, st);
+  launch_keys(h->p.x, h->p.y, h->p.z, n, h->d_uni, h->p.key, h->idx, g, st);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(h->ev[1], st));
+  radix_sort_pairs(h->p.key, h->idx, h->key_alt, h->idx_alt, n, h->sort_hist, h->scan_scratch, h->d_total, st);
+  double** fields[] = {&h->p.x, &h->p.y, &h->p.z, &h->p.vx, &h->p.vy, &h->p.vz, &h->p.m, &h->p.soft};
+  for (auto f : fields) {
+    gather_f64(*f, h->tmp_d, h->idx, n, g, st);
+    std::swap(*f, h->tmp_d);
+  }
+  gather_i32(h->p.order, h->tmp_i, h->idx, n, g, st);
+  std::swap(h->p.order, h->tmp_i);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(h->ev[2], st));
+  return PT_OK;
+}
+
+// K5: octree build, levels, bucket order.
+int build_tree(pt_handle* h) {
+  cudaStream_t st = h->stream;
+  const int64_t n = h->n;
+  if (h->node_cap < 1024) {
+    h->nnodes = 0;
+    CKR(grow_nodes(h, std::max<int64_t>(1024, n / 2 + 1024)));
+  }
+  h->nnodes = 1;
+  launch_init_root(h->nd, n, h->cfg.bucket, st);
+  h->lev.assign(1, 0);
+  int64_t begin = 0, count = 1;
+  while (true) {
+    launch_flag_internal(h->nd.type, begin, count, h->flags, st);
+    scan_exclusive(h->flags, h->flags, count, h->scan_scratch, h->d_total, st);
+    uint32_t ni = 0;
+    CK(cudaMemcpyAsync(&ni, h->d_total, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    h->lev.push_back(begin + count);
+    if (ni == 0) break;
+    int64_t next = begin + count;
+    int64_t need = next + 8 * (int64_t)ni;
+    if (need > h->node_cap) {
+      h->nnodes = next;
+      CKR(grow_nodes(h, need));
+    }
+    launch_build_children(h->nd, h->p.key, begin, count, h->flags, next, h->cfg.bucket, st);
+    begin = next;
+    count = 8 * (int64_t)ni;
+    h->nnodes = need;
+  }
+  const int L = (int)h->lev.size() - 1;
+  for (int l = L - 1; l >= 0; l--) launch_count_subtree(h->nd, h->lev[l], h->lev[l + 1] - h->lev[l], st);
+  for (int l = 0; l < L; l++) launch_base_topdown(h->nd, h->lev[l], h->lev[l + 1] - h->lev[l], st);
+  int32_t nl = 0;
+  CK(cudaMemcpyAsync(&nl, h->nd.nleaf_sub, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  h->nbuckets = nl;
+  if (nl > h->cap_buckets) {
+    CKR(dalloc(h, &h->buckets, nl));
+    h->cap_buckets = nl;
+  }
+  launch_assign_buckets(h->nd, h->nnodes, h->buckets, nl, st);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(h->ev[3], st));
+  return PT_OK;
+}
+
+// K6: moments, upward pass, traversal records.
+int upward(pt_handle* h) {
+  cudaStream_t st = h->stream;
+  launch_leaf_moments(h->nd, h->nnodes, h->p, st);
+  const int L = (int)h->lev.size() - 1;
+  for (int l = L - 1; l >= 0; l--) launch_upward_level(h->nd, h->lev[l], h->lev[l + 1] - h->lev[l], st);
+  const double gfac = (4.0 / 3.0) / (h->cfg.theta * h->cfg.theta);  // GravityVisitor.h:14,18
+  const int mixed = h->cfg.precision == PT_MIXED;
+  launch_finalize(h->nd, h->nnodes, gfac, mixed, st);
+  if (mixed) {
+    if (h->cap_srcf < h->cap_n) {
+      CKR(dalloc(h, &h->srcf, h->cap_n));
+      CKR(dalloc(h, &h->softf, h->cap_n));
+      h->cap_srcf = h->cap_n;
+    }
+    launch_prep_sources(h->buckets, h->nbuckets, h->nd.walk, h->p, h->srcf, h->softf, st);
+  }
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(h->ev[4], st));
+  return PT_OK;
+}
+
+int run_traversal(pt_handle* h, TravParams& P, int grid) {
+  if (h->cfg.precision == PT_MIXED && P.mode != 1) launch_traverse_mixed(P, h->nd.mom, grid, h->stream);
+  else launch_traverse_f64(P, h->nd.mom, grid, h->stream);
+  CK(cudaGetLastError());
+  return PT_OK;
+}
+
+int traverse(pt_handle* h, int64_t b0, int64_t b1) {
+  cudaStream_t st = h->stream;
+  b0 = std::max<int64_t>(0, std::min(b0, h->nbuckets));
+  b1 = std::max<int64_t>(b0, std::min(b1, h->nbuckets));
+  h->trav_range_partial = !(b0 == 0 && b1 == h->nbuckets);
+  if (h->trav_range_partial) {
+    double* arrs[] = {h->p.ax, h->p.ay, h->p.az, h->p.pot, h->p.potf};
+    for (auto a : arrs) CK(cudaMemsetAsync(a, 0, h->n * sizeof(double), st));
+  }
+  TravParams P{};
+  P.p = h->p;
+  P.walk = h->nd.walk;
+  P.quad = h->nd.quad;
+  P.quadf = h->nd.quadf;
+  P.srcf = h->srcf;
+  P.softf = h->softf;
+  P.buckets = h->buckets;
+  P.b_begin = b0;
+  P.b_end = b1;
+  P.ox = P.oy = P.oz = 0.0;
+  P.counters = h->d_counters;
+  P.work = h->d_work;
+  P.status = h->d_status;
+  const int grid = h->sms * 16;
+  CK(cudaMemsetAsync(h->d_counters, 0, 3 * sizeof(unsigned long long), st));
+  const int64_t nb = b1 - b0;
+  h->lists_valid = false;
+  if (h->cfg.record_lists && nb > 0) {
+    if (nb + 1 > h->list_nb) {
+      CKR(dalloc(h, &h->list_count, nb + 1));
+      CKR(dalloc(h, &h->list_off, nb + 1));
+      h->list_nb = nb + 1;
+    }
+    P.mode = 1;
+    P.list_count = h->list_count;
+    CK(cudaMemsetAsync(h->d_work, 0, sizeof(unsigned), st));
+    CKR(run_traversal(h, P, grid));
+    std::vector<int64_t> cnt(nb), off(nb + 1);
+    CK(cudaMemcpyAsync(cnt.data(), h->list_count, nb * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    off[0] = 0;
+    for (int64_t i = 0; i < nb; i++) off[i + 1] = off[i] + cnt[i];
+    h->list_total = off[nb];
+    if (h->list_total > h->list_cap) {
+      CKR(dalloc(h, &h->list_node, h->list_total));
+      CKR(dalloc(h, &h->list_kind, h->list_total));
+      h->list_cap = h->list_total;
+    }
+    CK(cudaMemcpyAsync(h->list_off, off.data(), (nb + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(h->d_counters, 0, 3 * sizeof(unsigned long long), st));
+    P.mode = 2;
+    P.list_off = h->list_off;
+    P.list_node = h->list_node;
+    P.list_kind = h->list_kind;
+    if (h->cfg.precision == PT_MIXED) {
+      // lists come from the FP64 walk (identical for both forms); evaluate mixed
+      P.mode = 2;
+      CK(cudaMemsetAsync(h->d_work, 0, sizeof(unsigned), st));
+      launch_traverse_f64(P, h->nd.mom, grid, st);  // records lists (and FP64 forces)
+      CK(cudaMemsetAsync(h->d_counters, 0, 3 * sizeof(unsigned long long), st));
+      P.mode = 0;
+    }
+    h->lists_valid = true;
+  } else {
+    P.mode = 0;
+  }
+  CK(cudaMemsetAsync(h->d_work, 0, sizeof(unsigned), st));
+  CK(cudaEventRecord(h->ev[5], st));
+  CKR(run_traversal(h, P, grid));
+  CK(cudaEventRecord(h->ev[6], st));
+  return PT_OK;
+}
+
+int forces(pt_handle* h, int64_t b0, int64_t b1) {
+  if (!h->p.x) return fail(h, PT_E_STATE, "no particles: call pt_set_particles first");
+  cudaStream_t st = h->stream;
+  CK(cudaEventRecord(h->ev[0], st));
+  if (h->n == 0) {
+    h->nnodes = 0;
+    h->nbuckets = 0;
+    h->have_forces = true;
+    return PT_OK;
+  }
+  CKR(keys_and_sort(h));
+  CKR(build_tree(h));
+  CKR(upward(h));
+  CKR(traverse(h, b0, b1));
+  CKR(read_status(h));
+  unsigned long long c[3];
+  CK(cudaMemcpyAsync(c, h->d_counters, sizeof(c), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  pt_counters& k = h->last;
+  k.n_pp = c[0];
+  k.n_pc = c[1];
+  k.n_open = c[2];
+  k.n_nodes = h->nnodes;
+  k.n_buckets = h->nbuckets;
+  k.depth = (int32_t)h->lev.size() - 2;
+  CK(cudaEventElapsedTime(&k.ms_keys, h->ev[0], h->ev[1]));
+  CK(cudaEventElapsedTime(&k.ms_sort, h->ev[1], h->ev[2]));
+  CK(cudaEventElapsedTime(&k.ms_build, h->ev[2], h->ev[3]));
+  CK(cudaEventElapsedTime(&k.ms_upward, h->ev[3], h->ev[4]));
+  CK(cudaEventElapsedTime(&k.ms_traverse, h->ev[5], h->ev[6]));
+  CK(cudaEventElapsedTime(&k.ms_total, h->ev[0], h->ev[6]));
+  h->have_forces = true;
+  return PT_OK;
+}
+
+// examples/Gravity.C:63-67 with v_max from src/Subtree.h:164-170.
+int timestep(pt_handle* h, double* dt) {
+  cudaStream_t st = h->stream;
+  CK(cudaMemsetAsync(h->d_vmax2, 0, sizeof(unsigned long long), st));
+  launch_vmax2(h->p.vx, h->p.vy, h->p.vz, h->n, h->d_vmax2, grid_for(h, h->n), st);
+  unsigned long long bits = 0;
+  double uni[6];
+  CK(cudaMemcpyAsync(&bits, h->d_vmax2, sizeof(bits), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(uni, h->d_uni, sizeof(uni), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  double v2;
+  std::memcpy(&v2, &bits, sizeof(v2));
+  double vmax = std::sqrt(v2);
+  double len = uni[3] - uni[0];
+  double t = len / vmax / std::cbrt((double)h->n);
+  *dt = std::min(t, h->cfg.dt_max);
+  return PT_OK;
+}
+
+int unpermute_f64(pt_handle* h, const double* dsrc, double* host_out) {
+  if (!host_out) return PT_OK;
+  launch_scatter_f64(dsrc, h->tmp_d, h->p.order, h->n, grid_for(h, h->n), h->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(host_out, h->tmp_d, h->n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  return PT_OK;
+}
+
+int set_particles_impl(pt_handle* h, int64_t n, const double* const src[8], cudaMemcpyKind kind) {
+  if (n < 0 || n > (int64_t)INT32_MAX - 64) return fail(h, PT_E_ARG, "particle count out of range");
+  for (int i = 0; i < 8 && n > 0; i++)
+    if (!src[i]) return fail(h, PT_E_ARG, "null particle array");
+  CKR(ensure_particles(h, n));
+  h->n = n;
+  double* dst[8] = {h->p.x, h->p.y, h->p.z, h->p.vx, h->p.vy, h->p.vz, h->p.m, h->p.soft};
+  for (int i = 0; i < 8 && n > 0; i++)
+    CK(cudaMemcpyAsync(dst[i], src[i], n * sizeof(double), kind, h->stream));
+  launch_iota_i32(h->p.order, n, grid_for(h, n), h->stream);
+  CK(cudaGetLastError());
+  h->have_forces = false;
+  h->lists_valid = false;
+  return PT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pt_abi_version(void) { return PT_ABI_VERSION; }
+
+int pt_config_default(pt_config* c) {
+  if (!c) return PT_E_ARG;
+  std::memset(c, 0, sizeof(*c));
+  c->theta = 0.7;
+  c->bucket = 16;
+  c->precision = PT_FP64;
+  c->integrator = PT_KKD;
+  c->dt_max = 1e-5;
+  c->device = 0;
+  c->record_lists = 0;
+  return PT_OK;
+}
+
+int pt_create(const pt_config* cfg, pt_handle** out) {
+  if (!cfg || !out) return PT_E_ARG;
+  *out = nullptr;
+  if (!(cfg->theta > 0.0) || cfg->bucket < 1 || cfg->bucket > 32) return PT_E_ARG;
+  if (cfg->precision != PT_FP64 && cfg->precision != PT_MIXED) return PT_E_ARG;
+  if (cfg->integrator != PT_KKD && cfg->integrator != PT_KDK) return PT_E_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return PT_E_CUDA;
+  if (cfg->device < 0 || cfg->device >= ndev) return PT_E_ARG;
+  pt_handle* h = new pt_handle();
+  h->cfg = *cfg;
+  auto bail = [&](int code) {
+    pt_destroy(h);
+    return code;
+  };
+  if (cudaSetDevice(cfg->device) != cudaSuccess) return bail(PT_E_CUDA);
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess) return bail(PT_E_CUDA);
+  h->sms = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) return bail(PT_E_CUDA);
+  h->stream = h->own_stream;
+  for (auto& e : h->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return bail(PT_E_CUDA);
+  h->bbox_blocks = h->sms * 4;
+  if (dalloc(h, &h->bbox_partial, 6 * (size_t)h->bbox_blocks) != PT_OK) return bail(PT_E_NOMEM);
+  if (dalloc(h, &h->d_uni, 12) != PT_OK) return bail(PT_E_NOMEM);
+  if (dalloc(h, &h->d_status, 1) != PT_OK) return bail(PT_E_NOMEM);
+  if (dalloc(h, &h->d_counters, 3) != PT_OK) return bail(PT_E_NOMEM);
+  if (dalloc(h, &h->d_work, 1) != PT_OK) return bail(PT_E_NOMEM);
+  if (dalloc(h, &h->d_vmax2, 1) != PT_OK) return bail(PT_E_NOMEM);
+  if (dalloc(h, &h->d_total, 4) != PT_OK) return bail(PT_E_NOMEM);
+  if (cudaMemset(h->d_status, 0, sizeof(unsigned)) != cudaSuccess) return bail(PT_E_CUDA);
+  *out = h;
+  return PT_OK;
+}
+
+int pt_destroy(pt_handle* h) {
+  if (!h) return PT_OK;
+  cudaSetDevice(h->cfg.device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  double** dbl[] = {&h->p.x, &h->p.y, &h->p.z, &h->p.vx, &h->p.vy, &h->p.vz, &h->p.m, &h->p.soft,
+                    &h->p.ax, &h->p.ay, &h->p.az, &h->p.pot, &h->p.potf, &h->tmp_d};
+  for (auto pp : dbl) dfree(*pp);
+  dfree(h->p.order); dfree(h->tmp_i); dfree(h->p.key); dfree(h->key_alt); dfree(h->idx); dfree(h->idx_alt);
+  dfree(h->sort_hist); dfree(h->scan_scratch); dfree(h->d_total); dfree(h->bbox_partial); dfree(h->d_uni);
+  dfree(h->d_status); dfree(h->d_counters); dfree(h->d_work); dfree(h->d_vmax2); dfree(h->srcf); dfree(h->softf);
+  Nodes& o = h->nd;
+  dfree(o.key); dfree(o.type); dfree(o.depth); dfree(o.pstart); dfree(o.pcount); dfree(o.parent);
+  dfree(o.first_child); dfree(o.count); dfree(o.mom); dfree(o.walk); dfree(o.quad); dfree(o.quadf);
+  dfree(o.fifo); dfree(o.nleaf_sub); dfree(o.nempty_sub); dfree(o.leaf_base); dfree(o.empty_base);
+  dfree(h->flags); dfree(h->buckets); dfree(h->list_count); dfree(h->list_off); dfree(h->list_node);
+  dfree(h->list_kind); dfree(h->dsum);
+  for (auto& e : h->ev)
+    if (e) cudaEventDestroy(e);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  delete h;
+  return PT_OK;
+}
+
+const char* pt_last_error(const pt_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int pt_set_stream(pt_handle* h, void* stream) {
+  if (!h) return PT_E_ARG;
+  h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+  return PT_OK;
+}
+
+int pt_set_theta(pt_handle* h, double theta) {
+  if (!h || !(theta > 0.0)) return PT_E_ARG;
+  h->cfg.theta = theta;
+  return PT_OK;
+}
+
+int pt_set_precision(pt_handle* h, int precision) {
+  if (!h || (precision != PT_FP64 && precision != PT_MIXED)) return PT_E_ARG;
+  h->cfg.precision = precision;
+  return PT_OK;
+}
+
+int pt_set_particles(pt_handle* h, int64_t n, const double* x, const double* y, const double* z, const double* vx,
+                     const double* vy, const double* vz, const double* m, const double* soft) {
+  if (!h) return PT_E_ARG;
+  cudaSetDevice(h->cfg.device);
+  const double* src[8] = {x, y, z, vx, vy, vz, m, soft};
+  CKR(set_particles_impl(h, n, src, cudaMemcpyHostToDevice));
+  CK(cudaStreamSynchronize(h->stream));
+  return PT_OK;
+}
+
+int pt_set_particles_device(pt_handle* h, int64_t n, const double* x, const double* y, const double* z,
+                            const double* vx, const double* vy, const double* vz, const double* m,
+                            const double* soft) {
+  if (!h) return PT_E_ARG;
+  cudaSetDevice(h->cfg.device);
+  const double* src[8] = {x, y, z, vx, vy, vz, m, soft};
+  return set_particles_impl(h, n, src, cudaMemcpyDeviceToDevice);
+}
+
+int64_t pt_num_particles(const pt_handle* h) { return h ? h->n : -1; }
+
+int pt_compute_forces(pt_handle* h) {
+  if (!h) return PT_E_ARG;
+  cudaSetDevice(h->cfg.device);
+  return forces(h, 0, INT64_MAX);
+}
+
+int pt_compute_forces_range(pt_handle* h, int64_t b0, int64_t b1) {
+  if (!h || b0 < 0 || b1 < b0) return PT_E_ARG;
+  cudaSetDevice(h->cfg.device);
+  return forces(h, b0, b1);
+}
+
+int pt_get_accel(pt_handle* h, double* ax, double* ay, double* az, double* pot, double* pot_full) {
+  if (!h) return PT_E_ARG;
+  if (!h->have_forces) return fail(h, PT_E_STATE, "no force pass yet");
+  if (h->n == 0) return PT_OK;
+  cudaSetDevice(h->cfg.device);
+  const double* src[5] = {h->p.ax, h->p.ay, h->p.az, h->p.pot, h->p.potf};
+  double* dst[5] = {ax, ay, az, pot, pot_full};
+  for (int i = 0; i < 5; i++) {
+    CKR(unpermute_f64(h, src[i], dst[i]));
+    if (dst[i]) CK(cudaStreamSynchronize(h->stream));
+  }
+  return PT_OK;
+}
+
+int pt_device_accel(pt_handle* h, const double** ax, const double** ay, const double** az, const int32_t** order) {
+  if (!h) return PT_E_ARG;
+  if (ax) *ax = h->p.ax;
+  if (ay) *ay = h->p.ay;
+  if (az) *az = h->p.az;
+  if (order) *order = h->p.order;
+  return PT_OK;
+}
+
+int pt_step(pt_handle* h, int nsteps) {
+  if (!h || nsteps < 0) return PT_E_ARG;
+  if (!h->p.x) return fail(h, PT_E_STATE, "no particles");
+  cudaSetDevice(h->cfg.device);
+  const int g = grid_for(h, h->n);
+  for (int s = 0; s < nsteps; s++) {
+    if (h->cfg.integrator == PT_KKD) {
+      CKR(forces(h, 0, INT64_MAX));
+      double dt;
+      CKR(timestep(h, &dt));
+      h->last_dt = dt;
+      launch_kick_perturb(h->p, h->n, dt, g, h->stream);
+      CK(cudaGetLastError());
+      h->have_forces = false;
+    } else {
+      if (!h->have_forces) CKR(forces(h, 0, INT64_MAX));
+      double dt;
+      CKR(timestep(h, &dt));
+      h->last_dt = dt;
+      launch_kick_half(h->p, h->n, dt, g, h->stream);
+      launch_drift(h->p, h->n, dt, g, h->stream);
+      CK(cudaGetLastError());
+      CKR(forces(h, 0, INT64_MAX));
+      launch_kick_half(h->p, h->n, dt, g, h->stream);
+      CK(cudaGetLastError());
+    }
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return PT_OK;
+}
+
+int pt_get_state(pt_handle* h, double* x, double* y, double* z, double* vx, double* vy, double* vz) {
+  if (!h) return PT_E_ARG;
+  if (h->n == 0) return PT_OK;
+  cudaSetDevice(h->cfg.device);
+  const double* src[6] = {h->p.x, h->p.y, h->p.z, h->p.vx, h->p.vy, h->p.vz};
+  double* dst[6] = {x, y, z, vx, vy, vz};
+  for (int i = 0; i < 6; i++) {
+    CKR(unpermute_f64(h, src[i], dst[i]));
+    if (dst[i]) CK(cudaStreamSynchronize(h->stream));
+  }
+  return PT_OK;
+}
+
+int pt_last_dt(const pt_handle* h, double* dt) {
+  if (!h || !dt) return PT_E_ARG;
+  *dt = h->last_dt;
+  return PT_OK;
+}
+
+int pt_get_keys(pt_handle* h, uint64_t* keys) {
+  if (!h || !keys) return PT_E_ARG;
+  if (!h->have_forces) return fail(h, PT_E_STATE, "no force pass yet");
+  if (h->n == 0) return PT_OK;
+  cudaSetDevice(h->cfg.device);
+  launch_scatter_u64(h->p.key, h->key_alt, h->p.order, h->n, grid_for(h, h->n), h->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(keys, h->key_alt, h->n * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return PT_OK;
+}
+
+int pt_get_universe(pt_handle* h, double* lo3, double* hi3) {
+  if (!h || !lo3 || !hi3) return PT_E_ARG;
+  double u[6];
+  CK(cudaMemcpyAsync(u, h->d_uni, sizeof(u), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int d = 0; d < 3; d++) {
+    lo3[d] = u[d];
+    hi3[d] = u[3 + d];
+  }
+  return PT_OK;
+}
+
+int pt_get_tree_size(pt_handle* h, int64_t* n_nodes, int64_t* n_buckets) {
+  if (!h) return PT_E_ARG;
+  if (n_nodes) *n_nodes = h->nnodes;
+  if (n_buckets) *n_buckets = h->nbuckets;
+  return PT_OK;
+}
+
+int pt_get_tree(pt_handle* h, uint64_t* keys, int32_t* ints4, double* dbls18) {
+  if (!h) return PT_E_ARG;
+  const int64_t nn = h->nnodes;
+  if (nn == 0) return PT_OK;
+  cudaStream_t st = h->stream;
+  std::vector<int32_t> type(nn), depth(nn), count(nn);
+  std::vector<Mom> mom(nn);
+  if (keys) CK(cudaMemcpyAsync(keys, h->nd.key, nn * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(type.data(), h->nd.type, nn * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(depth.data(), h->nd.depth, nn * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(count.data(), h->nd.count, nn * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(mom.data(), h->nd.mom, nn * sizeof(Mom), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  for (int64_t i = 0; i < nn; i++) {
+    if (ints4) {
+      ints4[4 * i + 0] = type[i];
+      ints4[4 * i + 1] = depth[i];
+      ints4[4 * i + 2] = count[i];
+      ints4[4 * i + 3] = (type[i] == kTypeInternal) ? 8 : 0;
+    }
+    if (dbls18) {
+      const Mom& q = mom[i];
+      double* d = dbls18 + 18 * i;
+      d[0] = q.mass; d[1] = q.cm[0]; d[2] = q.cm[1]; d[3] = q.cm[2]; d[4] = q.soft; d[5] = q.radius;
+      d[6] = q.xx; d[7] = q.xy; d[8] = q.xz; d[9] = q.yy; d[10] = q.yz; d[11] = q.zz;
+      d[12] = q.lo[0]; d[13] = q.lo[1]; d[14] = q.lo[2]; d[15] = q.hi[0]; d[16] = q.hi[1]; d[17] = q.hi[2];
+    }
+  }
+  return PT_OK;
+}
+
+int pt_get_bucket_keys(pt_handle* h, uint64_t* keys) {
+  if (!h || !keys) return PT_E_ARG;
+  const int64_t nb = h->nbuckets;
+  if (nb == 0) return PT_OK;
+  std::vector<int32_t> b(nb);
+  std::vector<uint64_t> nk(h->nnodes);
+  CK(cudaMemcpyAsync(b.data(), h->buckets, nb * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(nk.data(), h->nd.key, h->nnodes * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int64_t i = 0; i < nb; i++) keys[i] = nk[b[i]];
+  return PT_OK;
+}
+
+int pt_get_lists_size(pt_handle* h, int64_t* total) {
+  if (!h || !total) return PT_E_ARG;
+  if (!h->lists_valid) return fail(h, PT_E_STATE, "no interaction lists recorded (config.record_lists)");
+  *total = h->list_total;
+  return PT_OK;
+}
+
+int pt_get_lists(pt_handle* h, int64_t* offsets, uint64_t* keys, int32_t* kinds) {
+  if (!h) return PT_E_ARG;
+  if (!h->lists_valid) return fail(h, PT_E_STATE, "no interaction lists recorded (config.record_lists)");
+  const int64_t nb = h->list_nb - 1, tot = h->list_total;
+  std::vector<int64_t> off(nb + 1);
+  std::vector<int32_t> node(tot);
+  std::vector<int8_t> kind(tot);
+  std::vector<uint64_t> nk(h->nnodes);
+  cudaStream_t st = h->stream;
+  CK(cudaMemcpyAsync(off.data(), h->list_off, (nb + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  if (tot) {
+    CK(cudaMemcpyAsync(node.data(), h->list_node, tot * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(kind.data(), h->list_kind, tot * sizeof(int8_t), cudaMemcpyDeviceToHost, st));
+  }
+  CK(cudaMemcpyAsync(nk.data(), h->nd.key, h->nnodes * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (offsets)
+    for (int64_t i = 0; i <= nb; i++) offsets[i] = off[i];
+  for (int64_t i = 0; i < tot; i++) {
+    if (keys) keys[i] = nk[node[i]];
+    if (kinds) kinds[i] = kind[i];
+  }
+  return PT_OK;
+}
+
+int pt_get_counters(pt_handle* h, pt_counters* c) {
+  if (!h || !c) return PT_E_ARG;
+  *c = h->last;
+  return PT_OK;
+}
+
+int pt_direct_sum(pt_handle* h, int64_t nt, const int32_t* targets, double* ax, double* ay, double* az,
+                  double* pot) {
+  if (!h || nt < 0 || (nt > 0 && !targets)) return PT_E_ARG;
+  if (!h->p.x) return fail(h, PT_E_STATE, "no particles");
+  const int64_t n = h->n;
+  if (nt == 0 || n == 0) return PT_OK;
+  for (int64_t t = 0; t < nt; t++)
+    if (targets[t] < 0 || targets[t] >= n) return fail(h, PT_E_ARG, "target index out of range");
+  cudaSetDevice(h->cfg.device);
+  cudaStream_t st = h->stream;
+  const int tb = (int)((nt + 255) / 256);
+  int nsplit = std::max(1, std::min(256, (4 * h->sms + tb - 1) / tb));
+  if (n < 4096) nsplit = 1;
+  const int64_t need = 5 * n + 4 * nt * nsplit + nt;
+  if (need > h->dsum_cap) {
+    CKR(dalloc(h, &h->dsum, need));
+    h->dsum_cap = need;
+  }
+  // caller-order copies of x, y, z, m, soft
+  const double* src[5] = {h->p.x, h->p.y, h->p.z, h->p.m, h->p.soft};
+  for (int k = 0; k < 5; k++) launch_scatter_f64(src[k], h->dsum + k * n, h->p.order, n, grid_for(h, n), st);
+  int32_t* dt = reinterpret_cast<int32_t*>(h->dsum + 5 * n + 4 * nt * nsplit);
+  CK(cudaMemcpyAsync(dt, targets, nt * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  double* part = h->dsum + 5 * n;
+  launch_direct_sum(h->dsum, h->dsum + n, h->dsum + 2 * n, h->dsum + 3 * n, h->dsum + 4 * n, n, dt, nt, nsplit,
+                    part, st);
+  CK(cudaGetLastError());
+  std::vector<double> hp((size_t)4 * nt * nsplit);
+  CK(cudaMemcpyAsync(hp.data(), part, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  for (int64_t t = 0; t < nt; t++) {
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int sl = 0; sl < nsplit; sl++)
+      for (int k = 0; k < 4; k++) s[k] += hp[((size_t)sl * nt + t) * 4 + k];
+    if (ax) ax[t] = s[0];
+    if (ay) ay[t] = s[1];
+    if (az) az[t] = s[2];
+    if (pot) pot[t] = s[3];
+  }
+  return PT_OK;
+}
+
+}  // extern "C"

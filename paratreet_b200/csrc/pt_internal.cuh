@@ -1,0 +1,106 @@
+// pt_internal.cuh -- device data layout and kernel entry points shared by the
+// CUDA translation units of the B200 gravity path.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace pt {
+
+constexpr int kMaxDepth = 21;          // 63 key bits / 3 (src/common.h:29-31)
+constexpr int kTypeLeaf = 1;           // Node<Data>::Type numbering, src/Node.h:82-95
+constexpr int kTypeEmpty = 2;
+constexpr int kTypeInternal = 6;
+constexpr int kMinParticleNode = 6;    // examples/GravityVisitor.h:35
+
+// Device status word bits (written by kernels, read by the host after a pass).
+enum : unsigned {
+  kErrNonFinite = 1u << 0,
+  kErrStack = 1u << 1,
+  kErrBucketTooBig = 1u << 2,
+  kErrListOverflow = 1u << 3,
+  kErrCapacity = 1u << 4,
+};
+
+// Particle state, structure of arrays, FP64, in key-sorted order after a build.
+struct Particles {
+  double *x, *y, *z, *vx, *vy, *vz, *m, *soft;
+  int32_t* order;  // caller index of each sorted slot
+  uint64_t* key;
+  double *ax, *ay, *az, *pot, *potf;
+};
+
+// Per-node walk record: what one lane needs to classify one child.
+struct __align__(16) WalkRec {
+  double cm[3];      // MultipoleMoments::cm
+  double orsq;       // radius^2 * gravity_factor (GravityVisitor::open, :164)
+  int32_t first_child;  // first of 8 contiguous children, -1 for leaves
+  int32_t type;      // kTypeLeaf / kTypeEmpty / kTypeInternal
+  int32_t count;     // CentroidData::count
+  int32_t pstart;    // first particle (sorted order)
+  int32_t pcount;    // particles in the node's key range
+  int32_t pad[3];
+};
+static_assert(sizeof(WalkRec) == 64, "WalkRec is one 64-byte record");
+
+// Per-node P2C record (FP64): mass, soft and the 6 second moments.
+struct __align__(16) QuadRec {
+  double mass, soft, xx, xy, xz, yy, yz, zz;
+};
+static_assert(sizeof(QuadRec) == 64, "QuadRec is one 64-byte record");
+
+// Per-node P2C record for the mixed form (FP32): the same fields.
+struct __align__(16) QuadRecF {
+  float mass, soft, xx, xy, xz, yy, yz, zz;
+};
+
+// Full FP64 node moments (18 doubles), the layout pt_get_tree reports.
+struct Mom {
+  double mass, cm[3], soft, radius;
+  double xx, xy, xz, yy, yz, zz;
+  double lo[3], hi[3];
+};
+
+// Node arrays (breadth-first order: level by level, children of one parent
+// contiguous).
+struct Nodes {
+  uint64_t* key;
+  int32_t* type;
+  int32_t* depth;
+  int32_t* pstart;
+  int32_t* pcount;
+  int32_t* parent;
+  int32_t* first_child;
+  int32_t* count;       // CentroidData::count
+  Mom* mom;
+  WalkRec* walk;
+  QuadRec* quad;
+  QuadRecF* quadf;
+  uint64_t* fifo;       // upward-pass FIFO position key (depth-of-chain << 40 | rank)
+  int32_t* nleaf_sub;   // Leaf nodes in subtree
+  int32_t* nempty_sub;  // EmptyLeaf nodes in subtree
+  int32_t* leaf_base;   // DFS rank base of Leaf nodes in subtree
+  int32_t* empty_base;  // DFS rank base of EmptyLeaf nodes in subtree
+};
+
+struct TravParams {
+  Particles p;
+  const WalkRec* walk;
+  const QuadRec* quad;
+  const QuadRecF* quadf;
+  const float4* srcf;     // mixed: per-particle (x,y,z) relative to its leaf's cm, mass
+  const float* softf;     // mixed: per-particle softening (FP32)
+  const int32_t* buckets; // bucket b -> node index (DFS order)
+  int64_t b_begin, b_end;
+  double ox, oy, oz;      // GravityVisitor offset (periodic replicas; 0 otherwise)
+  int mode;               // 0 evaluate, 1 count lists only, 2 evaluate + record lists
+  int64_t* list_count;    // mode 1: entries per bucket
+  const int64_t* list_off;// mode 2: CSR offsets
+  int32_t* list_node;     // mode 2: node index per entry
+  int8_t* list_kind;      // mode 2: 0 P2P, 1 P2C
+  unsigned long long* counters;  // n_pp, n_pc, n_open
+  unsigned int* work;     // dynamic bucket counter
+  unsigned int* status;
+};
+
+}  // namespace pt

@@ -1,0 +1,63 @@
+// pt_launch.h -- host-side launchers of the kernels in k_*.cu.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "pt_internal.cuh"
+
+namespace pt {
+
+// k_keys.cu
+void launch_bbox(const double* x, const double* y, const double* z, int64_t n, double* partial, int nblocks,
+                 double* uni, unsigned* status, cudaStream_t st);
+void launch_keys(const double* x, const double* y, const double* z, int64_t n, const double* uni, uint64_t* key,
+                 uint32_t* idx, int grid, cudaStream_t st);
+void launch_vmax2(const double* vx, const double* vy, const double* vz, int64_t n, unsigned long long* out,
+                  int grid, cudaStream_t st);
+
+// k_sort.cu
+size_t scan_scratch_bytes(int64_t n);
+void scan_exclusive(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* scratch, uint32_t* total,
+                    cudaStream_t st);
+size_t sort_hist_elems(int64_t n);
+void radix_sort_pairs(uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, int64_t n, uint32_t* hist,
+                      uint32_t* scratch, uint32_t* total, cudaStream_t st);
+void gather_f64(const double* in, double* out, const uint32_t* idx, int64_t n, int grid, cudaStream_t st);
+void gather_i32(const int32_t* in, int32_t* out, const uint32_t* idx, int64_t n, int grid, cudaStream_t st);
+
+// k_build.cu
+void launch_init_root(Nodes nd, int64_t n, int bucket, cudaStream_t st);
+void launch_flag_internal(const int32_t* type, int64_t begin, int64_t count, uint32_t* flags, cudaStream_t st);
+void launch_build_children(Nodes nd, const uint64_t* keys, int64_t begin, int64_t count, const uint32_t* rank,
+                           int64_t next_begin, int bucket, cudaStream_t st);
+void launch_count_subtree(Nodes nd, int64_t begin, int64_t count, cudaStream_t st);
+void launch_base_topdown(Nodes nd, int64_t begin, int64_t count, cudaStream_t st);
+void launch_assign_buckets(Nodes nd, int64_t nnodes, int32_t* buckets, int nleaves, cudaStream_t st);
+
+// k_fp64.cu
+void launch_leaf_moments(Nodes nd, int64_t nnodes, Particles p, cudaStream_t st);
+void launch_upward_level(Nodes nd, int64_t begin, int64_t count, cudaStream_t st);
+void launch_finalize(Nodes nd, int64_t nnodes, double gfac, int want_f32, cudaStream_t st);
+void launch_traverse_f64(const TravParams& P, const Mom* mom, int grid, cudaStream_t st);
+void launch_kick_perturb(Particles p, int64_t n, double dt, int grid, cudaStream_t st);
+void launch_kick_half(Particles p, int64_t n, double dt, int grid, cudaStream_t st);
+void launch_drift(Particles p, int64_t n, double dt, int grid, cudaStream_t st);
+void launch_direct_sum(const double* x, const double* y, const double* z, const double* m, const double* soft,
+                       int64_t n, const int32_t* tgt, int64_t nt, int nsplit, double* part, cudaStream_t st);
+
+// k_mixed.cu
+void launch_prep_sources(const int32_t* buckets, int64_t nbuckets, const WalkRec* walk, Particles p, float4* srcf,
+                         float* softf, cudaStream_t st);
+void launch_traverse_mixed(const TravParams& P, const Mom* mom, int grid, cudaStream_t st);
+
+// k_util.cu
+void launch_scatter_f64(const double* in, double* out, const int32_t* order, int64_t n, int grid, cudaStream_t st);
+void launch_scatter_u64(const uint64_t* in, uint64_t* out, const int32_t* order, int64_t n, int grid,
+                        cudaStream_t st);
+void launch_iota_i32(int32_t* out, int64_t n, int grid, cudaStream_t st);
+void launch_inverse_perm(const int32_t* order, int32_t* inv, int64_t n, int grid, cudaStream_t st);
+void launch_map_index(const int32_t* inv, const int32_t* in, int32_t* out, int64_t n, cudaStream_t st);
+
+}  // namespace pt

@@ -1,0 +1,161 @@
+// pt_walk.cuh -- the warp-per-bucket tree walk shared by the FP64 and mixed
+// traversal kernels.
+//
+// Semantics: TransposedDownTraverser::recurse (src/Traverser.h:154-217) for
+// one target bucket is a pre-order depth-first walk from the root: a Leaf is
+// handed to GravityVisitor::leaf (P2P, the bucket itself included), an
+// Internal node is tested with GravityVisitor::open and either descended or
+// handed to GravityVisitor::node (P2C), an EmptyLeaf is skipped.  Per target
+// particle the interactions are applied in exactly that order.
+//
+// B200 mapping: one warp owns one bucket (lanes = target particles).  When a
+// node is opened, lanes 0..7 classify its 8 contiguous children in parallel
+// (64-byte WalkRec each, one coalesced 512-byte read); three ballots give
+// per-child P2P / P2C / open masks.  The terminal children before the first
+// opened child are handed to the evaluator in child order, the remaining
+// masks are pushed on a per-warp shared-memory frame stack, and the walk
+// descends.  Every decision is warp-uniform, so there is no divergence in the
+// walk itself.  The opening test uses __dadd_rn/__dmul_rn so it evaluates
+// identically (no FMA contraction) in every translation unit: the FP64 and
+// mixed forms see the same interaction lists.
+#pragma once
+
+#include "pt_internal.cuh"
+
+namespace pt {
+
+constexpr int kWalkStack = 32;
+constexpr unsigned kFull = 0xffffffffu;
+
+struct WalkFrame {
+  int32_t c0;     // index of child 0
+  uint32_t bits;  // P2P mask (0-7) | P2C mask (8-15) << 8 | open mask (16-23) << 16
+};
+
+// Space::intersect(box, centre, rsq) of the reference's utility submodule
+// (stand-in convention: squared gap accumulated x, y, z; intersect iff <=).
+// Used by GravityVisitor::open (:180) and ::openSoftening (:127).
+__device__ __forceinline__ bool box_sphere_exact(const double lo[3], const double hi[3], double cx,
+                                                 double cy, double cz, double rsq) {
+  double dsq = 0.0, d;
+  if ((d = __dadd_rn(lo[0], -cx)) > 0) dsq = __dadd_rn(dsq, __dmul_rn(d, d));
+  else if ((d = __dadd_rn(cx, -hi[0])) > 0) dsq = __dadd_rn(dsq, __dmul_rn(d, d));
+  if ((d = __dadd_rn(lo[1], -cy)) > 0) dsq = __dadd_rn(dsq, __dmul_rn(d, d));
+  else if ((d = __dadd_rn(cy, -hi[1])) > 0) dsq = __dadd_rn(dsq, __dmul_rn(d, d));
+  if ((d = __dadd_rn(lo[2], -cz)) > 0) dsq = __dadd_rn(dsq, __dmul_rn(d, d));
+  else if ((d = __dadd_rn(cz, -hi[2])) > 0) dsq = __dadd_rn(dsq, __dmul_rn(d, d));
+  return dsq <= rsq;
+}
+
+// GravityVisitor::openSoftening (:122-128): the softening spheres overlap, or
+// the target bucket's box meets the source sphere of radius 2*soft.
+__device__ __forceinline__ bool open_softening_exact(double scx, double scy, double scz, double ssoft,
+                                                     double tcx, double tcy, double tcz, double tsoft,
+                                                     const double lo[3], const double hi[3]) {
+  double r1 = __dmul_rn(2.0, ssoft), r2 = __dmul_rn(2.0, tsoft);
+  double dx = __dadd_rn(scx, -tcx), dy = __dadd_rn(scy, -tcy), dz = __dadd_rn(scz, -tcz);
+  double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+  double rs = __dadd_rn(r1, r2);
+  if (d2 <= __dmul_rn(rs, rs)) return true;
+  return box_sphere_exact(lo, hi, scx, scy, scz, __dmul_rn(r1, r1));
+}
+
+struct BucketGeom {
+  double lo[3], hi[3];  // target bucket's particle bbox (CentroidData::box)
+  double cm[3];         // target bucket's centre of mass
+  double soft;          // target bucket's mass-weighted softening
+};
+
+// Classify up to 8 nodes [c0, c0+nvalid) against the bucket; returns frame bits.
+__device__ __forceinline__ uint32_t classify_children(const WalkRec* __restrict__ walk, int c0, int nvalid,
+                                                      const BucketGeom& g, double ox, double oy, double oz,
+                                                      int lane, unsigned long long& n_open) {
+  int code = 0;
+  if (lane < nvalid) {
+    const WalkRec w = walk[c0 + lane];
+    if (w.type == kTypeLeaf) {
+      code = 1;
+    } else if (w.type == kTypeInternal) {
+      bool open = (w.count <= kMinParticleNode) ||
+                  box_sphere_exact(g.lo, g.hi, __dadd_rn(w.cm[0], ox), __dadd_rn(w.cm[1], oy),
+                                   __dadd_rn(w.cm[2], oz), w.orsq);
+      code = open ? 3 : 2;
+    }
+  }
+  uint32_t pp = __ballot_sync(kFull, code == 1);
+  uint32_t pc = __ballot_sync(kFull, code == 2);
+  uint32_t op = __ballot_sync(kFull, code == 3);
+  n_open += (unsigned long long)__popc(pc | op);
+  return (pp & 0xffu) | ((pc & 0xffu) << 8) | ((op & 0xffu) << 16);
+}
+
+// Walk the tree for one bucket; ev.p2p(node) / ev.p2c(node) are called in
+// the reference's per-bucket order.  Returns false on stack overflow.
+template <class Eval>
+__device__ __forceinline__ bool walk_bucket(const WalkRec* __restrict__ walk, const BucketGeom& g, double ox,
+                                            double oy, double oz, WalkFrame* stack, int lane, Eval& ev,
+                                            unsigned long long& n_open) {
+  int c0 = 0;  // the root, tested as a one-child frame
+  uint32_t bits = classify_children(walk, 0, 1, g, ox, oy, oz, lane, n_open);
+  int sp = 0;
+  while (true) {
+    if (bits == 0) {
+      if (sp == 0) break;
+      --sp;
+      WalkFrame f = stack[sp];
+      c0 = f.c0;
+      bits = f.bits;
+      continue;
+    }
+    uint32_t pp = bits & 0xffu, pc = (bits >> 8) & 0xffu, op = (bits >> 16) & 0xffu;
+    int fo = op ? (__ffs(op) - 1) : 8;
+    uint32_t low = (1u << fo) - 1u;
+    uint32_t run = (pp | pc) & low;
+    while (run) {
+      int k = __ffs(run) - 1;
+      run &= run - 1u;
+      if ((pp >> k) & 1u) ev.p2p(c0 + k);
+      else ev.p2c(c0 + k);
+    }
+    pp &= ~low;
+    pc &= ~low;
+    if (fo < 8) {
+      op &= ~(1u << fo);
+      uint32_t rem = pp | (pc << 8) | (op << 16);
+      if (rem) {
+        if (sp >= kWalkStack) return false;
+        __syncwarp();
+        if (lane == 0) stack[sp] = WalkFrame{c0, rem};
+        __syncwarp();
+        ++sp;
+      }
+      int child = c0 + fo;
+      int nc0 = walk[child].first_child;
+      c0 = nc0;
+      bits = classify_children(walk, nc0, 8, g, ox, oy, oz, lane, n_open);
+    } else {
+      bits = 0;
+    }
+  }
+  return true;
+}
+
+// Evaluator that only records / counts the interaction list of a bucket.
+struct ListRecorder {
+  int lane;
+  int mode;  // 1 count, 2 record
+  int64_t n;
+  int64_t base;
+  int32_t* node_out;
+  int8_t* kind_out;
+  __device__ void p2p(int node) {
+    if (mode == 2 && lane == 0) { node_out[base + n] = node; kind_out[base + n] = 0; }
+    ++n;
+  }
+  __device__ void p2c(int node) {
+    if (mode == 2 && lane == 0) { node_out[base + n] = node; kind_out[base + n] = 1; }
+    ++n;
+  }
+};
+
+}  // namespace pt

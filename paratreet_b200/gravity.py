@@ -1,0 +1,234 @@
+"""Host-side mirror of ParaTreeT's Gravity example interface, over the C ABI.
+
+The reference's user-facing pieces for this path and what stands in for them:
+
+* ``GravityVisitor(offset, theta)`` (examples/GravityVisitor.h:9-31): same
+  traits (CallSelfLeaf, ForceEvenDepth, TargetMustBeLeaf), same opening
+  factors; here it configures the device traversal instead of being called
+  per node.
+* ``Configuration`` fields used by the path (src/Configuration.h:131-153:
+  max_particles_per_leaf ``-l``, num_iterations ``-i``) and ExMain's
+  ``theta`` / ``max_timestep`` ``-j`` (examples/Main.C:55-57, :64-78).
+* ``Partition<Data>::startDown<Visitor>(Visitor)`` (src/Partition.h:129-134):
+  ``GravitySimulation.start_down(visitor)`` runs one force pass.
+* ``Driver<Data>::run`` (src/Driver.h:183-288): ``GravitySimulation.run``.
+* ``outputParticleAccelerations`` (src/Paratreet.h:242-249):
+  ``GravitySimulation.accelerations``.
+
+All compute runs in libpt_gravity.so on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+
+PRECISIONS = {"fp64": L.PT_FP64, "mixed": L.PT_MIXED}
+INTEGRATORS = {"kkd": L.PT_KKD, "kdk": L.PT_KDK}
+
+
+class GravityVisitor:
+    """Parameters of examples/GravityVisitor.h for the device traversal."""
+
+    CallSelfLeaf = True
+    ForceEvenDepth = True
+    TargetMustBeLeaf = True
+    opening_geometry_factor_squared = 4.0 / 3.0
+
+    def __init__(self, offset=(0.0, 0.0, 0.0), theta: float = 0.7):
+        if not theta > 0:
+            raise ValueError("theta must be positive")
+        self.offset = tuple(float(v) for v in offset)
+        self.theta = float(theta)
+        self.gravity_factor = self.opening_geometry_factor_squared / (self.theta * self.theta)
+        self.monopole_gravity_factor = np.sqrt(self.opening_geometry_factor_squared) / self.theta ** 4
+
+
+@dataclass
+class Configuration:
+    max_particles_per_leaf: int = 16
+    theta: float = 0.7
+    max_timestep: float = 1e-5
+    precision: str = "fp64"
+    integrator: str = "kkd"
+    device: int = 0
+    record_lists: bool = False
+
+
+@dataclass
+class TreeDump:
+    keys: np.ndarray
+    types: np.ndarray
+    depth: np.ndarray
+    count: np.ndarray
+    moments: np.ndarray  # (n, 18): mass, cm3, soft, radius, xx, xy, xz, yy, yz, zz, lo3, hi3
+
+
+@dataclass
+class InteractionLists:
+    bucket_keys: np.ndarray
+    offsets: np.ndarray
+    keys: np.ndarray
+    kinds: np.ndarray  # 0 leaf() P2P, 1 node() P2C
+
+
+_FIELDS = ("x", "y", "z", "vx", "vy", "vz", "m", "soft")
+
+
+class GravitySimulation:
+    """One simulation's device state (one handle of the C ABI)."""
+
+    def __init__(self, conf: Configuration | None = None, **kw):
+        conf = conf or Configuration(**kw)
+        self.conf = conf
+        self._lib = L.load()
+        cfg = L.PtConfig()
+        self._check(self._lib.pt_config_default(C.byref(cfg)))
+        cfg.theta = conf.theta
+        cfg.bucket = conf.max_particles_per_leaf
+        cfg.precision = PRECISIONS[conf.precision]
+        cfg.integrator = INTEGRATORS[conf.integrator]
+        cfg.dt_max = conf.max_timestep
+        cfg.device = conf.device
+        cfg.record_lists = 1 if conf.record_lists else 0
+        h = C.c_void_p()
+        rc = self._lib.pt_create(C.byref(cfg), C.byref(h))
+        if rc != L.PT_OK:
+            raise L.PtError(rc, "pt_create failed (CUDA device or configuration)")
+        self._h = h
+        self.n = 0
+
+    # -- plumbing -----------------------------------------------------------
+    def _check(self, rc: int):
+        if rc != L.PT_OK:
+            msg = self._lib.pt_last_error(getattr(self, "_h", None)) if hasattr(self, "_h") else b""
+            raise L.PtError(rc, (msg or b"").decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.pt_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_stream(self, stream_ptr: int | None):
+        self._check(self._lib.pt_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
+
+    def set_theta(self, theta: float):
+        self._check(self._lib.pt_set_theta(self._h, theta))
+        self.conf.theta = theta
+
+    def set_precision(self, precision: str):
+        self._check(self._lib.pt_set_precision(self._h, PRECISIONS[precision]))
+        self.conf.precision = precision
+
+    # -- particles ----------------------------------------------------------
+    def set_particles(self, p: dict):
+        arrs = [np.ascontiguousarray(p[k], dtype=np.float64) for k in _FIELDS]
+        n = arrs[0].size
+        self._keep = arrs
+        self._check(self._lib.pt_set_particles(self._h, n, *[L.ptr(a) for a in arrs]))
+        self.n = n
+
+    def set_particles_device(self, n: int, ptrs):
+        """ptrs: 8 device pointers (x, y, z, vx, vy, vz, m, soft), FP64."""
+        self._check(self._lib.pt_set_particles_device(self._h, n, *[C.c_void_p(int(q)) for q in ptrs]))
+        self.n = n
+
+    # -- force pass ---------------------------------------------------------
+    def start_down(self, visitor: GravityVisitor | None = None, buckets: tuple[int, int] | None = None):
+        """Partition::startDown<GravityVisitor>: one force evaluation."""
+        if visitor is not None:
+            if any(visitor.offset):
+                raise NotImplementedError("periodic replica offsets are not supported yet")
+            if visitor.theta != self.conf.theta:
+                self.set_theta(visitor.theta)
+        if buckets is None:
+            self._check(self._lib.pt_compute_forces(self._h))
+        else:
+            self._check(self._lib.pt_compute_forces_range(self._h, int(buckets[0]), int(buckets[1])))
+
+    compute_forces = start_down
+
+    def accelerations(self, out=None):
+        n = self.n
+        out = out or {k: np.empty(n) for k in ("ax", "ay", "az", "pot", "pot_full")}
+        self._check(self._lib.pt_get_accel(self._h, *[L.ptr(out.get(k)) for k in ("ax", "ay", "az", "pot", "pot_full")]))
+        return out
+
+    def run(self, num_iterations: int):
+        """Driver::run: num_iterations of forces, kick, perturb."""
+        self._check(self._lib.pt_step(self._h, int(num_iterations)))
+
+    def state(self):
+        out = {k: np.empty(self.n) for k in ("x", "y", "z", "vx", "vy", "vz")}
+        self._check(self._lib.pt_get_state(self._h, *[L.ptr(out[k]) for k in ("x", "y", "z", "vx", "vy", "vz")]))
+        return out
+
+    def last_dt(self) -> float:
+        v = C.c_double()
+        self._check(self._lib.pt_last_dt(self._h, C.byref(v)))
+        return v.value
+
+    # -- inspection ---------------------------------------------------------
+    def keys(self):
+        k = np.empty(self.n, np.uint64)
+        self._check(self._lib.pt_get_keys(self._h, L.ptr(k)))
+        return k
+
+    def universe(self):
+        lo, hi = np.empty(3), np.empty(3)
+        self._check(self._lib.pt_get_universe(self._h, L.ptr(lo), L.ptr(hi)))
+        return lo, hi
+
+    def tree(self) -> TreeDump:
+        nn, nb = C.c_int64(), C.c_int64()
+        self._check(self._lib.pt_get_tree_size(self._h, C.byref(nn), C.byref(nb)))
+        n = nn.value
+        k = np.empty(n, np.uint64)
+        ints = np.empty(4 * n, np.int32)
+        d = np.empty(18 * n)
+        self._check(self._lib.pt_get_tree(self._h, L.ptr(k), L.ptr(ints), L.ptr(d)))
+        ints = ints.reshape(n, 4)
+        return TreeDump(k, ints[:, 0].copy(), ints[:, 1].copy(), ints[:, 2].copy(), d.reshape(n, 18))
+
+    def bucket_keys(self):
+        nn, nb = C.c_int64(), C.c_int64()
+        self._check(self._lib.pt_get_tree_size(self._h, C.byref(nn), C.byref(nb)))
+        k = np.empty(nb.value, np.uint64)
+        self._check(self._lib.pt_get_bucket_keys(self._h, L.ptr(k)))
+        return k
+
+    def lists(self) -> InteractionLists:
+        bk = self.bucket_keys()
+        tot = C.c_int64()
+        self._check(self._lib.pt_get_lists_size(self._h, C.byref(tot)))
+        off = np.empty(bk.size + 1, np.int64)
+        keys = np.empty(max(tot.value, 1), np.uint64)
+        kinds = np.empty(max(tot.value, 1), np.int32)
+        self._check(self._lib.pt_get_lists(self._h, L.ptr(off), L.ptr(keys), L.ptr(kinds)))
+        return InteractionLists(bk, off, keys[: tot.value], kinds[: tot.value])
+
+    def counters(self) -> dict:
+        c = L.PtCounters()
+        self._check(self._lib.pt_get_counters(self._h, C.byref(c)))
+        return {f: getattr(c, f) for f, _ in L.PtCounters._fields_ if f != "reserved"}
+
+    def direct_sum(self, targets):
+        t = np.ascontiguousarray(targets, dtype=np.int32)
+        out = [np.empty(t.size) for _ in range(4)]
+        self._check(self._lib.pt_direct_sum(self._h, t.size, L.ptr(t), *[L.ptr(o) for o in out]))
+        return out

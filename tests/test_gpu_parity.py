@@ -1,0 +1,248 @@
+"""GPU parity tests: the CUDA path through the C ABI against the CPU oracle
+(and the reference-sources golden digests).
+
+FP64 form: bit-exact keys, tree topology, moments, interaction lists,
+accelerations, potentials and kick/perturb state.  Mixed form: same lists,
+forces within 1e-5 rms relative of the FP64 form (FP32 interactions).
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from paratreet_b200 import ics
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+CASES = sorted(f[4:-5] for f in os.listdir(GOLD) if f.startswith("ref_") and f.endswith(".json"))
+
+
+def sim(**kw):
+    from paratreet_b200.gravity import GravitySimulation
+    return GravitySimulation(**kw)
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def rel_err(a, b):
+    num = np.sqrt((a[0] - b[0]) ** 2 + (a[1] - b[1]) ** 2 + (a[2] - b[2]) ** 2)
+    den = np.sqrt(b[0] ** 2 + b[1] ** 2 + b[2] ** 2)
+    return num / np.where(den > 0, den, 1.0)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fp64_matches_reference_golden(name):
+    with open(os.path.join(GOLD, f"ref_{name}.json")) as f:
+        g = json.load(f)
+    p = getattr(ics, g["generator"])(**g["kwargs"])
+    with sim(max_particles_per_leaf=g["bucket"], theta=g["theta"], max_timestep=g["dt_max"],
+             record_lists=True) as s:
+        s.set_particles(p)
+        s.start_down()
+        h = g["sha256"]
+        assert sha(s.keys()) == h["keys"]
+        t = O.sort_tree(s.tree())
+        assert t.keys.size == g["n_nodes"]
+        assert sha(t.keys) == h["node_keys"]
+        assert sha(t.types.astype(np.int32)) == h["node_types"]
+        assert sha(t.count.astype(np.int32)) == h["node_counts"]
+        assert sha(t.moments) == h["node_moments"]
+        L = s.lists()
+        assert sha(L.bucket_keys) == h["bucket_keys"]
+        assert sha(L.offsets.astype(np.int64)) == h["list_offsets"]
+        assert sha(L.keys) == h["list_keys"]
+        assert sha(L.kinds.astype(np.int32)) == h["list_kinds"]
+        a = s.accelerations()
+        for k in ("ax", "ay", "az", "pot"):
+            assert sha(a[k]) == h[k], k
+        c = s.counters()
+        assert (c["n_pp"], c["n_pc"]) == (g["n_pp"], g["n_pc"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fp64_steps_match_reference_golden(name):
+    with open(os.path.join(GOLD, f"ref_{name}.json")) as f:
+        g = json.load(f)
+    p = getattr(ics, g["generator"])(**g["kwargs"])
+    with sim(max_particles_per_leaf=g["bucket"], theta=g["theta"], max_timestep=g["dt_max"]) as s:
+        s.set_particles(p)
+        s.run(g["steps"])
+        st = s.state()
+        for k in ("x", "y", "z", "vx", "vy", "vz"):
+            assert sha(st[k]) == g["after_steps"]["sha256"][k], k
+        assert s.last_dt() == g["after_steps"]["last_dt"]
+
+
+@pytest.mark.parametrize("gen,n,bucket,theta", [
+    ("plummer", 20000, 16, 0.7), ("mixture", 50000, 16, 0.7), ("plummer", 30000, 32, 0.5),
+    ("hernquist", 20000, 32, 1.0), ("plummer", 5000, 4, 0.7), ("mixture", 20000, 1, 0.7),
+])
+def test_fp64_bit_exact_vs_oracle(gen, n, bucket, theta):
+    p = getattr(ics, gen)(n)
+    ref = O.PortSim(p, bucket=bucket, theta=theta, dt_max=0.01, threads=8)
+    ref.forces(record_lists=True)
+    with sim(max_particles_per_leaf=bucket, theta=theta, max_timestep=0.01, record_lists=True) as s:
+        s.set_particles(p)
+        s.start_down()
+        assert np.array_equal(s.keys(), ref.keys())
+        lo, hi = s.universe()
+        rlo, rhi = ref.universe()
+        assert np.array_equal(lo, rlo) and np.array_equal(hi, rhi)
+        tg, tr = O.sort_tree(s.tree()), O.sort_tree(ref.tree())
+        assert np.array_equal(tg.keys, tr.keys)
+        assert np.array_equal(tg.types, tr.types)
+        assert np.array_equal(tg.count, tr.count)
+        assert np.array_equal(tg.moments, tr.moments)
+        Lg, Lr = s.lists(), ref.lists()
+        assert np.array_equal(Lg.bucket_keys, Lr.bucket_keys)
+        assert np.array_equal(Lg.offsets, Lr.offsets)
+        assert np.array_equal(Lg.keys, Lr.keys)
+        assert np.array_equal(Lg.kinds, Lr.kinds)
+        a = s.accelerations()
+        rax, ray, raz, rpot, rpotf = ref.acc()
+        assert np.array_equal(a["ax"], rax)
+        assert np.array_equal(a["ay"], ray)
+        assert np.array_equal(a["az"], raz)
+        assert np.array_equal(a["pot"], rpot)
+        assert np.array_equal(a["pot_full"], rpotf)
+
+
+def test_fp64_mixture_1m_ten_steps():
+    """The 2^20 mixture workload: 10 kick/perturb steps at dt=1e-4."""
+    p = ics.mixture(1 << 20, seed=7, soft=1e-4)
+    ref = O.PortSim(p, bucket=16, theta=0.7, dt_max=1e-4, threads=os.cpu_count() or 8)
+    ref.run(10)
+    with sim(max_particles_per_leaf=16, theta=0.7, max_timestep=1e-4) as s:
+        s.set_particles(p)
+        s.run(10)
+        st = s.state()
+        rs = ref.state()
+        for k, r in zip(("x", "y", "z", "vx", "vy", "vz"), rs):
+            assert np.array_equal(st[k], r), k
+        a = s.accelerations()
+        rax, ray, raz, rpot, _ = ref.acc()
+        assert np.array_equal(a["ax"], rax) and np.array_equal(a["pot"], rpot)
+
+
+@pytest.mark.parametrize("gen,n,bucket", [("plummer", 20000, 16), ("mixture", 50000, 32), ("hernquist", 20000, 32)])
+def test_mixed_matches_fp64(gen, n, bucket):
+    p = getattr(ics, gen)(n)
+    with sim(max_particles_per_leaf=bucket, record_lists=True) as s64:
+        s64.set_particles(p)
+        s64.start_down()
+        a64 = s64.accelerations()
+        L64 = s64.lists()
+    with sim(max_particles_per_leaf=bucket, precision="mixed", record_lists=True) as sm:
+        sm.set_particles(p)
+        sm.start_down()
+        am = sm.accelerations()
+        Lm = sm.lists()
+    assert np.array_equal(L64.keys, Lm.keys) and np.array_equal(L64.offsets, Lm.offsets)
+    e = rel_err((am["ax"], am["ay"], am["az"]), (a64["ax"], a64["ay"], a64["az"]))
+    assert np.sqrt(np.mean(e ** 2)) < 1e-5
+    assert np.max(e) < 1e-3
+    pe = np.abs(am["pot_full"] - a64["pot_full"]) / np.abs(a64["pot_full"])
+    assert np.sqrt(np.mean(pe ** 2)) < 1e-5
+
+
+def test_direct_sum_matches_oracle():
+    p = ics.plummer(6000, seed=9, soft=0.01)
+    tgt = np.arange(0, 6000, 7, dtype=np.int32)
+    rax, ray, raz, rpot = O.direct_sum(p, tgt, threads=8)
+    with sim() as s:
+        s.set_particles(p)
+        ax, ay, az, pot = s.direct_sum(tgt)
+    assert np.array_equal(ax, rax) and np.array_equal(pot, rpot)
+
+
+def test_direct_sum_split_known_answer():
+    """GPU direct sum (source-split) vs the reference's direct.acc."""
+    z = np.load(os.path.join(GOLD, "lambs_kat.npz"))
+    pos = z["pos"].astype(np.float64)
+    n = pos.shape[0]
+    p = {"x": pos[:, 0].copy(), "y": pos[:, 1].copy(), "z": pos[:, 2].copy(), "vx": np.zeros(n),
+         "vy": np.zeros(n), "vz": np.zeros(n), "m": z["mass"].astype(np.float64),
+         "soft": z["eps"].astype(np.float64)}
+    with sim() as s:
+        s.set_particles(p)
+        ax, ay, az, _ = s.direct_sum(z["targets"])
+    e = rel_err((ax, ay, az), tuple(z["acc"].T))
+    assert e.max() <= 1e-6 and np.sqrt(np.mean(e ** 2)) <= 1e-7
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 3, 16, 17, 33])
+def test_tiny_inputs(n):
+    p = ics.plummer(max(n, 1))
+    if n == 0:
+        p = {k: v[:0] for k, v in p.items()}
+    ref = O.PortSim(p, bucket=16)
+    ref.forces()
+    with sim(max_particles_per_leaf=16) as s:
+        s.set_particles(p)
+        s.start_down()
+        if n:
+            a = s.accelerations()
+            rax = ref.acc()[0]
+            assert np.array_equal(a["ax"], rax)
+
+
+def test_duplicate_positions_depth_limit():
+    p = ics.plummer(300)
+    for k in ("x", "y", "z"):
+        p[k][:40] = p[k][0]
+    ref = O.PortSim(p, bucket=16)
+    ref.forces()
+    with sim(max_particles_per_leaf=16) as s:
+        s.set_particles(p)
+        s.start_down()
+        a = s.accelerations()
+        assert np.array_equal(a["ax"], ref.acc()[0])
+        assert s.tree().depth.max() == 21
+
+
+def test_nonfinite_input_is_reported():
+    from paratreet_b200._lib import PtError
+    p = ics.plummer(1000)
+    p["y"][17] = np.nan
+    with sim() as s:
+        s.set_particles(p)
+        with pytest.raises(PtError) as e:
+            s.start_down()
+        assert e.value.code == -6
+        # the handle stays usable
+        s.set_particles(ics.plummer(1000))
+        s.start_down()
+
+
+def test_bucket_ranges_partition_the_pass():
+    p = ics.plummer(30000, seed=4)
+    with sim(max_particles_per_leaf=16) as s:
+        s.set_particles(p)
+        s.start_down()
+        full = s.accelerations()
+        nb = s.counters()["n_buckets"]
+        parts = []
+        for b0, b1 in ((0, nb // 3), (nb // 3, nb)):
+            s.start_down(buckets=(b0, b1))
+            parts.append(s.accelerations())
+    ax = parts[0]["ax"] + parts[1]["ax"]
+    assert np.array_equal(ax, full["ax"])
+
+
+def test_zero_mass_particles():
+    p = ics.plummer(5000, seed=11)
+    p["m"][::3] = 0.0
+    ref = O.PortSim(p, bucket=8)
+    ref.forces(record_lists=True)
+    with sim(max_particles_per_leaf=8, record_lists=True) as s:
+        s.set_particles(p)
+        s.start_down()
+        tg, tr = O.sort_tree(s.tree()), O.sort_tree(ref.tree())
+        assert np.array_equal(tg.moments, tr.moments)
+        assert np.array_equal(s.accelerations()["ax"], ref.acc()[0])
