@@ -53,12 +53,18 @@ __device__ __forceinline__ int first_ge(const uint64_t* __restrict__ keys, int l
 
 __global__ void __launch_bounds__(256) build_children(Nodes nd, const uint64_t* __restrict__ keys, int64_t begin,
                                                       int64_t count, const uint32_t* __restrict__ rank,
-                                                      int64_t next_begin, int bucket) {
+                                                      int64_t next_begin, int bucket, int64_t cap,
+                                                      unsigned* status) {
   int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= count) return;
   int64_t i = begin + t;
   if (nd.type[i] != kTypeInternal) return;
   int64_t c0 = next_begin + 8 * (int64_t)rank[t];
+  if (c0 < next_begin || c0 + 8 > cap) {  // never expected: the host sized the level
+    atomicOr(status, kErrCapacity);
+    nd.type[i] = kTypeLeaf;
+    return;
+  }
   nd.first_child[i] = (int32_t)c0;
   int depth = nd.depth[i] + 1;
   uint64_t ck = nd.key[i] << 3;
@@ -136,8 +142,9 @@ void launch_flag_internal(const int32_t* type, int64_t begin, int64_t count, uin
 }
 
 void launch_build_children(Nodes nd, const uint64_t* keys, int64_t begin, int64_t count, const uint32_t* rank,
-                           int64_t next_begin, int bucket, cudaStream_t st) {
-  if (count > 0) build_children<<<blocks_for(count), 256, 0, st>>>(nd, keys, begin, count, rank, next_begin, bucket);
+                           int64_t next_begin, int bucket, int64_t cap, unsigned* status, cudaStream_t st) {
+  if (count > 0)
+    build_children<<<blocks_for(count), 256, 0, st>>>(nd, keys, begin, count, rank, next_begin, bucket, cap, status);
 }
 
 void launch_count_subtree(Nodes nd, int64_t begin, int64_t count, cudaStream_t st) {

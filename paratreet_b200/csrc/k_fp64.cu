@@ -35,6 +35,8 @@ __device__ __forceinline__ void mom_clear(Mom& q) {
   q.xx = q.xy = q.xz = q.yy = q.yz = q.zz = 0.0;
   q.lo[0] = q.lo[1] = q.lo[2] = DBL_MAX;
   q.hi[0] = q.hi[1] = q.hi[2] = -DBL_MAX;
+  q.reach = 0.0;
+  q.soft_max = 0.0;
 }
 
 // MultipoleMoments::operator+=(Particle), examples/MultipoleMoments.h:274-353.
@@ -145,6 +147,16 @@ __global__ void __launch_bounds__(256) leaf_moments(Nodes nd, int64_t nnodes, Pa
     } else {
       q.radius = 1.0;
     }
+    // not part of the reference's data: reach and max softening of the leaf,
+    // used only to select the mixed form's unsoftened fast path
+    double r2max = 0.0, smax = 0.0;
+    for (int j = s0; j < s0 + sn; j++) {
+      double dx = p.x[j] - q.cm[0], dy = p.y[j] - q.cm[1], dz = p.z[j] - q.cm[2];
+      r2max = fmax(r2max, dx * dx + dy * dy + dz * dz);
+      smax = fmax(smax, p.soft[j]);
+    }
+    q.reach = sqrt(r2max);
+    q.soft_max = smax;
   }
   nd.mom[i] = q;
   nd.count[i] = cnt;
@@ -191,13 +203,19 @@ __global__ void __launch_bounds__(256) finalize_records(Nodes nd, int64_t nnodes
   const Mom q = nd.mom[i];
   WalkRec w;
   w.cm[0] = q.cm[0]; w.cm[1] = q.cm[1]; w.cm[2] = q.cm[2];
-  w.orsq = q.radius * q.radius * gfac;  // GravityVisitor::open, :164
-  w.first_child = nd.first_child[i];
   w.type = nd.type[i];
+  if (w.type == kTypeLeaf) {
+    w.reach = q.reach;
+    w.soft_max = q.soft_max;
+  } else {
+    w.orsq = q.radius * q.radius * gfac;  // GravityVisitor::open, :164
+    w.soft = q.soft;
+  }
+  w.first_child = nd.first_child[i];
   w.count = nd.count[i];
   w.pstart = nd.pstart[i];
   w.pcount = nd.pcount[i];
-  w.pad[0] = w.pad[1] = w.pad[2] = 0;
+  w.pad = 0;
   nd.walk[i] = w;
   QuadRec r;
   r.mass = q.mass; r.soft = q.soft;
@@ -278,8 +296,9 @@ struct F64Eval {
     }
   }
 
-  // GravityVisitor::node, examples/GravityVisitor.h:184-224 (non-HEXADECAPOLE)
-  __device__ void p2c(int node) {
+  // GravityVisitor::node, examples/GravityVisitor.h:184-224 (non-HEXADECAPOLE);
+  // mono = openSoftening held (decided in the walk), i.e. addGravity (:130-139)
+  __device__ void p2c(int node, bool mono) {
     const WalkRec w = walk[node];
     const QuadRec q = quad[node];
     n_pc += (unsigned long long)nt;
@@ -289,7 +308,7 @@ struct F64Eval {
     }
     if (w.count == 0) return;
     const double cx = w.cm[0] + ox, cy = w.cm[1] + oy, cz = w.cm[2] + oz;
-    if (open_softening_exact(cx, cy, cz, q.soft, g->cm[0], g->cm[1], g->cm[2], g->soft, g->lo, g->hi)) {
+    if (mono) {
       if (lane < nt) {  // addGravity, :130-139
         double dx = cx - xi, dy = cy - yi, dz = cz - zi;
         double rsq = dx * dx + dy * dy + dz * dz;
@@ -328,14 +347,6 @@ struct F64Eval {
   }
 };
 
-__device__ __forceinline__ void load_bucket_geom(const Mom* mom, int node, BucketGeom& g) {
-  const Mom& q = mom[node];
-  g.lo[0] = q.lo[0]; g.lo[1] = q.lo[1]; g.lo[2] = q.lo[2];
-  g.hi[0] = q.hi[0]; g.hi[1] = q.hi[1]; g.hi[2] = q.hi[2];
-  g.cm[0] = q.cm[0]; g.cm[1] = q.cm[1]; g.cm[2] = q.cm[2];
-  g.soft = q.soft;
-}
-
 __global__ void __launch_bounds__(kTravWarps * 32) traverse_f64(TravParams P, const Mom* __restrict__ mom) {
   __shared__ WalkFrame stacks[kTravWarps][kWalkStack];
   __shared__ double stage[kTravWarps][5 * 32];
@@ -348,6 +359,10 @@ __global__ void __launch_bounds__(kTravWarps * 32) traverse_f64(TravParams P, co
     int64_t b = P.b_begin + (int64_t)bi;
     if (b >= P.b_end) break;
     const int tnode = P.buckets[b];
+    if (tnode < 0 || tnode >= P.nnodes) {
+      if (lane == 0) atomicOr(P.status, kErrCapacity);
+      continue;
+    }
     BucketGeom g;
     load_bucket_geom(mom, tnode, g);
     const int t0 = P.walk[tnode].pstart, nt = P.walk[tnode].pcount;
@@ -357,7 +372,8 @@ __global__ void __launch_bounds__(kTravWarps * 32) traverse_f64(TravParams P, co
     }
     if (P.mode == 1) {  // count the interaction list only
       ListRecorder rec{lane, 1, 0, 0, nullptr, nullptr};
-      if (!walk_bucket(P.walk, g, P.ox, P.oy, P.oz, stacks[wid], lane, rec, c_open) && lane == 0)
+      if (!walk_bucket(P.walk, P.nnodes, g, P.ox, P.oy, P.oz, stacks[wid], lane, rec, c_open, P.status) &&
+          lane == 0)
         atomicOr(P.status, kErrStack);
       if (lane == 0) P.list_count[b - P.b_begin] = rec.n;
       continue;
@@ -385,7 +401,7 @@ __global__ void __launch_bounds__(kTravWarps * 32) traverse_f64(TravParams P, co
     ev.lbase = ev.record ? P.list_off[b - P.b_begin] : 0;
     ev.lnode = P.list_node;
     ev.lkind = P.list_kind;
-    if (!walk_bucket(P.walk, g, P.ox, P.oy, P.oz, stacks[wid], lane, ev, c_open) && lane == 0)
+    if (!walk_bucket(P.walk, P.nnodes, g, P.ox, P.oy, P.oz, stacks[wid], lane, ev, c_open, P.status) && lane == 0)
       atomicOr(P.status, kErrStack);
     if (lane < nt) {
       int i = t0 + lane;

@@ -1,24 +1,42 @@
 // k_mixed.cu -- K7 mixed-precision traversal.
 //
-// Same walk (and so the same interaction lists) as the FP64 form: the tree,
-// the opening tests and the softening-overlap tests stay FP64.  Every P2P
-// (GravityVisitor::leaf, examples/GravityVisitor.h:144-160) and quadrupole
-// P2C (GravityVisitor::node, :184-224) interaction is evaluated in FP32 on
-// offsets relative to the target bucket's centre of mass:
+// Same interactions as the FP64 form: the tree, the opening tests
+// (GravityVisitor::open) and the softening-overlap tests
+// (GravityVisitor::openSoftening) are evaluated in FP64 with the same
+// expressions, so every bucket meets exactly the reference's set of leaf()
+// and node() interactions.  Every P2P (GravityVisitor::leaf,
+// examples/GravityVisitor.h:144-160) and P2C (GravityVisitor::node, :184-224)
+// interaction is evaluated in FP32 on offsets relative to the target bucket's
+// centre of mass:
 //   targets   (x_i - cm_bucket)                      FP64 subtract -> FP32
-//   sources   (x_j - cm_leaf) [FP32, per step] + (cm_leaf - cm_bucket)
+//   sources   (x_j - cm_leaf) [FP32, once per pass] + (cm_leaf - cm_bucket)
 //             [FP64 subtract per (leaf, bucket) -> FP32]
-//   P2C       (x_i - cm_bucket) - (cm_node - cm_bucket)[FP64 -> FP32]
-// Each source leaf's <=32-term partial is summed in plain FP32 and then
-// Kahan-added into the per-target FP32 accumulators; P2C terms are
-// Kahan-added directly.  Acceleration and the full potential (P2P spline,
-// P2C quadrupole, monopole) are produced.
+//   P2C       (x_i - cm_bucket) - (cm_node - cm_bucket) [FP64 -> FP32]
+// Terms are summed in plain FP32 within one flush of the interaction buffers
+// (<= 64 entries) and the flush partials are Kahan-added into per-target FP32
+// accumulators.  Acceleration and the full potential are produced.
+//
+// B200 mapping (one warp per bucket, dynamic bucket queue in DFS order):
+//  walk     lanes 8e..8e+7 classify the 8 children of up to 4 opened nodes at
+//           once (32 FP64 tests per step); leaves and accepted nodes are
+//           appended to shared-memory buffers with their FP32 offsets, opened
+//           nodes to a per-warp LIFO.  The interaction order is not the
+//           reference's (only the FP64 form keeps it).
+//  eval     the bucket's n_t targets are replicated over G = 32 / T lane
+//           groups (T = next power of two >= n_t); group g takes every G-th
+//           source / node of a 32-entry chunk staged in shared memory, so a
+//           10-particle bucket keeps all 32 lanes busy.  Leaves whose nearest
+//           particle pair is provably beyond the softening length take a
+//           branch-free Newtonian loop (rsqrt on the SFU).
+//  reduce   per-lane Kahan sums -> FP64, butterfly over the G groups.
 #include "pt_internal.cuh"
 #include "pt_walk.cuh"
 
 namespace pt {
 
 constexpr int kMixWarps = 4;
+constexpr int kMixStack = 640;  // opened nodes pending; <= 21 levels x 28 + 32
+constexpr int kMixBuf = 64;     // buffered terminals per kind (a step adds <= 32)
 
 struct Kahan {
   float s, c;
@@ -28,6 +46,23 @@ struct Kahan {
     c = (t - s) - y;
     s = t;
   }
+  __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+};
+
+// Per-warp shared memory.
+struct MixWarp {
+  BucketGeom geom;          // the target bucket (FP64), read by the walk
+  int32_t stack[kMixStack];
+  float4 cbuf[kMixBuf];     // P2C: offset xyz, node index bits (mono: node | 1<<31)
+  float4 fbuf[kMixBuf];     // P2P far leaves: offset xyz, node index bits
+  float4 nbuf[kMixBuf];     // P2P near leaves: offset xyz, node index bits
+  int32_t pre[kMixBuf + 1]; // prefix of leaf sizes during a P2P flush
+  int32_t ps0[kMixBuf];     // first particle of each buffered leaf
+  float4 src[32];           // staged sources: x, y, z (rel. bucket), m
+  float ssoft[32];
+  float4 qa[32];            // staged P2C: offset xyz, mass
+  float4 qb[32];            // xx, xy, xz, yy
+  float4 qc[32];            // yz, zz, soft (< 0: monopole), trace/2
 };
 
 // SPLINE in FP32 (r2 > 0): force term b, potential term a.
@@ -43,7 +78,8 @@ __device__ __forceinline__ void spline_f32(float r2, float rinv, float twoh, flo
     } else {
       a = -1.0f / 15.0f * rinv +
           dih * (8.0f / 5.0f - 4.0f / 3.0f * u2 + u2 * u - 3.0f / 10.0f * u2 * u2 + 1.0f / 30.0f * u2 * u2 * u);
-      b = -1.0f / 15.0f * rinv * rinv * rinv + dih * dih * dih * (8.0f / 3.0f - 3.0f * u + 6.0f / 5.0f * u2 - 1.0f / 6.0f * u2 * u);
+      b = -1.0f / 15.0f * rinv * rinv * rinv +
+          dih * dih * dih * (8.0f / 3.0f - 3.0f * u + 6.0f / 5.0f * u2 - 1.0f / 6.0f * u2 * u);
     }
   } else {
     a = rinv;
@@ -51,7 +87,7 @@ __device__ __forceinline__ void spline_f32(float r2, float rinv, float twoh, flo
   }
 }
 
-// SPLINEQ in FP32, as the reference evaluates it (examples/GravityVisitor.h:37-80).
+// SPLINEQ in FP32 with the reference's grouping (examples/GravityVisitor.h:37-80).
 __device__ __forceinline__ void splineq_f32(float dir, float r2, float twoh, float& a, float& b, float& c, float& d) {
   if (r2 < twoh * twoh) {
     float dih = 2.0f / twoh;
@@ -65,7 +101,8 @@ __device__ __forceinline__ void splineq_f32(float dir, float r2, float twoh, flo
       d = 3.0f / 2.0f * d6 * dir;
     } else {
       float r3 = dir * dir * dir;
-      a = -1.0f / 15.0f * dir + dih * (8.0f / 5.0f) - 4.0f / 3.0f * u2 + u2 * u - 3.0f / 10.0f * u2 * u2 + 1.0f / 30.0f * u2 * u2 * u;
+      a = -1.0f / 15.0f * dir + dih * (8.0f / 5.0f) - 4.0f / 3.0f * u2 + u2 * u - 3.0f / 10.0f * u2 * u2 +
+          1.0f / 30.0f * u2 * u2 * u;
       b = -1.0f / 15.0f * r3 + d3 * 8.0f / 3.0f - 3.0f * u + 6.0f / 5.0f * u2 - 1.0f / 6.0f * u2 * u;
       c = -1.0f / 5.0f * r3 * dir * dir + 3.0f * d4 * dir + d5 * (-12.0f) / 5.0f + 1.0f / 2.0f * u;
       d = -r3 * r3 * dir + 3.0f * d4 * r3 - 1.0f / 2.0f * d6 * dir;
@@ -78,165 +115,335 @@ __device__ __forceinline__ void splineq_f32(float dir, float r2, float twoh, flo
   }
 }
 
-struct MixedEval {
-  const WalkRec* walk;
-  const QuadRec* quad;
-  const QuadRecF* quadf;
-  const float4* srcf;
-  const float* softf;
-  float4* stage;   // this warp's 32 staged sources (x, y, z rel. bucket; m)
-  float* stages;   // their softening
-  int lane, nt;
-  float tx, ty, tz, ts;  // target rel. bucket cm
+__device__ __forceinline__ float4 pack_entry(float ox, float oy, float oz, int node, bool flag) {
+  return make_float4(ox, oy, oz, __int_as_float(node | (flag ? (int)0x80000000 : 0)));
+}
+__device__ __forceinline__ int entry_node(float4 e) { return __float_as_int(e.w) & 0x7fffffff; }
+__device__ __forceinline__ bool entry_flag(float4 e) { return (__float_as_int(e.w) & 0x80000000) != 0; }
+
+struct MixCtx {
+  int lane, t, grp, G, nt;
+  float tx, ty, tz, ts;                 // this lane's target (rel. bucket cm)
+  float pax, pay, paz, ppf;             // flush partials
   Kahan ax, ay, az, pf;
-  const BucketGeom* g;
-  double ox, oy, oz;
   unsigned long long n_pp, n_pc;
 
-  __device__ void p2p(int node) {
-    const WalkRec w = walk[node];
-    const int s0 = w.pstart, sn = w.pcount;
-    const float offx = (float)((w.cm[0] + ox) - g->cm[0]);
-    const float offy = (float)((w.cm[1] + oy) - g->cm[1]);
-    const float offz = (float)((w.cm[2] + oz) - g->cm[2]);
-    float pax = 0.f, pay = 0.f, paz = 0.f, ppf = 0.f;
-    for (int base = 0; base < sn; base += 32) {
-      int cnt = min(32, sn - base);
-      __syncwarp();
-      if (lane < cnt) {
-        float4 s = srcf[s0 + base + lane];
-        stage[lane] = make_float4(s.x + offx, s.y + offy, s.z + offz, s.w);
-        stages[lane] = softf[s0 + base + lane];
-      }
-      __syncwarp();
-      if (lane < nt) {
-        for (int j = 0; j < cnt; j++) {
-          float4 s = stage[j];
-          float dx = s.x - tx, dy = s.y - ty, dz = s.z - tz;
-          float r2 = dx * dx + dy * dy + dz * dz;
-          if (r2 > 0.f) {
-            float rinv = rsqrtf(r2);
-            float a, b;
-            spline_f32(r2, rinv, stages[j] + ts, a, b);
-            float bm = b * s.w;
-            pax += dx * bm;
-            pay += dy * bm;
-            paz += dz * bm;
-            ppf -= s.w * a;
-          }
-        }
-      }
-    }
-    ax.add(pax);
-    ay.add(pay);
-    az.add(paz);
-    pf.add(ppf);
-    n_pp += (unsigned long long)sn * (unsigned long long)nt;
-  }
-
-  __device__ void p2c(int node) {
-    const WalkRec w = walk[node];
-    n_pc += (unsigned long long)nt;
-    if (w.count == 0) return;
-    const double cx = w.cm[0] + ox, cy = w.cm[1] + oy, cz = w.cm[2] + oz;
-    const float offx = (float)(cx - g->cm[0]), offy = (float)(cy - g->cm[1]), offz = (float)(cz - g->cm[2]);
-    const QuadRecF q = quadf[node];
-    const double qsoft = quad[node].soft;
-    if (open_softening_exact(cx, cy, cz, qsoft, g->cm[0], g->cm[1], g->cm[2], g->soft, g->lo, g->hi)) {
-      if (lane < nt) {
-        float dx = offx - tx, dy = offy - ty, dz = offz - tz;
-        float r2 = dx * dx + dy * dy + dz * dz;
-        if (r2 > 0.f) {
-          float rinv = rsqrtf(r2);
-          float f = q.mass * rinv * rinv * rinv;
-          ax.add(dx * f);
-          ay.add(dy * f);
-          az.add(dz * f);
-          pf.add(-q.mass * rinv);
-        }
-      }
-      return;
-    }
-    if (lane < nt) {
-      float rx = tx - offx, ry = ty - offy, rz = tz - offz;
-      float r2 = rx * rx + ry * ry + rz * rz;
-      float dir = rsqrtf(r2);
-      float a, b, c, d;
-      splineq_f32(dir, r2, q.soft + ts, a, b, c, d);
-      float qx = q.xx * rx + q.xy * ry + q.xz * rz;
-      float qy = q.xy * rx + q.yy * ry + q.yz * rz;
-      float qz = q.xz * rx + q.yz * ry + q.zz * rz;
-      float qir = 0.5f * (qx * rx + qy * ry + qz * rz);
-      float tr = 0.5f * (q.xx + q.yy + q.zz);
-      float qir3 = b * q.mass + d * qir - c * tr;
-      pf.add(-q.mass * a - c * qir + b * tr);
-      ax.add(-qir3 * rx + c * qx);
-      ay.add(-qir3 * ry + c * qy);
-      az.add(-qir3 * rz + c * qz);
-    }
+  __device__ __forceinline__ void commit() {
+    ax.add(pax); ay.add(pay); az.add(paz); pf.add(ppf);
+    pax = pay = paz = ppf = 0.f;
   }
 };
 
-__global__ void __launch_bounds__(kMixWarps * 32) traverse_mixed(TravParams P, const Mom* __restrict__ mom) {
-  __shared__ WalkFrame stacks[kMixWarps][kWalkStack];
-  __shared__ float4 stage[kMixWarps][32];
-  __shared__ float stages[kMixWarps][32];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+// Evaluate all buffered P2P leaves of one kind (far: no pair can be softened).
+template <bool kFar>
+__device__ __forceinline__ void flush_p2p(MixWarp& w, const float4* __restrict__ buf, int nleaves,
+                                          const WalkRec* __restrict__ walk, const float4* __restrict__ srcf,
+                                          const float* __restrict__ softf, MixCtx& x) {
+  // prefix of leaf sizes (nleaves <= 64: two entries per lane)
+  int s0a = 0, s0b = 0, na = 0, nb = 0;
+  if (x.lane < nleaves) { const WalkRec& r = walk[entry_node(buf[x.lane])]; s0a = r.pstart; na = r.pcount; }
+  if (x.lane + 32 < nleaves) { const WalkRec& r = walk[entry_node(buf[x.lane + 32])]; s0b = r.pstart; nb = r.pcount; }
+  int inca = na, incb = nb;
+  for (int o = 1; o < 32; o <<= 1) {
+    int ya = __shfl_up_sync(kFull, inca, o), yb = __shfl_up_sync(kFull, incb, o);
+    if (x.lane >= o) { inca += ya; incb += yb; }
+  }
+  const int tota = __shfl_sync(kFull, inca, 31);
+  const int total = tota + __shfl_sync(kFull, incb, 31);
+  __syncwarp();
+  if (x.lane < nleaves) { w.pre[x.lane] = inca - na; w.ps0[x.lane] = s0a; }
+  if (x.lane + 32 < nleaves) { w.pre[x.lane + 32] = tota + incb - nb; w.ps0[x.lane + 32] = s0b; }
+  if (x.lane == 0) w.pre[nleaves] = total;
+  __syncwarp();
+  for (int cs = 0; cs < total; cs += 32) {
+    const int q = cs + x.lane;
+    if (q < total) {
+      int lo = 0, hi = nleaves - 1;  // last leaf with pre <= q
+      while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (w.pre[mid] <= q) lo = mid;
+        else hi = mid - 1;
+      }
+      const float4 e = buf[lo];
+      const int j = w.ps0[lo] + (q - w.pre[lo]);
+      const float4 s = srcf[j];
+      w.src[x.lane] = make_float4(s.x + e.x, s.y + e.y, s.z + e.z, s.w);
+      if (!kFar) w.ssoft[x.lane] = softf[j];
+    }
+    __syncwarp();
+    const int cnt = min(32, total - cs);
+    if (kFar && x.t < x.nt) {
+      float bx = 0.f, by = 0.f, bz = 0.f, bp = 0.f;  // second chain
+      int jj = x.grp;
+      for (; jj + x.G < cnt; jj += 2 * x.G) {
+        const float4 s = w.src[jj];
+        const float4 u = w.src[jj + x.G];
+        const float dx = s.x - x.tx, dy = s.y - x.ty, dz = s.z - x.tz;
+        const float ex = u.x - x.tx, ey = u.y - x.ty, ez = u.z - x.tz;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        const float q2 = ex * ex + ey * ey + ez * ez;
+        const float rinv = rsqrtf(r2), qinv = rsqrtf(q2);
+        const float mr = s.w * rinv, mq = u.w * qinv;
+        const float mr3 = mr * rinv * rinv, mq3 = mq * qinv * qinv;
+        x.pax += dx * mr3;
+        x.pay += dy * mr3;
+        x.paz += dz * mr3;
+        x.ppf -= mr;
+        bx += ex * mq3;
+        by += ey * mq3;
+        bz += ez * mq3;
+        bp -= mq;
+      }
+      if (jj < cnt) {
+        const float4 s = w.src[jj];
+        const float dx = s.x - x.tx, dy = s.y - x.ty, dz = s.z - x.tz;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        const float rinv = rsqrtf(r2);
+        const float mr = s.w * rinv;
+        const float mr3 = mr * rinv * rinv;
+        x.pax += dx * mr3;
+        x.pay += dy * mr3;
+        x.paz += dz * mr3;
+        x.ppf -= mr;
+      }
+      x.pax += bx;
+      x.pay += by;
+      x.paz += bz;
+      x.ppf += bp;
+    } else if (!kFar && x.t < x.nt) {
+      for (int jj = x.grp; jj < cnt; jj += x.G) {
+        const float4 s = w.src[jj];
+        const float dx = s.x - x.tx, dy = s.y - x.ty, dz = s.z - x.tz;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 > 0.f) {
+          const float rinv = rsqrtf(r2);
+          float a, b;
+          spline_f32(r2, rinv, w.ssoft[jj] + x.ts, a, b);
+          const float bm = b * s.w;
+          x.pax += dx * bm;
+          x.pay += dy * bm;
+          x.paz += dz * bm;
+          x.ppf -= s.w * a;
+        }
+      }
+    }
+    __syncwarp();
+  }
+  x.n_pp += (unsigned long long)total * (unsigned long long)x.nt;
+  x.commit();
+}
+
+// One P2C term (quadrupole, examples/GravityVisitor.h:207-220, in FP32).
+// A monopole entry (openSoftening held, addGravity :130-139) is staged with
+// zero second moments and a NaN softening, which takes the unsoftened branch
+// and reduces the expression to -M r / r^3 and -M / r.
+__device__ __forceinline__ void p2c_term(const float4 A, const float4 B, const float4 Cc, float tx, float ty,
+                                         float tz, float ts, float& ax, float& ay, float& az, float& pf) {
+  const float rx = tx - A.x, ry = ty - A.y, rz = tz - A.z;
+  const float r2 = rx * rx + ry * ry + rz * rz;
+  const float dir = rsqrtf(r2);
+  float a, b, c, d;
+  const float twoh = Cc.z + ts;
+  if (r2 < twoh * twoh) {
+    splineq_f32(dir, r2, twoh, a, b, c, d);
+  } else {
+    a = dir;
+    const float d2 = dir * dir;
+    b = a * d2;
+    c = 3.0f * b * d2;
+    d = 5.0f * c * d2;
+  }
+  const float qx = B.x * rx + B.y * ry + B.z * rz;
+  const float qy = B.y * rx + B.w * ry + Cc.x * rz;
+  const float qz = B.z * rx + Cc.x * ry + Cc.y * rz;
+  const float qir = 0.5f * (qx * rx + qy * ry + qz * rz);
+  const float qir3 = b * A.w + d * qir - c * Cc.w;
+  pf += -A.w * a - c * qir + b * Cc.w;
+  ax += -qir3 * rx + c * qx;
+  ay += -qir3 * ry + c * qy;
+  az += -qir3 * rz + c * qz;
+}
+
+// Evaluate all buffered P2C nodes.
+__device__ __forceinline__ void flush_p2c(MixWarp& w, int nent, const QuadRecF* __restrict__ quadf, MixCtx& x) {
+  const float qnan = __int_as_float(0x7fc00000);
+  for (int cs = 0; cs < nent; cs += 32) {
+    const int q = cs + x.lane;
+    if (q < nent) {
+      const float4 e = w.cbuf[q];
+      const QuadRecF r = quadf[entry_node(e)];
+      w.qa[x.lane] = make_float4(e.x, e.y, e.z, r.mass);
+      if (entry_flag(e)) {
+        w.qb[x.lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+        w.qc[x.lane] = make_float4(0.f, 0.f, qnan, 0.f);
+      } else {
+        w.qb[x.lane] = make_float4(r.xx, r.xy, r.xz, r.yy);
+        w.qc[x.lane] = make_float4(r.yz, r.zz, r.soft, 0.5f * (r.xx + r.yy + r.zz));
+      }
+    }
+    __syncwarp();
+    const int cnt = min(32, nent - cs);
+    if (x.t < x.nt) {
+      float bx = 0.f, by = 0.f, bz = 0.f, bp = 0.f;  // second chain
+      int ee = x.grp;
+      for (; ee + x.G < cnt; ee += 2 * x.G) {
+        p2c_term(w.qa[ee], w.qb[ee], w.qc[ee], x.tx, x.ty, x.tz, x.ts, x.pax, x.pay, x.paz, x.ppf);
+        const int e2 = ee + x.G;
+        p2c_term(w.qa[e2], w.qb[e2], w.qc[e2], x.tx, x.ty, x.tz, x.ts, bx, by, bz, bp);
+      }
+      if (ee < cnt) p2c_term(w.qa[ee], w.qb[ee], w.qc[ee], x.tx, x.ty, x.tz, x.ts, x.pax, x.pay, x.paz, x.ppf);
+      x.pax += bx;
+      x.pay += by;
+      x.paz += bz;
+      x.ppf += bp;
+    }
+    __syncwarp();
+  }
+  x.n_pc += (unsigned long long)nent * (unsigned long long)x.nt;
+  x.commit();
+}
+
+// Append this lane's entry (if flag) to a warp buffer in lane order.
+__device__ __forceinline__ int append(float4* buf, int n, bool flag, float4 v, int lane) {
+  const unsigned m = __ballot_sync(kFull, flag);
+  if (flag) buf[n + __popc(m & ((1u << lane) - 1u))] = v;
+  return n + __popc(m);
+}
+
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kMixWarps * 32, kMinBlocks) traverse_mixed(TravParams P, const Mom* __restrict__ mom) {
+  __shared__ MixWarp warps[kMixWarps];
+  MixWarp& w = warps[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
   unsigned long long c_pp = 0, c_pc = 0, c_open = 0;
   while (true) {
     unsigned bi = 0;
     if (lane == 0) bi = atomicAdd(P.work, 1u);
     bi = __shfl_sync(kFull, bi, 0);
-    int64_t b = P.b_begin + (int64_t)bi;
+    const int64_t b = P.b_begin + (int64_t)bi;
     if (b >= P.b_end) break;
     const int tnode = P.buckets[b];
-    BucketGeom g;
-    {
-      const Mom& q = mom[tnode];
-      for (int d = 0; d < 3; d++) { g.lo[d] = q.lo[d]; g.hi[d] = q.hi[d]; g.cm[d] = q.cm[d]; }
-      g.soft = q.soft;
+    if (tnode < 0 || tnode >= P.nnodes) {
+      if (lane == 0) atomicOr(P.status, kErrCapacity);
+      continue;
     }
+    __syncwarp();
+    if (lane == 0) load_bucket_geom(mom, tnode, w.geom);
+    __syncwarp();
+    const BucketGeom& g = w.geom;
     const int t0 = P.walk[tnode].pstart, nt = P.walk[tnode].pcount;
-    if (nt > 32) {
+    if (nt > 32 || nt < 1) {
       if (lane == 0) atomicOr(P.status, kErrBucketTooBig);
       continue;
     }
-    MixedEval ev;
-    ev.walk = P.walk;
-    ev.quad = P.quad;
-    ev.quadf = P.quadf;
-    ev.srcf = P.srcf;
-    ev.softf = P.softf;
-    ev.stage = stage[wid];
-    ev.stages = stages[wid];
-    ev.lane = lane;
-    ev.nt = nt;
-    ev.tx = ev.ty = ev.tz = ev.ts = 0.f;
-    if (lane < nt) {
-      ev.tx = (float)(P.p.x[t0 + lane] - g.cm[0]);
-      ev.ty = (float)(P.p.y[t0 + lane] - g.cm[1]);
-      ev.tz = (float)(P.p.z[t0 + lane] - g.cm[2]);
-      ev.ts = (float)P.p.soft[t0 + lane];
+    MixCtx x;
+    x.lane = lane;
+    x.nt = nt;
+    int lt = 0;
+    while ((1 << lt) < nt) lt++;
+    x.t = lane & ((1 << lt) - 1);
+    x.grp = lane >> lt;
+    x.G = 32 >> lt;
+    x.tx = x.ty = x.tz = x.ts = 0.f;
+    if (x.t < nt) {
+      const int i = t0 + x.t;
+      x.tx = (float)(P.p.x[i] - g.cm[0]);
+      x.ty = (float)(P.p.y[i] - g.cm[1]);
+      x.tz = (float)(P.p.z[i] - g.cm[2]);
+      x.ts = (float)P.p.soft[i];
     }
-    ev.ax = Kahan{0.f, 0.f};
-    ev.ay = Kahan{0.f, 0.f};
-    ev.az = Kahan{0.f, 0.f};
-    ev.pf = Kahan{0.f, 0.f};
-    ev.g = &g;
-    ev.ox = P.ox; ev.oy = P.oy; ev.oz = P.oz;
-    ev.n_pp = 0; ev.n_pc = 0;
-    if (!walk_bucket(P.walk, g, P.ox, P.oy, P.oz, stacks[wid], lane, ev, c_open) && lane == 0)
-      atomicOr(P.status, kErrStack);
-    if (lane < nt) {
-      int i = t0 + lane;
-      P.p.ax[i] = (double)ev.ax.s + (double)(-ev.ax.c);
-      P.p.ay[i] = (double)ev.ay.s + (double)(-ev.ay.c);
-      P.p.az[i] = (double)ev.az.s + (double)(-ev.az.c);
+    x.pax = x.pay = x.paz = x.ppf = 0.f;
+    x.ax = x.ay = x.az = x.pf = Kahan{0.f, 0.f};
+    x.n_pp = x.n_pc = 0;
+
+    int sp = 0, nc = 0, nfar = 0, nnear = 0;
+    int nexp = 1;          // nodes expanded this step
+    int e0 = -1;           // first expanded node; -1 = the root itself
+    bool ok = true;
+    int ex[4] = {-1, -1, -1, -1};
+    while (true) {
+      // lanes 8e..8e+7: children of expanded node e (the root step tests node 0)
+      const int e = lane >> 3, c = lane & 7;
+      int node = -1;
+      if (e0 < 0) {
+        if (lane == 0) node = 0;
+      } else if (e < nexp) {
+        node = P.walk[ex[e]].first_child + c;
+      }
+      int cls = kClsNone;
+      WalkRec r;
+      if (node >= 0) {
+        if (node >= P.nnodes) {
+          atomicOr(P.status, kErrCapacity);
+        } else {
+          r = P.walk[node];
+          cls = classify_node(r, g, P.ox, P.oy, P.oz);
+        }
+      }
+      c_open += (unsigned long long)__popc(__ballot_sync(kFull, node >= 0 && node < P.nnodes &&
+                                                                    r.type == kTypeInternal));
+      float ofx = 0.f, ofy = 0.f, ofz = 0.f;
+      bool far = false;
+      if (cls == kClsP2P || cls == kClsQuad || cls == kClsMono) {
+        const double cx = r.cm[0] + P.ox, cy = r.cm[1] + P.oy, cz = r.cm[2] + P.oz;
+        ofx = (float)(cx - g.cm[0]);
+        ofy = (float)(cy - g.cm[1]);
+        ofz = (float)(cz - g.cm[2]);
+        if (cls == kClsP2P) {
+          const double reach = r.reach + r.soft_max + g.soft_max;
+          far = box_dist2(g.lo, g.hi, cx, cy, cz) > reach * reach;
+        }
+      }
+      const float4 ent = pack_entry(ofx, ofy, ofz, node, cls == kClsMono);
+      nc = append(w.cbuf, nc, cls == kClsQuad || cls == kClsMono, ent, lane);
+      nfar = append(w.fbuf, nfar, cls == kClsP2P && far, ent, lane);
+      nnear = append(w.nbuf, nnear, cls == kClsP2P && !far, ent, lane);
+      {
+        const bool op = (cls == kClsOpen);
+        const unsigned m = __ballot_sync(kFull, op);
+        if (sp + __popc(m) > kMixStack) {
+          ok = false;
+          break;
+        }
+        if (op) w.stack[sp + __popc(m & ((1u << lane) - 1u))] = node;
+        sp += __popc(m);
+      }
+      __syncwarp();
+      if (nc >= 32) { flush_p2c(w, nc, P.quadf, x); nc = 0; }
+      if (nfar >= 32) { flush_p2p<true>(w, w.fbuf, nfar, P.walk, P.srcf, P.softf, x); nfar = 0; }
+      if (nnear >= 32) { flush_p2p<false>(w, w.nbuf, nnear, P.walk, P.srcf, P.softf, x); nnear = 0; }
+      if (sp == 0) break;
+      nexp = sp < 4 ? sp : 4;
+      sp -= nexp;
+      for (int k = 0; k < 4; k++) ex[k] = (k < nexp) ? w.stack[sp + k] : -1;
+      e0 = ex[0];
+      __syncwarp();
+    }
+    if (!ok) {
+      if (lane == 0) atomicOr(P.status, kErrStack);
+      continue;
+    }
+    if (nc) flush_p2c(w, nc, P.quadf, x);
+    if (nfar) flush_p2p<true>(w, w.fbuf, nfar, P.walk, P.srcf, P.softf, x);
+    if (nnear) flush_p2p<false>(w, w.nbuf, nnear, P.walk, P.srcf, P.softf, x);
+
+    double vx = x.ax.value(), vy = x.ay.value(), vz = x.az.value(), vp = x.pf.value();
+    for (int o = 1 << lt; o < 32; o <<= 1) {
+      vx += __shfl_xor_sync(kFull, vx, o);
+      vy += __shfl_xor_sync(kFull, vy, o);
+      vz += __shfl_xor_sync(kFull, vz, o);
+      vp += __shfl_xor_sync(kFull, vp, o);
+    }
+    if (x.grp == 0 && x.t < nt) {
+      const int i = t0 + x.t;
+      P.p.ax[i] = vx;
+      P.p.ay[i] = vy;
+      P.p.az[i] = vz;
       P.p.pot[i] = 0.0;
-      P.p.potf[i] = (double)ev.pf.s + (double)(-ev.pf.c);
+      P.p.potf[i] = vp;
     }
-    c_pp += ev.n_pp;
-    c_pc += ev.n_pc;
+    c_pp += x.n_pp;
+    c_pc += x.n_pc;
   }
   if (lane == 0) {
     atomicAdd(&P.counters[0], c_pp);
@@ -268,8 +475,10 @@ void launch_prep_sources(const int32_t* buckets, int64_t nbuckets, const WalkRec
   prep_sources<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(buckets, nbuckets, walk, p, srcf, softf);
 }
 
-void launch_traverse_mixed(const TravParams& P, const Mom* mom, int grid, cudaStream_t st) {
-  traverse_mixed<<<grid, kMixWarps * 32, 0, st>>>(P, mom);
+// variant: 0 = at most 6 CTAs/SM (80 registers), 1 = 5 CTAs/SM (no spills)
+void launch_traverse_mixed(const TravParams& P, const Mom* mom, int grid, int variant, cudaStream_t st) {
+  if (variant == 1) traverse_mixed<5><<<grid, kMixWarps * 32, 0, st>>>(P, mom);
+  else traverse_mixed<6><<<grid, kMixWarps * 32, 0, st>>>(P, mom);
 }
 
 }  // namespace pt

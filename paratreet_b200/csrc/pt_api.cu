@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -68,8 +69,10 @@ struct pt_handle {
   cudaEvent_t ev[7]{};
   pt_counters last{};
   double last_dt = 0.0;
-  bool have_forces = false;
+  bool have_forces = false;     // a force pass ran since the particles were set
+  bool forces_current = false;  // ... and the positions have not moved since
   bool trav_range_partial = false;
+  int mixed_variant = 0;  // occupancy variant of the mixed traversal (PT_MIXED_VARIANT)
 };
 
 namespace {
@@ -179,7 +182,16 @@ int grow_nodes(pt_handle* h, int64_t need) {
   dfree(o.first_child); dfree(o.count); dfree(o.mom); dfree(o.walk); dfree(o.quad); dfree(o.quadf);
   dfree(o.fifo); dfree(o.nleaf_sub); dfree(o.nempty_sub); dfree(o.leaf_base); dfree(o.empty_base);
   h->nd = nn;
-  CKR(dalloc(h, &h->flags, nc));
+  // flags holds the current level's child ranks while the build is running:
+  // the new buffer must start with the old contents.
+  uint32_t* nf = nullptr;
+  CK(cudaMalloc((void**)&nf, nc * sizeof(uint32_t)));
+  if (h->flags && h->node_cap > 0) {
+    CK(cudaMemcpyAsync(nf, h->flags, h->node_cap * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  dfree(h->flags);
+  h->flags = nf;
   h->node_cap = nc;
   return PT_OK;
 }
@@ -249,7 +261,7 @@ int build_tree(pt_handle* h) {
       h->nnodes = next;
       CKR(grow_nodes(h, need));
     }
-    launch_build_children(h->nd, h->p.key, begin, count, h->flags, next, h->cfg.bucket, st);
+    launch_build_children(h->nd, h->p.key, begin, count, h->flags, next, h->cfg.bucket, h->node_cap, h->d_status, st);
     begin = next;
     count = 8 * (int64_t)ni;
     h->nnodes = need;
@@ -294,7 +306,8 @@ int upward(pt_handle* h) {
 }
 
 int run_traversal(pt_handle* h, TravParams& P, int grid) {
-  if (h->cfg.precision == PT_MIXED && P.mode != 1) launch_traverse_mixed(P, h->nd.mom, grid, h->stream);
+  if (h->cfg.precision == PT_MIXED && P.mode != 1)
+    launch_traverse_mixed(P, h->nd.mom, grid, h->mixed_variant, h->stream);
   else launch_traverse_f64(P, h->nd.mom, grid, h->stream);
   CK(cudaGetLastError());
   return PT_OK;
@@ -320,6 +333,7 @@ int traverse(pt_handle* h, int64_t b0, int64_t b1) {
   P.b_begin = b0;
   P.b_end = b1;
   P.ox = P.oy = P.oz = 0.0;
+  P.nnodes = h->nnodes;
   P.counters = h->d_counters;
   P.work = h->d_work;
   P.status = h->d_status;
@@ -381,6 +395,7 @@ int forces(pt_handle* h, int64_t b0, int64_t b1) {
     h->nnodes = 0;
     h->nbuckets = 0;
     h->have_forces = true;
+    h->forces_current = true;
     return PT_OK;
   }
   CKR(keys_and_sort(h));
@@ -405,6 +420,7 @@ int forces(pt_handle* h, int64_t b0, int64_t b1) {
   CK(cudaEventElapsedTime(&k.ms_traverse, h->ev[5], h->ev[6]));
   CK(cudaEventElapsedTime(&k.ms_total, h->ev[0], h->ev[6]));
   h->have_forces = true;
+  h->forces_current = true;
   return PT_OK;
 }
 
@@ -447,6 +463,7 @@ int set_particles_impl(pt_handle* h, int64_t n, const double* const src[8], cuda
   launch_iota_i32(h->p.order, n, grid_for(h, n), h->stream);
   CK(cudaGetLastError());
   h->have_forces = false;
+  h->forces_current = false;
   h->lists_valid = false;
   return PT_OK;
 }
@@ -489,6 +506,7 @@ int pt_create(const pt_config* cfg, pt_handle** out) {
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess) return bail(PT_E_CUDA);
   h->sms = prop.multiProcessorCount;
+  if (const char* v = std::getenv("PT_MIXED_VARIANT")) h->mixed_variant = std::atoi(v);
   if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) return bail(PT_E_CUDA);
   h->stream = h->own_stream;
   for (auto& e : h->ev)
@@ -618,9 +636,9 @@ int pt_step(pt_handle* h, int nsteps) {
       h->last_dt = dt;
       launch_kick_perturb(h->p, h->n, dt, g, h->stream);
       CK(cudaGetLastError());
-      h->have_forces = false;
+      h->forces_current = false;
     } else {
-      if (!h->have_forces) CKR(forces(h, 0, INT64_MAX));
+      if (!h->forces_current) CKR(forces(h, 0, INT64_MAX));
       double dt;
       CKR(timestep(h, &dt));
       h->last_dt = dt;

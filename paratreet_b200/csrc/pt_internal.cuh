@@ -32,14 +32,21 @@ struct Particles {
 
 // Per-node walk record: what one lane needs to classify one child.
 struct __align__(16) WalkRec {
-  double cm[3];      // MultipoleMoments::cm
-  double orsq;       // radius^2 * gravity_factor (GravityVisitor::open, :164)
+  double cm[3];         // MultipoleMoments::cm
+  union {
+    double orsq;        // Internal: radius^2 * gravity_factor (GravityVisitor::open, :164)
+    double reach;       // Leaf: max |x_j - cm| over the leaf's particles
+  };
+  union {
+    double soft;        // Internal: MultipoleMoments::soft (openSoftening, :124)
+    double soft_max;    // Leaf: max particle softening in the leaf
+  };
   int32_t first_child;  // first of 8 contiguous children, -1 for leaves
-  int32_t type;      // kTypeLeaf / kTypeEmpty / kTypeInternal
-  int32_t count;     // CentroidData::count
-  int32_t pstart;    // first particle (sorted order)
-  int32_t pcount;    // particles in the node's key range
-  int32_t pad[3];
+  int32_t type;         // kTypeLeaf / kTypeEmpty / kTypeInternal
+  int32_t count;        // CentroidData::count
+  int32_t pstart;       // first particle (sorted order)
+  int32_t pcount;       // particles in the node's key range
+  int32_t pad;
 };
 static_assert(sizeof(WalkRec) == 64, "WalkRec is one 64-byte record");
 
@@ -59,6 +66,7 @@ struct Mom {
   double mass, cm[3], soft, radius;
   double xx, xy, xz, yy, yz, zz;
   double lo[3], hi[3];
+  double reach, soft_max;  // leaves only: max |x_j - cm|, max particle softening
 };
 
 // Node arrays (breadth-first order: level by level, children of one parent
@@ -93,6 +101,7 @@ struct TravParams {
   const int32_t* buckets; // bucket b -> node index (DFS order)
   int64_t b_begin, b_end;
   double ox, oy, oz;      // GravityVisitor offset (periodic replicas; 0 otherwise)
+  int64_t nnodes;
   int mode;               // 0 evaluate, 1 count lists only, 2 evaluate + record lists
   int64_t* list_count;    // mode 1: entries per bucket
   const int64_t* list_off;// mode 2: CSR offsets

@@ -31,7 +31,7 @@ void gather_i32(const int32_t* in, int32_t* out, const uint32_t* idx, int64_t n,
 void launch_init_root(Nodes nd, int64_t n, int bucket, cudaStream_t st);
 void launch_flag_internal(const int32_t* type, int64_t begin, int64_t count, uint32_t* flags, cudaStream_t st);
 void launch_build_children(Nodes nd, const uint64_t* keys, int64_t begin, int64_t count, const uint32_t* rank,
-                           int64_t next_begin, int bucket, cudaStream_t st);
+                           int64_t next_begin, int bucket, int64_t cap, unsigned* status, cudaStream_t st);
 void launch_count_subtree(Nodes nd, int64_t begin, int64_t count, cudaStream_t st);
 void launch_base_topdown(Nodes nd, int64_t begin, int64_t count, cudaStream_t st);
 void launch_assign_buckets(Nodes nd, int64_t nnodes, int32_t* buckets, int nleaves, cudaStream_t st);
@@ -50,7 +50,7 @@ void launch_direct_sum(const double* x, const double* y, const double* z, const 
 // k_mixed.cu
 void launch_prep_sources(const int32_t* buckets, int64_t nbuckets, const WalkRec* walk, Particles p, float4* srcf,
                          float* softf, cudaStream_t st);
-void launch_traverse_mixed(const TravParams& P, const Mom* mom, int grid, cudaStream_t st);
+void launch_traverse_mixed(const TravParams& P, const Mom* mom, int grid, int variant, cudaStream_t st);
 
 // k_util.cu
 void launch_scatter_f64(const double* in, double* out, const int32_t* order, int64_t n, int grid, cudaStream_t st);

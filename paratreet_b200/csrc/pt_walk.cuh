@@ -1,5 +1,6 @@
-// pt_walk.cuh -- the warp-per-bucket tree walk shared by the FP64 and mixed
-// traversal kernels.
+// pt_walk.cuh -- the ordered warp-per-bucket tree walk of the FP64 traversal
+// (and of interaction-list recording), plus the FP64-exact opening tests that
+// every traversal shares.
 //
 // Semantics: TransposedDownTraverser::recurse (src/Traverser.h:154-217) for
 // one target bucket is a pre-order depth-first walk from the root: a Leaf is
@@ -10,14 +11,14 @@
 //
 // B200 mapping: one warp owns one bucket (lanes = target particles).  When a
 // node is opened, lanes 0..7 classify its 8 contiguous children in parallel
-// (64-byte WalkRec each, one coalesced 512-byte read); three ballots give
-// per-child P2P / P2C / open masks.  The terminal children before the first
-// opened child are handed to the evaluator in child order, the remaining
-// masks are pushed on a per-warp shared-memory frame stack, and the walk
-// descends.  Every decision is warp-uniform, so there is no divergence in the
-// walk itself.  The opening test uses __dadd_rn/__dmul_rn so it evaluates
-// identically (no FMA contraction) in every translation unit: the FP64 and
-// mixed forms see the same interaction lists.
+// (64-byte WalkRec each, one coalesced 512-byte read) into P2P / P2C
+// (quadrupole) / P2C (softened monopole, GravityVisitor::openSoftening) /
+// open; four ballots give the per-child masks.  The terminal children before
+// the first opened child are handed to the evaluator in child order, the
+// remaining masks are pushed on a per-warp shared-memory frame stack, and the
+// walk descends.  Every decision is warp-uniform.  The tests use
+// __dadd_rn/__dmul_rn so that they evaluate identically (no FMA contraction)
+// in every translation unit: all traversal forms see the same interactions.
 #pragma once
 
 #include "pt_internal.cuh"
@@ -27,9 +28,12 @@ namespace pt {
 constexpr int kWalkStack = 32;
 constexpr unsigned kFull = 0xffffffffu;
 
+// Child classes.
+enum : int { kClsNone = 0, kClsP2P = 1, kClsQuad = 2, kClsOpen = 3, kClsMono = 4 };
+
 struct WalkFrame {
   int32_t c0;     // index of child 0
-  uint32_t bits;  // P2P mask (0-7) | P2C mask (8-15) << 8 | open mask (16-23) << 16
+  uint32_t bits;  // P2P (0-7) | P2C quadrupole (8-15) | P2C monopole (16-23) | open (24-31)
 };
 
 // Space::intersect(box, centre, rsq) of the reference's utility submodule
@@ -45,6 +49,16 @@ __device__ __forceinline__ bool box_sphere_exact(const double lo[3], const doubl
   if ((d = __dadd_rn(lo[2], -cz)) > 0) dsq = __dadd_rn(dsq, __dmul_rn(d, d));
   else if ((d = __dadd_rn(cz, -hi[2])) > 0) dsq = __dadd_rn(dsq, __dmul_rn(d, d));
   return dsq <= rsq;
+}
+
+// Squared distance from a point to a box (0 inside); conservative helper.
+__device__ __forceinline__ double box_dist2(const double lo[3], const double hi[3], double cx, double cy,
+                                            double cz) {
+  double dsq = 0.0, d;
+  if ((d = lo[0] - cx) > 0) dsq += d * d; else if ((d = cx - hi[0]) > 0) dsq += d * d;
+  if ((d = lo[1] - cy) > 0) dsq += d * d; else if ((d = cy - hi[1]) > 0) dsq += d * d;
+  if ((d = lo[2] - cz) > 0) dsq += d * d; else if ((d = cz - hi[2]) > 0) dsq += d * d;
+  return dsq;
 }
 
 // GravityVisitor::openSoftening (:122-128): the softening spheres overlap, or
@@ -64,39 +78,62 @@ struct BucketGeom {
   double lo[3], hi[3];  // target bucket's particle bbox (CentroidData::box)
   double cm[3];         // target bucket's centre of mass
   double soft;          // target bucket's mass-weighted softening
+  double soft_max;      // max particle softening in the bucket
 };
 
-// Classify up to 8 nodes [c0, c0+nvalid) against the bucket; returns frame bits.
-__device__ __forceinline__ uint32_t classify_children(const WalkRec* __restrict__ walk, int c0, int nvalid,
-                                                      const BucketGeom& g, double ox, double oy, double oz,
-                                                      int lane, unsigned long long& n_open) {
-  int code = 0;
-  if (lane < nvalid) {
-    const WalkRec w = walk[c0 + lane];
-    if (w.type == kTypeLeaf) {
-      code = 1;
-    } else if (w.type == kTypeInternal) {
-      bool open = (w.count <= kMinParticleNode) ||
-                  box_sphere_exact(g.lo, g.hi, __dadd_rn(w.cm[0], ox), __dadd_rn(w.cm[1], oy),
-                                   __dadd_rn(w.cm[2], oz), w.orsq);
-      code = open ? 3 : 2;
-    }
-  }
-  uint32_t pp = __ballot_sync(kFull, code == 1);
-  uint32_t pc = __ballot_sync(kFull, code == 2);
-  uint32_t op = __ballot_sync(kFull, code == 3);
-  n_open += (unsigned long long)__popc(pc | op);
-  return (pp & 0xffu) | ((pc & 0xffu) << 8) | ((op & 0xffu) << 16);
+__device__ __forceinline__ void load_bucket_geom(const Mom* mom, int node, BucketGeom& g) {
+  const Mom& q = mom[node];
+  g.lo[0] = q.lo[0]; g.lo[1] = q.lo[1]; g.lo[2] = q.lo[2];
+  g.hi[0] = q.hi[0]; g.hi[1] = q.hi[1]; g.hi[2] = q.hi[2];
+  g.cm[0] = q.cm[0]; g.cm[1] = q.cm[1]; g.cm[2] = q.cm[2];
+  g.soft = q.soft;
+  g.soft_max = q.soft_max;
 }
 
-// Walk the tree for one bucket; ev.p2p(node) / ev.p2c(node) are called in
+// Class of one node against the bucket (GravityVisitor::open / node).
+__device__ __forceinline__ int classify_node(const WalkRec& w, const BucketGeom& g, double ox, double oy, double oz) {
+  if (w.type == kTypeLeaf) return kClsP2P;
+  if (w.type != kTypeInternal) return kClsNone;
+  const double cx = __dadd_rn(w.cm[0], ox), cy = __dadd_rn(w.cm[1], oy), cz = __dadd_rn(w.cm[2], oz);
+  if (w.count <= kMinParticleNode || box_sphere_exact(g.lo, g.hi, cx, cy, cz, w.orsq)) return kClsOpen;
+  if (w.count == 0) return kClsNone;
+  return open_softening_exact(cx, cy, cz, w.soft, g.cm[0], g.cm[1], g.cm[2], g.soft, g.lo, g.hi) ? kClsMono
+                                                                                                : kClsQuad;
+}
+
+// Classify up to 8 nodes [c0, c0+nvalid) against the bucket; returns frame bits.
+__device__ __forceinline__ uint32_t classify_children(const WalkRec* __restrict__ walk, int64_t nnodes, int c0,
+                                                      int nvalid, const BucketGeom& g, double ox, double oy,
+                                                      double oz, int lane, unsigned long long& n_open,
+                                                      unsigned* status) {
+  int code = kClsNone;
+  bool internal = false;
+  if (lane < nvalid) {
+    int64_t idx = (int64_t)c0 + lane;
+    if (c0 < 0 || idx >= nnodes) {
+      atomicOr(status, kErrCapacity);
+    } else {
+      const WalkRec w = walk[idx];
+      internal = (w.type == kTypeInternal);
+      code = classify_node(w, g, ox, oy, oz);
+    }
+  }
+  uint32_t pp = __ballot_sync(kFull, code == kClsP2P) & 0xffu;
+  uint32_t pq = __ballot_sync(kFull, code == kClsQuad) & 0xffu;
+  uint32_t pm = __ballot_sync(kFull, code == kClsMono) & 0xffu;
+  uint32_t op = __ballot_sync(kFull, code == kClsOpen) & 0xffu;
+  n_open += (unsigned long long)__popc(__ballot_sync(kFull, internal) & 0xffu);
+  return pp | (pq << 8) | (pm << 16) | (op << 24);
+}
+
+// Walk the tree for one bucket; ev.p2p(node), ev.p2c(node, mono) are called in
 // the reference's per-bucket order.  Returns false on stack overflow.
 template <class Eval>
-__device__ __forceinline__ bool walk_bucket(const WalkRec* __restrict__ walk, const BucketGeom& g, double ox,
-                                            double oy, double oz, WalkFrame* stack, int lane, Eval& ev,
-                                            unsigned long long& n_open) {
+__device__ __forceinline__ bool walk_bucket(const WalkRec* __restrict__ walk, int64_t nnodes, const BucketGeom& g,
+                                            double ox, double oy, double oz, WalkFrame* stack, int lane, Eval& ev,
+                                            unsigned long long& n_open, unsigned* status) {
   int c0 = 0;  // the root, tested as a one-child frame
-  uint32_t bits = classify_children(walk, 0, 1, g, ox, oy, oz, lane, n_open);
+  uint32_t bits = classify_children(walk, nnodes, 0, 1, g, ox, oy, oz, lane, n_open, status);
   int sp = 0;
   while (true) {
     if (bits == 0) {
@@ -107,21 +144,22 @@ __device__ __forceinline__ bool walk_bucket(const WalkRec* __restrict__ walk, co
       bits = f.bits;
       continue;
     }
-    uint32_t pp = bits & 0xffu, pc = (bits >> 8) & 0xffu, op = (bits >> 16) & 0xffu;
+    uint32_t pp = bits & 0xffu, pq = (bits >> 8) & 0xffu, pm = (bits >> 16) & 0xffu, op = bits >> 24;
     int fo = op ? (__ffs(op) - 1) : 8;
     uint32_t low = (1u << fo) - 1u;
-    uint32_t run = (pp | pc) & low;
+    uint32_t run = (pp | pq | pm) & low;
     while (run) {
       int k = __ffs(run) - 1;
       run &= run - 1u;
       if ((pp >> k) & 1u) ev.p2p(c0 + k);
-      else ev.p2c(c0 + k);
+      else ev.p2c(c0 + k, ((pm >> k) & 1u) != 0);
     }
     pp &= ~low;
-    pc &= ~low;
+    pq &= ~low;
+    pm &= ~low;
     if (fo < 8) {
       op &= ~(1u << fo);
-      uint32_t rem = pp | (pc << 8) | (op << 16);
+      uint32_t rem = pp | (pq << 8) | (pm << 16) | (op << 24);
       if (rem) {
         if (sp >= kWalkStack) return false;
         __syncwarp();
@@ -129,10 +167,9 @@ __device__ __forceinline__ bool walk_bucket(const WalkRec* __restrict__ walk, co
         __syncwarp();
         ++sp;
       }
-      int child = c0 + fo;
-      int nc0 = walk[child].first_child;
+      int nc0 = walk[c0 + fo].first_child;
       c0 = nc0;
-      bits = classify_children(walk, nc0, 8, g, ox, oy, oz, lane, n_open);
+      bits = classify_children(walk, nnodes, nc0, 8, g, ox, oy, oz, lane, n_open, status);
     } else {
       bits = 0;
     }
@@ -152,7 +189,7 @@ struct ListRecorder {
     if (mode == 2 && lane == 0) { node_out[base + n] = node; kind_out[base + n] = 0; }
     ++n;
   }
-  __device__ void p2c(int node) {
+  __device__ void p2c(int node, bool) {
     if (mode == 2 && lane == 0) { node_out[base + n] = node; kind_out[base + n] = 1; }
     ++n;
   }
