@@ -365,11 +365,7 @@ __global__ void __launch_bounds__(kTravWarps * 32) traverse_f64(TravParams P, co
     }
     BucketGeom g;
     load_bucket_geom(mom, tnode, g);
-    const int t0 = P.walk[tnode].pstart, nt = P.walk[tnode].pcount;
-    if (nt > 32) {  // buckets are limited to 32 at handle creation
-      if (lane == 0) atomicOr(P.status, kErrBucketTooBig);
-      continue;
-    }
+    const int tbase = P.walk[tnode].pstart, ntot = P.walk[tnode].pcount;
     if (P.mode == 1) {  // count the interaction list only
       ListRecorder rec{lane, 1, 0, 0, nullptr, nullptr};
       if (!walk_bucket(P.walk, P.nnodes, g, P.ox, P.oy, P.oz, stacks[wid], lane, rec, c_open, P.status) &&
@@ -378,41 +374,50 @@ __global__ void __launch_bounds__(kTravWarps * 32) traverse_f64(TravParams P, co
       if (lane == 0) P.list_count[b - P.b_begin] = rec.n;
       continue;
     }
-    F64Eval ev;
-    ev.p = &P.p;
-    ev.walk = P.walk;
-    ev.quad = P.quad;
-    ev.stage = stage[wid];
-    ev.lane = lane;
-    ev.nt = nt;
-    ev.xi = ev.yi = ev.zi = ev.si = 0.0;
-    if (lane < nt) {
-      ev.xi = P.p.x[t0 + lane];
-      ev.yi = P.p.y[t0 + lane];
-      ev.zi = P.p.z[t0 + lane];
-      ev.si = P.p.soft[t0 + lane];
+    // A bucket holds more than 32 particles only when more than `bucket`
+    // particles share one 63-bit key (depth-21 leaf); its targets are then
+    // walked in chunks of 32 (the decisions depend on the bucket only).
+    for (int tc = 0; tc < ntot; tc += 32) {
+      const int t0 = tbase + tc, nt = min(32, ntot - tc);
+      unsigned long long opens = 0;
+      F64Eval ev;
+      ev.p = &P.p;
+      ev.walk = P.walk;
+      ev.quad = P.quad;
+      ev.stage = stage[wid];
+      ev.lane = lane;
+      ev.nt = nt;
+      ev.xi = ev.yi = ev.zi = ev.si = 0.0;
+      if (lane < nt) {
+        ev.xi = P.p.x[t0 + lane];
+        ev.yi = P.p.y[t0 + lane];
+        ev.zi = P.p.z[t0 + lane];
+        ev.si = P.p.soft[t0 + lane];
+      }
+      ev.ax = ev.ay = ev.az = ev.pot = ev.potf = 0.0;
+      ev.ox = P.ox; ev.oy = P.oy; ev.oz = P.oz;
+      ev.g = &g;
+      ev.n_pp = 0; ev.n_pc = 0;
+      ev.record = (P.mode == 2 && tc == 0);
+      ev.nlist = 0;
+      ev.lbase = ev.record ? P.list_off[b - P.b_begin] : 0;
+      ev.lnode = P.list_node;
+      ev.lkind = P.list_kind;
+      if (!walk_bucket(P.walk, P.nnodes, g, P.ox, P.oy, P.oz, stacks[wid], lane, ev, opens, P.status) &&
+          lane == 0)
+        atomicOr(P.status, kErrStack);
+      if (tc == 0) c_open += opens;
+      if (lane < nt) {
+        int i = t0 + lane;
+        P.p.ax[i] = ev.ax;
+        P.p.ay[i] = ev.ay;
+        P.p.az[i] = ev.az;
+        P.p.pot[i] = ev.pot;
+        P.p.potf[i] = ev.potf;
+      }
+      c_pp += ev.n_pp;
+      c_pc += ev.n_pc;
     }
-    ev.ax = ev.ay = ev.az = ev.pot = ev.potf = 0.0;
-    ev.ox = P.ox; ev.oy = P.oy; ev.oz = P.oz;
-    ev.g = &g;
-    ev.n_pp = 0; ev.n_pc = 0;
-    ev.record = (P.mode == 2);
-    ev.nlist = 0;
-    ev.lbase = ev.record ? P.list_off[b - P.b_begin] : 0;
-    ev.lnode = P.list_node;
-    ev.lkind = P.list_kind;
-    if (!walk_bucket(P.walk, P.nnodes, g, P.ox, P.oy, P.oz, stacks[wid], lane, ev, c_open, P.status) && lane == 0)
-      atomicOr(P.status, kErrStack);
-    if (lane < nt) {
-      int i = t0 + lane;
-      P.p.ax[i] = ev.ax;
-      P.p.ay[i] = ev.ay;
-      P.p.az[i] = ev.az;
-      P.p.pot[i] = ev.pot;
-      P.p.potf[i] = ev.potf;
-    }
-    c_pp += ev.n_pp;
-    c_pc += ev.n_pc;
   }
   if (lane == 0) {
     atomicAdd(&P.counters[0], c_pp);

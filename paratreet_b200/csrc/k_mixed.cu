@@ -54,8 +54,9 @@ struct MixWarp {
   BucketGeom geom;          // the target bucket (FP64), read by the walk
   int32_t stack[kMixStack];
   float4 cbuf[kMixBuf];     // P2C: offset xyz, node index bits (mono: node | 1<<31)
-  float4 fbuf[kMixBuf];     // P2P far leaves: offset xyz, node index bits
-  float4 nbuf[kMixBuf];     // P2P near leaves: offset xyz, node index bits
+  float4 pbuf[kMixBuf];     // P2P leaves: offset xyz, node index bits; far leaves
+                            // fill from the front, near leaves from the back
+  float kahan[8][32];       // per-lane compensated sums (s, c) of ax, ay, az, pot
   int32_t pre[kMixBuf + 1]; // prefix of leaf sizes during a P2P flush
   int32_t ps0[kMixBuf];     // first particle of each buffered leaf
   float4 src[32];           // staged sources: x, y, z (rel. bucket), m
@@ -125,11 +126,19 @@ struct MixCtx {
   int lane, t, grp, G, nt;
   float tx, ty, tz, ts;                 // this lane's target (rel. bucket cm)
   float pax, pay, paz, ppf;             // flush partials
-  Kahan ax, ay, az, pf;
-  unsigned long long n_pp, n_pc;
+  float (*kah)[32];                     // this warp's compensated sums in shared memory
+  unsigned n_src, n_node;               // sources / nodes evaluated for this target chunk
 
+  // Kahan-add the flush partials into the lane's compensated sums.
   __device__ __forceinline__ void commit() {
-    ax.add(pax); ay.add(pay); az.add(paz); pf.add(ppf);
+    const float v[4] = {pax, pay, paz, ppf};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      Kahan q{kah[2 * k][lane], kah[2 * k + 1][lane]};
+      q.add(v[k]);
+      kah[2 * k][lane] = q.s;
+      kah[2 * k + 1][lane] = q.c;
+    }
     pax = pay = paz = ppf = 0.f;
   }
 };
@@ -155,24 +164,33 @@ __device__ __forceinline__ void flush_p2p(MixWarp& w, const float4* __restrict__
   if (x.lane + 32 < nleaves) { w.pre[x.lane + 32] = tota + incb - nb; w.ps0[x.lane + 32] = s0b; }
   if (x.lane == 0) w.pre[nleaves] = total;
   __syncwarp();
-  for (int cs = 0; cs < total; cs += 32) {
+  // Chunks of 32 sources; the loads of chunk k+1 are issued before chunk k is
+  // evaluated so that their L2 latency overlaps the arithmetic.
+  int base_leaf = 0;  // leaf holding the next chunk's first source
+  float4 nraw = make_float4(0.f, 0.f, 0.f, 0.f), noff = nraw;
+  float nsoft = 0.f;
+  auto fetch = [&](int cs) {
     const int q = cs + x.lane;
+    int lo = base_leaf;  // last leaf with pre <= q: a chunk spans few leaves
+    while (lo + 1 < nleaves && w.pre[lo + 1] <= q) lo++;
+    base_leaf = __shfl_sync(kFull, lo, 31);
     if (q < total) {
-      int lo = 0, hi = nleaves - 1;  // last leaf with pre <= q
-      while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (w.pre[mid] <= q) lo = mid;
-        else hi = mid - 1;
-      }
-      const float4 e = buf[lo];
+      noff = buf[lo];
       const int j = w.ps0[lo] + (q - w.pre[lo]);
-      const float4 s = srcf[j];
-      w.src[x.lane] = make_float4(s.x + e.x, s.y + e.y, s.z + e.z, s.w);
-      if (!kFar) w.ssoft[x.lane] = softf[j];
+      nraw = srcf[j];
+      if (!kFar) nsoft = softf[j];
+    }
+  };
+  fetch(0);
+  for (int cs = 0; cs < total; cs += 32) {
+    if (cs + x.lane < total) {
+      w.src[x.lane] = make_float4(nraw.x + noff.x, nraw.y + noff.y, nraw.z + noff.z, nraw.w);
+      if (!kFar) w.ssoft[x.lane] = nsoft;
     }
     __syncwarp();
+    if (cs + 32 < total) fetch(cs + 32);
     const int cnt = min(32, total - cs);
-    if (kFar && x.t < x.nt) {
+    if (kFar && x.grp < x.G) {
       float bx = 0.f, by = 0.f, bz = 0.f, bp = 0.f;  // second chain
       int jj = x.grp;
       for (; jj + x.G < cnt; jj += 2 * x.G) {
@@ -210,7 +228,7 @@ __device__ __forceinline__ void flush_p2p(MixWarp& w, const float4* __restrict__
       x.pay += by;
       x.paz += bz;
       x.ppf += bp;
-    } else if (!kFar && x.t < x.nt) {
+    } else if (!kFar && x.grp < x.G) {
       for (int jj = x.grp; jj < cnt; jj += x.G) {
         const float4 s = w.src[jj];
         const float dx = s.x - x.tx, dy = s.y - x.ty, dz = s.z - x.tz;
@@ -229,7 +247,7 @@ __device__ __forceinline__ void flush_p2p(MixWarp& w, const float4* __restrict__
     }
     __syncwarp();
   }
-  x.n_pp += (unsigned long long)total * (unsigned long long)x.nt;
+  x.n_src += (unsigned)total;
   x.commit();
 }
 
@@ -267,23 +285,32 @@ __device__ __forceinline__ void p2c_term(const float4 A, const float4 B, const f
 // Evaluate all buffered P2C nodes.
 __device__ __forceinline__ void flush_p2c(MixWarp& w, int nent, const QuadRecF* __restrict__ quadf, MixCtx& x) {
   const float qnan = __int_as_float(0x7fc00000);
-  for (int cs = 0; cs < nent; cs += 32) {
+  float4 ne = make_float4(0.f, 0.f, 0.f, 0.f), nq0 = ne, nq1 = ne;  // next chunk's entry and record
+  auto fetch = [&](int cs) {
     const int q = cs + x.lane;
     if (q < nent) {
-      const float4 e = w.cbuf[q];
-      const QuadRecF r = quadf[entry_node(e)];
-      w.qa[x.lane] = make_float4(e.x, e.y, e.z, r.mass);
-      if (entry_flag(e)) {
+      ne = w.cbuf[q];
+      const float4* rec = reinterpret_cast<const float4*>(quadf + entry_node(ne));
+      nq0 = rec[0];  // mass, soft, xx, xy
+      nq1 = rec[1];  // xz, yy, yz, zz
+    }
+  };
+  fetch(0);
+  for (int cs = 0; cs < nent; cs += 32) {
+    if (cs + x.lane < nent) {
+      w.qa[x.lane] = make_float4(ne.x, ne.y, ne.z, nq0.x);
+      if (entry_flag(ne)) {
         w.qb[x.lane] = make_float4(0.f, 0.f, 0.f, 0.f);
         w.qc[x.lane] = make_float4(0.f, 0.f, qnan, 0.f);
       } else {
-        w.qb[x.lane] = make_float4(r.xx, r.xy, r.xz, r.yy);
-        w.qc[x.lane] = make_float4(r.yz, r.zz, r.soft, 0.5f * (r.xx + r.yy + r.zz));
+        w.qb[x.lane] = make_float4(nq0.z, nq0.w, nq1.x, nq1.y);
+        w.qc[x.lane] = make_float4(nq1.z, nq1.w, nq0.y, 0.5f * (nq0.z + nq1.y + nq1.w));
       }
     }
     __syncwarp();
+    if (cs + 32 < nent) fetch(cs + 32);
     const int cnt = min(32, nent - cs);
-    if (x.t < x.nt) {
+    if (x.grp < x.G) {
       float bx = 0.f, by = 0.f, bz = 0.f, bp = 0.f;  // second chain
       int ee = x.grp;
       for (; ee + x.G < cnt; ee += 2 * x.G) {
@@ -299,7 +326,7 @@ __device__ __forceinline__ void flush_p2c(MixWarp& w, int nent, const QuadRecF* 
     }
     __syncwarp();
   }
-  x.n_pc += (unsigned long long)nent * (unsigned long long)x.nt;
+  x.n_node += (unsigned)nent;
   x.commit();
 }
 
@@ -331,119 +358,130 @@ __global__ void __launch_bounds__(kMixWarps * 32, kMinBlocks) traverse_mixed(Tra
     if (lane == 0) load_bucket_geom(mom, tnode, w.geom);
     __syncwarp();
     const BucketGeom& g = w.geom;
-    const int t0 = P.walk[tnode].pstart, nt = P.walk[tnode].pcount;
-    if (nt > 32 || nt < 1) {
-      if (lane == 0) atomicOr(P.status, kErrBucketTooBig);
-      continue;
-    }
-    MixCtx x;
-    x.lane = lane;
-    x.nt = nt;
-    int lt = 0;
-    while ((1 << lt) < nt) lt++;
-    x.t = lane & ((1 << lt) - 1);
-    x.grp = lane >> lt;
-    x.G = 32 >> lt;
-    x.tx = x.ty = x.tz = x.ts = 0.f;
-    if (x.t < nt) {
-      const int i = t0 + x.t;
-      x.tx = (float)(P.p.x[i] - g.cm[0]);
-      x.ty = (float)(P.p.y[i] - g.cm[1]);
-      x.tz = (float)(P.p.z[i] - g.cm[2]);
-      x.ts = (float)P.p.soft[i];
-    }
-    x.pax = x.pay = x.paz = x.ppf = 0.f;
-    x.ax = x.ay = x.az = x.pf = Kahan{0.f, 0.f};
-    x.n_pp = x.n_pc = 0;
+    const int tbase = P.walk[tnode].pstart, ntot = P.walk[tnode].pcount;
+    // more than 32 particles only in a depth-21 leaf of identical keys: its
+    // targets are walked in chunks of 32 (decisions depend on the bucket only)
+    for (int tc = 0; tc < ntot; tc += 32) {
+      const int t0 = tbase + tc, nt = min(32, ntot - tc);
+      unsigned long long opens = 0;
+      MixCtx x;
+      x.lane = lane;
+      x.nt = nt;
+      x.t = lane % nt;
+      x.grp = lane / nt;
+      x.G = 32 / nt;
+      x.tx = x.ty = x.tz = x.ts = 0.f;
+      if (x.grp < x.G) {
+        const int i = t0 + x.t;
+        x.tx = (float)(P.p.x[i] - g.cm[0]);
+        x.ty = (float)(P.p.y[i] - g.cm[1]);
+        x.tz = (float)(P.p.z[i] - g.cm[2]);
+        x.ts = (float)P.p.soft[i];
+      }
+      x.pax = x.pay = x.paz = x.ppf = 0.f;
+      x.kah = w.kahan;
+#pragma unroll
+      for (int k = 0; k < 8; k++) w.kahan[k][lane] = 0.f;
+      x.n_src = x.n_node = 0;
 
-    int sp = 0, nc = 0, nfar = 0, nnear = 0;
-    int nexp = 1;          // nodes expanded this step
-    int e0 = -1;           // first expanded node; -1 = the root itself
-    bool ok = true;
-    int ex[4] = {-1, -1, -1, -1};
-    while (true) {
-      // lanes 8e..8e+7: children of expanded node e (the root step tests node 0)
-      const int e = lane >> 3, c = lane & 7;
-      int node = -1;
-      if (e0 < 0) {
-        if (lane == 0) node = 0;
-      } else if (e < nexp) {
-        node = P.walk[ex[e]].first_child + c;
-      }
-      int cls = kClsNone;
-      WalkRec r;
-      if (node >= 0) {
-        if (node >= P.nnodes) {
-          atomicOr(P.status, kErrCapacity);
-        } else {
-          r = P.walk[node];
-          cls = classify_node(r, g, P.ox, P.oy, P.oz);
+      int sp = 0, nc = 0, nfar = 0, nnear = 0;
+      int nexp = 1;          // nodes expanded this step
+      int pop = -1;          // stack slot of the first expanded node; -1 = the root step
+      bool ok = true;
+      while (true) {
+        // lanes 8e..8e+7: children of expanded node e (the root step tests node 0)
+        const int e = lane >> 3, c = lane & 7;
+        int node = -1;
+        if (pop < 0) {
+          if (lane == 0) node = 0;
+        } else if (e < nexp) {
+          node = w.stack[pop + e] + c;  // the stack holds first children of opened nodes
         }
-      }
-      c_open += (unsigned long long)__popc(__ballot_sync(kFull, node >= 0 && node < P.nnodes &&
-                                                                    r.type == kTypeInternal));
-      float ofx = 0.f, ofy = 0.f, ofz = 0.f;
-      bool far = false;
-      if (cls == kClsP2P || cls == kClsQuad || cls == kClsMono) {
-        const double cx = r.cm[0] + P.ox, cy = r.cm[1] + P.oy, cz = r.cm[2] + P.oz;
-        ofx = (float)(cx - g.cm[0]);
-        ofy = (float)(cy - g.cm[1]);
-        ofz = (float)(cz - g.cm[2]);
-        if (cls == kClsP2P) {
-          const double reach = r.reach + r.soft_max + g.soft_max;
-          far = box_dist2(g.lo, g.hi, cx, cy, cz) > reach * reach;
+        int cls = kClsNone;
+        WalkRec r;
+        if (node >= 0) {
+          if (node >= P.nnodes) {
+            atomicOr(P.status, kErrCapacity);
+          } else {
+            r = P.walk[node];
+            cls = classify_node(r, g, P.ox, P.oy, P.oz);
+          }
         }
-      }
-      const float4 ent = pack_entry(ofx, ofy, ofz, node, cls == kClsMono);
-      nc = append(w.cbuf, nc, cls == kClsQuad || cls == kClsMono, ent, lane);
-      nfar = append(w.fbuf, nfar, cls == kClsP2P && far, ent, lane);
-      nnear = append(w.nbuf, nnear, cls == kClsP2P && !far, ent, lane);
-      {
-        const bool op = (cls == kClsOpen);
-        const unsigned m = __ballot_sync(kFull, op);
-        if (sp + __popc(m) > kMixStack) {
-          ok = false;
-          break;
+        opens += (unsigned long long)__popc(__ballot_sync(kFull, node >= 0 && node < P.nnodes &&
+                                                                      r.type == kTypeInternal));
+        float ofx = 0.f, ofy = 0.f, ofz = 0.f;
+        bool far = false;
+        if (cls == kClsP2P || cls == kClsQuad || cls == kClsMono) {
+          const double cx = r.cm[0] + P.ox, cy = r.cm[1] + P.oy, cz = r.cm[2] + P.oz;
+          ofx = (float)(cx - g.cm[0]);
+          ofy = (float)(cy - g.cm[1]);
+          ofz = (float)(cz - g.cm[2]);
+          if (cls == kClsP2P) {
+            const double reach = r.reach + r.soft_max + g.soft_max;
+            far = box_dist2(g.lo, g.hi, cx, cy, cz) > reach * reach;
+          }
         }
-        if (op) w.stack[sp + __popc(m & ((1u << lane) - 1u))] = node;
-        sp += __popc(m);
+        const float4 ent = pack_entry(ofx, ofy, ofz, node, cls == kClsMono);
+        nc = append(w.cbuf, nc, cls == kClsQuad || cls == kClsMono, ent, lane);
+        nfar = append(w.pbuf, nfar, cls == kClsP2P && far, ent, lane);
+        {  // near leaves grow down from the end of the shared buffer
+          const bool nr = (cls == kClsP2P && !far);
+          const unsigned m = __ballot_sync(kFull, nr);
+          if (nr) w.pbuf[kMixBuf - 1 - nnear - __popc(m & ((1u << lane) - 1u))] = ent;
+          nnear += __popc(m);
+        }
+        {
+          const bool op = (cls == kClsOpen);
+          const unsigned m = __ballot_sync(kFull, op);
+          if (sp + __popc(m) > kMixStack) {
+            ok = false;
+            break;
+          }
+          if (op) w.stack[sp + __popc(m & ((1u << lane) - 1u))] = r.first_child;
+          sp += __popc(m);
+        }
+        __syncwarp();
+        // one flush site per kind (the walk's last step drains every buffer)
+        const bool last = (sp == 0);
+        if (nc >= 32 || (last && nc)) { flush_p2c(w, nc, P.quadf, x); nc = 0; }
+        if (nfar + nnear >= 32 || last) {
+          if (nfar) flush_p2p<true>(w, w.pbuf, nfar, P.walk, P.srcf, P.softf, x);
+          if (nnear) flush_p2p<false>(w, w.pbuf + (kMixBuf - nnear), nnear, P.walk, P.srcf, P.softf, x);
+          nfar = nnear = 0;
+        }
+        if (last) break;
+        nexp = sp < 4 ? sp : 4;
+        sp -= nexp;
+        pop = sp;
+        __syncwarp();
+      }
+      if (!ok) {
+        if (lane == 0) atomicOr(P.status, kErrStack);
+        break;
+      }
+
+      // sum the G lane groups of each target (staging area reused as FP64 scratch)
+      double* red = reinterpret_cast<double*>(w.qa);
+      __syncwarp();
+#pragma unroll
+      for (int k = 0; k < 4; k++) red[4 * lane + k] = (double)w.kahan[2 * k][lane] - (double)w.kahan[2 * k + 1][lane];
+      __syncwarp();
+      if (lane < nt) {
+        double v[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int gg = 0; gg < x.G; gg++)
+          for (int k = 0; k < 4; k++) v[k] += red[4 * (gg * nt + lane) + k];
+        const int i = t0 + lane;
+        P.p.ax[i] = v[0];
+        P.p.ay[i] = v[1];
+        P.p.az[i] = v[2];
+        P.p.pot[i] = 0.0;
+        P.p.potf[i] = v[3];
       }
       __syncwarp();
-      if (nc >= 32) { flush_p2c(w, nc, P.quadf, x); nc = 0; }
-      if (nfar >= 32) { flush_p2p<true>(w, w.fbuf, nfar, P.walk, P.srcf, P.softf, x); nfar = 0; }
-      if (nnear >= 32) { flush_p2p<false>(w, w.nbuf, nnear, P.walk, P.srcf, P.softf, x); nnear = 0; }
-      if (sp == 0) break;
-      nexp = sp < 4 ? sp : 4;
-      sp -= nexp;
-      for (int k = 0; k < 4; k++) ex[k] = (k < nexp) ? w.stack[sp + k] : -1;
-      e0 = ex[0];
-      __syncwarp();
+      c_pp += (unsigned long long)x.n_src * (unsigned long long)nt;
+      c_pc += (unsigned long long)x.n_node * (unsigned long long)nt;
+      if (tc == 0) c_open += opens;
     }
-    if (!ok) {
-      if (lane == 0) atomicOr(P.status, kErrStack);
-      continue;
-    }
-    if (nc) flush_p2c(w, nc, P.quadf, x);
-    if (nfar) flush_p2p<true>(w, w.fbuf, nfar, P.walk, P.srcf, P.softf, x);
-    if (nnear) flush_p2p<false>(w, w.nbuf, nnear, P.walk, P.srcf, P.softf, x);
-
-    double vx = x.ax.value(), vy = x.ay.value(), vz = x.az.value(), vp = x.pf.value();
-    for (int o = 1 << lt; o < 32; o <<= 1) {
-      vx += __shfl_xor_sync(kFull, vx, o);
-      vy += __shfl_xor_sync(kFull, vy, o);
-      vz += __shfl_xor_sync(kFull, vz, o);
-      vp += __shfl_xor_sync(kFull, vp, o);
-    }
-    if (x.grp == 0 && x.t < nt) {
-      const int i = t0 + x.t;
-      P.p.ax[i] = vx;
-      P.p.ay[i] = vy;
-      P.p.az[i] = vz;
-      P.p.pot[i] = 0.0;
-      P.p.potf[i] = vp;
-    }
-    c_pp += x.n_pp;
-    c_pc += x.n_pc;
   }
   if (lane == 0) {
     atomicAdd(&P.counters[0], c_pp);

@@ -158,7 +158,10 @@ def test_direct_sum_matches_oracle():
     with sim() as s:
         s.set_particles(p)
         ax, ay, az, pot = s.direct_sum(tgt)
-    assert np.array_equal(ax, rax) and np.array_equal(pot, rpot)
+    # the device sum splits the sources into slices (reassociation only)
+    e = rel_err((ax, ay, az), (rax, ray, raz))
+    assert e.max() < 1e-12
+    assert np.max(np.abs(pot - rpot) / np.abs(rpot)) < 1e-12
 
 
 def test_direct_sum_split_known_answer():
