@@ -22,6 +22,7 @@
 #ifndef PT_GRAVITY_H_
 #define PT_GRAVITY_H_
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -172,6 +173,24 @@ int pt_get_counters(pt_handle* h, pt_counters* c);
  * the kernel of examples/GravityVisitor.h:87-120 with twoh = soft_i + soft_j. */
 int pt_direct_sum(pt_handle* h, int64_t nt, const int32_t* targets, double* ax, double* ay,
                   double* az, double* pot);
+
+/* No counterpart in the reference.  The same FP64 direct sum for callers that
+ * cannot allocate device memory (their buffers come from a pool or budget of
+ * their own, and cudaMalloc / cudaFree would also synchronise the device):
+ * every pointer except errbuf is DEVICE memory supplied by the caller
+ * (sources x..soft of n particles, nt int32 target indices into them, nt
+ * outputs per array; any output may be NULL).  Nothing is allocated: the only
+ * scratch is a fixed 8 MiB array inside the library, held by every GPU that
+ * loads it until exit, which limits nt to 262,136 (larger nt is rejected with
+ * PT_E_ARG).  Works on the current device; the first call on a device looks up
+ * the array's address (make that call before any stream capture).  Issued on
+ * `stream` (cudaStream_t, NULL = default) and synchronised before return.
+ * Calls that overlap on the GPU share the array and race.  On error a message
+ * is written to errbuf (errlen bytes, may be NULL). */
+int pt_direct_sum_noalloc(int64_t n, const double* x, const double* y, const double* z,
+                          const double* m, const double* soft, int64_t nt, const int32_t* targets,
+                          double* ax, double* ay, double* az, double* pot, void* stream,
+                          char* errbuf, size_t errlen);
 
 #ifdef __cplusplus
 }
