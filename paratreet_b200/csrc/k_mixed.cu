@@ -61,35 +61,43 @@ struct MixWarp {
   int32_t ps0[kMixBuf];     // first particle of each buffered leaf
   float4 src[32];           // staged sources: x, y, z (rel. bucket), m
   float ssoft[32];
+  float sreach2[32];        // (soft_j + max bucket softening)^2: beyond it a pair is unsoftened
   float4 qa[32];            // staged P2C: offset xyz, mass
   float4 qb[32];            // xx, xy, xz, yy
   float4 qc[32];            // yz, zz, soft (< 0: monopole), trace/2
 };
 
+// SPLINE in FP32, softened branch (r < twoh): kept out of line so that the
+// rarely taken polynomial does not raise register pressure in the hot loops.
+__device__ __noinline__ void spline_f32_soft(float r2, float rinv, float twoh, float& a, float& b) {
+  float r = r2 * rinv;
+  float dih = 2.0f / twoh;
+  float u = r * dih;
+  float u2 = u * u;
+  if (u < 1.0f) {
+    a = dih * (7.0f / 5.0f - 2.0f / 3.0f * u2 + 3.0f / 10.0f * u2 * u2 - 1.0f / 10.0f * u2 * u2 * u);
+    b = dih * dih * dih * (4.0f / 3.0f - 6.0f / 5.0f * u2 + 1.0f / 2.0f * u2 * u);
+  } else {
+    a = -1.0f / 15.0f * rinv +
+        dih * (8.0f / 5.0f - 4.0f / 3.0f * u2 + u2 * u - 3.0f / 10.0f * u2 * u2 + 1.0f / 30.0f * u2 * u2 * u);
+    b = -1.0f / 15.0f * rinv * rinv * rinv +
+        dih * dih * dih * (8.0f / 3.0f - 3.0f * u + 6.0f / 5.0f * u2 - 1.0f / 6.0f * u2 * u);
+  }
+}
+
 // SPLINE in FP32 (r2 > 0): force term b, potential term a.
 __device__ __forceinline__ void spline_f32(float r2, float rinv, float twoh, float& a, float& b) {
   if (r2 < twoh * twoh) {
-    float r = r2 * rinv;
-    float dih = 2.0f / twoh;
-    float u = r * dih;
-    float u2 = u * u;
-    if (u < 1.0f) {
-      a = dih * (7.0f / 5.0f - 2.0f / 3.0f * u2 + 3.0f / 10.0f * u2 * u2 - 1.0f / 10.0f * u2 * u2 * u);
-      b = dih * dih * dih * (4.0f / 3.0f - 6.0f / 5.0f * u2 + 1.0f / 2.0f * u2 * u);
-    } else {
-      a = -1.0f / 15.0f * rinv +
-          dih * (8.0f / 5.0f - 4.0f / 3.0f * u2 + u2 * u - 3.0f / 10.0f * u2 * u2 + 1.0f / 30.0f * u2 * u2 * u);
-      b = -1.0f / 15.0f * rinv * rinv * rinv +
-          dih * dih * dih * (8.0f / 3.0f - 3.0f * u + 6.0f / 5.0f * u2 - 1.0f / 6.0f * u2 * u);
-    }
+    spline_f32_soft(r2, rinv, twoh, a, b);
   } else {
     a = rinv;
     b = rinv * rinv * rinv;
   }
 }
 
-// SPLINEQ in FP32 with the reference's grouping (examples/GravityVisitor.h:37-80).
-__device__ __forceinline__ void splineq_f32(float dir, float r2, float twoh, float& a, float& b, float& c, float& d) {
+// SPLINEQ in FP32 with the reference's grouping (examples/GravityVisitor.h:37-80);
+// only the softened branch is called (out of line, rarely taken).
+__device__ __noinline__ void splineq_f32(float dir, float r2, float twoh, float& a, float& b, float& c, float& d) {
   if (r2 < twoh * twoh) {
     float dih = 2.0f / twoh;
     float u = dih / dir;
@@ -185,7 +193,11 @@ __device__ __forceinline__ void flush_p2p(MixWarp& w, const float4* __restrict__
   for (int cs = 0; cs < total; cs += 32) {
     if (cs + x.lane < total) {
       w.src[x.lane] = make_float4(nraw.x + noff.x, nraw.y + noff.y, nraw.z + noff.z, nraw.w);
-      if (!kFar) w.ssoft[x.lane] = nsoft;
+      if (!kFar) {
+        w.ssoft[x.lane] = nsoft;
+        const float rr = nsoft + (float)w.geom.soft_max;
+        w.sreach2[x.lane] = rr * rr;
+      }
     }
     __syncwarp();
     if (cs + 32 < total) fetch(cs + 32);
@@ -233,7 +245,15 @@ __device__ __forceinline__ void flush_p2p(MixWarp& w, const float4* __restrict__
         const float4 s = w.src[jj];
         const float dx = s.x - x.tx, dy = s.y - x.ty, dz = s.z - x.tz;
         const float r2 = dx * dx + dy * dy + dz * dz;
-        if (r2 > 0.f) {
+        if (r2 > w.sreach2[jj]) {  // r > soft_i + soft_j: Newtonian, and r > 0
+          const float rinv = rsqrtf(r2);
+          const float mr = s.w * rinv;
+          const float mr3 = mr * rinv * rinv;
+          x.pax += dx * mr3;
+          x.pay += dy * mr3;
+          x.paz += dz * mr3;
+          x.ppf -= mr;
+        } else if (r2 > 0.f) {
           const float rinv = rsqrtf(r2);
           float a, b;
           spline_f32(r2, rinv, w.ssoft[jj] + x.ts, a, b);
@@ -311,18 +331,9 @@ __device__ __forceinline__ void flush_p2c(MixWarp& w, int nent, const QuadRecF* 
     if (cs + 32 < nent) fetch(cs + 32);
     const int cnt = min(32, nent - cs);
     if (x.grp < x.G) {
-      float bx = 0.f, by = 0.f, bz = 0.f, bp = 0.f;  // second chain
-      int ee = x.grp;
-      for (; ee + x.G < cnt; ee += 2 * x.G) {
+      // one P2C term has enough independent work; a 2-way unroll measured slower
+      for (int ee = x.grp; ee < cnt; ee += x.G)
         p2c_term(w.qa[ee], w.qb[ee], w.qc[ee], x.tx, x.ty, x.tz, x.ts, x.pax, x.pay, x.paz, x.ppf);
-        const int e2 = ee + x.G;
-        p2c_term(w.qa[e2], w.qb[e2], w.qc[e2], x.tx, x.ty, x.tz, x.ts, bx, by, bz, bp);
-      }
-      if (ee < cnt) p2c_term(w.qa[ee], w.qb[ee], w.qc[ee], x.tx, x.ty, x.tz, x.ts, x.pax, x.pay, x.paz, x.ppf);
-      x.pax += bx;
-      x.pay += by;
-      x.paz += bz;
-      x.ppf += bp;
     }
     __syncwarp();
   }
