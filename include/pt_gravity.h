@@ -168,6 +168,32 @@ int pt_get_lists_size(pt_handle* h, int64_t* total);
 int pt_get_lists(pt_handle* h, int64_t* offsets, uint64_t* keys, int32_t* kinds);
 int pt_get_counters(pt_handle* h, pt_counters* c);
 
+/* Differentiation ---------------------------------------------------------
+ * No reference counterpart (ParaTreeT has no gradients).  All three need a
+ * force pass over every bucket with config.record_lists set, and work on its
+ * interaction lists: a "fixed interaction list" is the set of leaf() and
+ * node() interactions of each bucket that the pass recorded. */
+/* Re-evaluates the recorded lists in FP64 after replacing positions and/or
+ * masses (caller order, host; NULL keeps the current values) while keeping
+ * the tree topology and the lists: moments are recomputed, nothing is
+ * re-walked.  Results via pt_get_accel. */
+int pt_forces_frozen(pt_handle* h, const double* x, const double* y, const double* z, const double* m);
+/* Gradient of sum_i cot_i . a_i with respect to every position and mass for
+ * the recorded lists (FP64; tidal tensors through leaf() and node(), and the
+ * upward pass in closed form).  Host arrays in caller order. */
+int pt_adjoint(pt_handle* h, const double* cot_ax, const double* cot_ay, const double* cot_az, double* gx,
+               double* gy, double* gz, double* gm);
+/* Loss L = 0.5 sum_i |x_i(T) - y_i|^2 after nsteps leapfrog (KDK) steps of
+ * fixed dt from the handle's current particles, and its gradient with respect
+ * to the initial positions, velocities and masses.  (x, v) are checkpointed
+ * every ckpt_every steps (<= 0: round(sqrt(nsteps))); each segment is
+ * recomputed forward during the backward sweep.  Forces use the handle's
+ * precision, the adjoint is FP64.  Host arrays in caller order; any gradient
+ * pointer may be NULL.  The handle is left at the initial state. */
+int pt_chain_grad(pt_handle* h, int nsteps, double dt, int ckpt_every, const double* yx, const double* yy,
+                  const double* yz, double* loss, double* gx, double* gy, double* gz, double* gvx,
+                  double* gvy, double* gvz, double* gm);
+
 /* FP64 direct sum (the force-error yardstick) ------------------------------
  * Isolated spline-softened sum over all particles for nt caller indices,
  * the kernel of examples/GravityVisitor.h:87-120 with twoh = soft_i + soft_j. */

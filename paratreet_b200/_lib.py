@@ -93,6 +93,9 @@ SIGNATURES = {
     "pt_get_lists": (C.c_int, [_vp, _vp, _vp, _vp]),
     "pt_get_counters": (C.c_int, [_vp, C.POINTER(PtCounters)]),
     "pt_direct_sum": (C.c_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp]),
+    "pt_forces_frozen": (C.c_int, [_vp] + [_vp] * 4),
+    "pt_adjoint": (C.c_int, [_vp] + [_vp] * 7),
+    "pt_chain_grad": (C.c_int, [_vp, C.c_int, C.c_double, C.c_int] + [_vp] * 3 + [_vp] * 8),
     "pt_direct_sum_noalloc": (C.c_int, [_i64] + [_vp] * 5 + [_i64] + [_vp] * 6 + [C.c_char_p, C.c_size_t]),
 }
 

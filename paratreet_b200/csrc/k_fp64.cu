@@ -303,7 +303,7 @@ struct F64Eval {
     const QuadRec q = quad[node];
     n_pc += (unsigned long long)nt;
     if (record) {
-      if (lane == 0) { lnode[lbase + nlist] = node; lkind[lbase + nlist] = 1; }
+      if (lane == 0) { lnode[lbase + nlist] = node; lkind[lbase + nlist] = mono ? 2 : 1; }
       ++nlist;
     }
     if (w.count == 0) return;
@@ -426,6 +426,68 @@ __global__ void __launch_bounds__(kTravWarps * 32) traverse_f64(TravParams P, co
   }
 }
 
+// Frozen-list replay: evaluates each bucket's recorded interaction list (in the
+// recorded order, i.e. the walk's) with the FP64 evaluator, without walking.
+// Used to differentiate the force pass for a fixed interaction list.
+__global__ void __launch_bounds__(kTravWarps * 32) replay_f64(TravParams P) {
+  __shared__ double stage[kTravWarps][5 * 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  while (true) {
+    unsigned bi = 0;
+    if (lane == 0) bi = atomicAdd(P.work, 1u);
+    bi = __shfl_sync(kFull, bi, 0);
+    const int64_t b = P.b_begin + (int64_t)bi;
+    if (b >= P.b_end) break;
+    const int tnode = P.buckets[b];
+    const int tbase = P.walk[tnode].pstart, ntot = P.walk[tnode].pcount;
+    const int64_t e0 = P.list_off[b - P.b_begin], e1 = P.list_off[b - P.b_begin + 1];
+    for (int tc = 0; tc < ntot; tc += 32) {
+      const int t0 = tbase + tc, nt = min(32, ntot - tc);
+      F64Eval ev;
+      ev.p = &P.p;
+      ev.walk = P.walk;
+      ev.quad = P.quad;
+      ev.stage = stage[wid];
+      ev.lane = lane;
+      ev.nt = nt;
+      ev.xi = ev.yi = ev.zi = ev.si = 0.0;
+      if (lane < nt) {
+        ev.xi = P.p.x[t0 + lane];
+        ev.yi = P.p.y[t0 + lane];
+        ev.zi = P.p.z[t0 + lane];
+        ev.si = P.p.soft[t0 + lane];
+      }
+      ev.ax = ev.ay = ev.az = ev.pot = ev.potf = 0.0;
+      ev.ox = P.ox; ev.oy = P.oy; ev.oz = P.oz;
+      ev.g = nullptr;
+      ev.n_pp = 0; ev.n_pc = 0;
+      ev.record = 0;
+      ev.nlist = 0;
+      ev.lbase = 0;
+      ev.lnode = nullptr;
+      ev.lkind = nullptr;
+      for (int64_t e = e0; e < e1; e++) {
+        const int node = P.list_node[e];
+        const int kind = P.list_kind[e];
+        if (node < 0 || node >= P.nnodes) {
+          if (lane == 0) atomicOr(P.status, kErrCapacity);
+          continue;
+        }
+        if (kind == 0) ev.p2p(node);
+        else ev.p2c(node, kind == 2);
+      }
+      if (lane < nt) {
+        const int i = t0 + lane;
+        P.p.ax[i] = ev.ax;
+        P.p.ay[i] = ev.ay;
+        P.p.az[i] = ev.az;
+        P.p.pot[i] = ev.pot;
+        P.p.potf[i] = ev.potf;
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------- integrate
 // src/Particle.C:7-9 (kick) then :11-21 (perturb) for the same dt.
 __global__ void __launch_bounds__(256) kick_perturb(Particles p, int64_t n, double dt) {
@@ -520,6 +582,9 @@ void launch_finalize(Nodes nd, int64_t nnodes, double gfac, int want_f32, cudaSt
 }
 void launch_traverse_f64(const TravParams& P, const Mom* mom, int grid, cudaStream_t st) {
   traverse_f64<<<grid, kTravWarps * 32, 0, st>>>(P, mom);
+}
+void launch_replay_f64(const TravParams& P, int grid, cudaStream_t st) {
+  replay_f64<<<grid, kTravWarps * 32, 0, st>>>(P);
 }
 void launch_kick_perturb(Particles p, int64_t n, double dt, int grid, cudaStream_t st) {
   kick_perturb<<<grid, 256, 0, st>>>(p, n, dt);

@@ -73,6 +73,11 @@ struct pt_handle {
   bool forces_current = false;  // ... and the positions have not moved since
   bool trav_range_partial = false;
   int mixed_variant = 0;  // occupancy variant of the mixed traversal (PT_MIXED_VARIANT)
+
+  double* adj = nullptr;  // adjoint scratch: cotangent (3N) and gradients (4N), sorted + caller order
+  int64_t adj_cap = 0;
+  double* nadj = nullptr;  // 10 adjoint values per node
+  int64_t nadj_cap = 0;
 };
 
 namespace {
@@ -208,6 +213,7 @@ int read_status(pt_handle* h) {
     if (st & kErrBucketTooBig) m += " bucket larger than 32;";
     if (st & kErrListOverflow) m += " interaction list overflow;";
     if (st & kErrCapacity) m += " capacity exceeded;";
+    if (st & kErrAdjointSoftened) m += " adjoint met a softened quadrupole term (not differentiated);";
     return fail(h, (st & kErrNonFinite) ? PT_E_NONFINITE : PT_E_DEVICE, m);
   }
   return PT_OK;
@@ -539,7 +545,7 @@ int pt_destroy(pt_handle* h) {
   dfree(o.first_child); dfree(o.count); dfree(o.mom); dfree(o.walk); dfree(o.quad); dfree(o.quadf);
   dfree(o.fifo); dfree(o.nleaf_sub); dfree(o.nempty_sub); dfree(o.leaf_base); dfree(o.empty_base);
   dfree(h->flags); dfree(h->buckets); dfree(h->list_count); dfree(h->list_off); dfree(h->list_node);
-  dfree(h->list_kind); dfree(h->dsum);
+  dfree(h->list_kind); dfree(h->dsum); dfree(h->adj); dfree(h->nadj);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -775,7 +781,7 @@ int pt_get_lists(pt_handle* h, int64_t* offsets, uint64_t* keys, int32_t* kinds)
     for (int64_t i = 0; i <= nb; i++) offsets[i] = off[i];
   for (int64_t i = 0; i < tot; i++) {
     if (keys) keys[i] = nk[node[i]];
-    if (kinds) kinds[i] = kind[i];
+    if (kinds) kinds[i] = kind[i] ? 1 : 0;  // node() entries, softened or not, are kind 1
   }
   return PT_OK;
 }
@@ -829,3 +835,307 @@ int pt_direct_sum(pt_handle* h, int64_t nt, const int32_t* targets, double* ax, 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- differentiation
+namespace {
+
+int ensure_adjoint(pt_handle* h) {
+  const int64_t need = 14 * std::max<int64_t>(h->n, 1);
+  if (need > h->adj_cap) {
+    CKR(dalloc(h, &h->adj, need));
+    h->adj_cap = need;
+  }
+  const int64_t nneed = 10 * std::max<int64_t>(h->nnodes, 1);
+  if (nneed > h->nadj_cap) {
+    CKR(dalloc(h, &h->nadj, nneed));
+    h->nadj_cap = nneed;
+  }
+  return PT_OK;
+}
+
+bool lists_cover_all(const pt_handle* h) {
+  return h->lists_valid && !h->trav_range_partial && h->list_nb - 1 == h->nbuckets;
+}
+
+// Leaf moments, upward pass and traversal records on the existing topology.
+int recompute_moments(pt_handle* h) {
+  cudaStream_t st = h->stream;
+  launch_leaf_moments(h->nd, h->nnodes, h->p, st);
+  const int L = (int)h->lev.size() - 1;
+  for (int l = L - 1; l >= 0; l--) launch_upward_level(h->nd, h->lev[l], h->lev[l + 1] - h->lev[l], st);
+  const double gfac = (4.0 / 3.0) / (h->cfg.theta * h->cfg.theta);
+  launch_finalize(h->nd, h->nnodes, gfac, h->cfg.precision == PT_MIXED, st);
+  CK(cudaGetLastError());
+  return PT_OK;
+}
+
+// Gradient of sum_i cot_i . a_i for the recorded lists.  cot: caller order,
+// device; outputs: caller order, device (gx, gy, gz, gm; added into when
+// accumulate is set).
+int adjoint_device(pt_handle* h, const double* cx, const double* cy, const double* cz, double* gx, double* gy,
+                   double* gz, double* gm, bool accumulate) {
+  cudaStream_t st = h->stream;
+  const int64_t n = h->n;
+  const int g = grid_for(h, n);
+  CKR(ensure_adjoint(h));
+  double* cs = h->adj;       // 3N sorted cotangent
+  double* gs = h->adj + 3 * n;  // 4N sorted gradient
+  double* tmp = h->adj + 7 * n;  // 4N caller-order gradient
+  launch_gather_by_order(cx, cs, h->p.order, n, g, st);
+  launch_gather_by_order(cy, cs + n, h->p.order, n, g, st);
+  launch_gather_by_order(cz, cs + 2 * n, h->p.order, n, g, st);
+  CK(cudaMemsetAsync(gs, 0, 4 * n * sizeof(double), st));
+  CK(cudaMemsetAsync(h->nadj, 0, 10 * h->nnodes * sizeof(double), st));
+  CK(cudaMemsetAsync(h->d_work, 0, sizeof(unsigned), st));
+  AdjParams A{};
+  A.p = h->p;
+  A.walk = h->nd.walk;
+  A.quad = h->nd.quad;
+  A.mom = h->nd.mom;
+  A.parent = h->nd.parent;
+  A.buckets = h->buckets;
+  A.nbuckets = h->nbuckets;
+  A.nnodes = h->nnodes;
+  A.list_off = h->list_off;
+  A.list_node = h->list_node;
+  A.list_kind = h->list_kind;
+  A.cax = cs;
+  A.cay = cs + n;
+  A.caz = cs + 2 * n;
+  A.gx = gs;
+  A.gy = gs + n;
+  A.gz = gs + 2 * n;
+  A.gm = gs + 3 * n;
+  A.nadj = h->nadj;
+  A.work = h->d_work;
+  A.status = h->d_status;
+  launch_adjoint(A, h->sms * 8, st);
+  CK(cudaGetLastError());
+  double* outs[4] = {gx, gy, gz, gm};
+  for (int k = 0; k < 4; k++) {
+    if (!outs[k]) continue;
+    if (accumulate) {
+      launch_scatter_f64(gs + k * n, tmp + k * n, h->p.order, n, g, st);
+      launch_axpy1(n, 1.0, tmp + k * n, outs[k], g, st);
+    } else {
+      launch_scatter_f64(gs + k * n, outs[k], h->p.order, n, g, st);
+    }
+  }
+  CK(cudaGetLastError());
+  return read_status(h);
+}
+
+}  // namespace
+
+extern "C" {
+
+int pt_forces_frozen(pt_handle* h, const double* x, const double* y, const double* z, const double* m) {
+  if (!h) return PT_E_ARG;
+  if (!lists_cover_all(h)) return fail(h, PT_E_STATE, "needs a full force pass with config.record_lists");
+  cudaSetDevice(h->cfg.device);
+  cudaStream_t st = h->stream;
+  const int64_t n = h->n;
+  const int g = grid_for(h, n);
+  CKR(ensure_adjoint(h));
+  const double* src[4] = {x, y, z, m};
+  double* dst[4] = {h->p.x, h->p.y, h->p.z, h->p.m};
+  for (int k = 0; k < 4; k++) {
+    if (!src[k]) continue;
+    CK(cudaMemcpyAsync(h->adj, src[k], n * sizeof(double), cudaMemcpyHostToDevice, st));
+    launch_gather_by_order(h->adj, dst[k], h->p.order, n, g, st);
+  }
+  CKR(recompute_moments(h));
+  TravParams P{};
+  P.p = h->p;
+  P.walk = h->nd.walk;
+  P.quad = h->nd.quad;
+  P.buckets = h->buckets;
+  P.b_begin = 0;
+  P.b_end = h->nbuckets;
+  P.nnodes = h->nnodes;
+  P.list_off = h->list_off;
+  P.list_node = h->list_node;
+  P.list_kind = h->list_kind;
+  P.status = h->d_status;
+  P.work = h->d_work;
+  CK(cudaMemsetAsync(h->d_work, 0, sizeof(unsigned), st));
+  launch_replay_f64(P, h->sms * 16, st);
+  CK(cudaGetLastError());
+  return read_status(h);
+}
+
+int pt_adjoint(pt_handle* h, const double* cax, const double* cay, const double* caz, double* gx, double* gy,
+               double* gz, double* gm) {
+  if (!h || !cax || !cay || !caz) return PT_E_ARG;
+  if (!lists_cover_all(h)) return fail(h, PT_E_STATE, "needs a full force pass with config.record_lists");
+  cudaSetDevice(h->cfg.device);
+  cudaStream_t st = h->stream;
+  const int64_t n = h->n;
+  if (n == 0) return PT_OK;
+  CKR(ensure_adjoint(h));
+  double* buf = nullptr;  // caller-order cotangent (3N) and gradients (4N)
+  CK(cudaMalloc((void**)&buf, 7 * n * sizeof(double)));
+  const double* hin[3] = {cax, cay, caz};
+  for (int k = 0; k < 3; k++) {
+    CK(cudaMemcpyAsync(buf + k * n, hin[k], n * sizeof(double), cudaMemcpyHostToDevice, st));
+  }
+  int rc = adjoint_device(h, buf, buf + n, buf + 2 * n, buf + 3 * n, buf + 4 * n, buf + 5 * n, buf + 6 * n, false);
+  if (rc == PT_OK) {
+    double* hout[4] = {gx, gy, gz, gm};
+    for (int k = 0; k < 4; k++)
+      if (hout[k]) cudaMemcpyAsync(hout[k], buf + (3 + k) * n, n * sizeof(double), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+  }
+  cudaFree(buf);
+  return rc;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- K-step chain
+namespace {
+
+// Caller-order state -> particle arrays (order reset to identity).
+int load_state(pt_handle* h, const double* X, const double* V, const double* M, const double* S) {
+  const int64_t n = h->n;
+  const double* src[8] = {X, X + n, X + 2 * n, V, V + n, V + 2 * n, M, S};
+  return set_particles_impl(h, n, src, cudaMemcpyDeviceToDevice);
+}
+
+// Force pass with interaction lists; accelerations in caller order into A (3N).
+int chain_forces(pt_handle* h, double* A) {
+  const int saved = h->cfg.record_lists;
+  h->cfg.record_lists = 1;
+  const int rc = forces(h, 0, INT64_MAX);
+  h->cfg.record_lists = saved;
+  CKR(rc);
+  const int64_t n = h->n;
+  const int g = grid_for(h, n);
+  launch_scatter_f64(h->p.ax, A, h->p.order, n, g, h->stream);
+  launch_scatter_f64(h->p.ay, A + n, h->p.order, n, g, h->stream);
+  launch_scatter_f64(h->p.az, A + 2 * n, h->p.order, n, g, h->stream);
+  CK(cudaGetLastError());
+  return PT_OK;
+}
+
+struct DevBuf {
+  double* p = nullptr;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
+
+}  // namespace
+
+extern "C" int pt_chain_grad(pt_handle* h, int nsteps, double dt, int ckpt_every, const double* yx, const double* yy,
+                             const double* yz, double* loss, double* gx, double* gy, double* gz, double* gvx,
+                             double* gvy, double* gvz, double* gm) {
+  if (!h || nsteps < 1 || !(dt > 0.0) || !yx || !yy || !yz) return PT_E_ARG;
+  if (!h->p.x || h->n == 0) return fail(h, PT_E_STATE, "no particles");
+  cudaSetDevice(h->cfg.device);
+  cudaStream_t st = h->stream;
+  const int64_t n = h->n;
+  const int g = grid_for(h, n);
+  const int K = nsteps;
+  int C = ckpt_every > 0 ? ckpt_every : std::max(1, (int)std::lround(std::sqrt((double)K)));
+  if (C > K) C = K;
+  const int nck = (K + C - 1) / C;
+  // layout (doubles): X0 V0 M0 S0 | X V A | Y | xb vb mb pend | ckpt (nck x 6N) | seg ((C+1) x 3N)
+  const int64_t off_X0 = 0, off_V0 = 3 * n, off_M0 = 6 * n, off_S0 = 7 * n, off_X = 8 * n, off_V = 11 * n,
+                off_A = 14 * n, off_Y = 17 * n, off_xb = 20 * n, off_vb = 23 * n, off_mb = 26 * n, off_pd = 27 * n,
+                off_ck = 30 * n, off_seg = off_ck + (int64_t)nck * 6 * n;
+  const int64_t total = off_seg + (int64_t)(C + 1) * 3 * n;
+  DevBuf buf;
+  CK(cudaMalloc((void**)&buf.p, total * sizeof(double)));
+  double* B = buf.p;
+  double *X0 = B + off_X0, *V0 = B + off_V0, *M0 = B + off_M0, *S0 = B + off_S0, *X = B + off_X, *V = B + off_V,
+         *A = B + off_A, *Y = B + off_Y, *xb = B + off_xb, *vb = B + off_vb, *mb = B + off_mb, *pd = B + off_pd,
+         *ck = B + off_ck, *seg = B + off_seg;
+  // initial state in caller order (the arrays may be key-sorted by an earlier pass)
+  const double* cur[8] = {h->p.x, h->p.y, h->p.z, h->p.vx, h->p.vy, h->p.vz, h->p.m, h->p.soft};
+  double* dst0[8] = {X0, X0 + n, X0 + 2 * n, V0, V0 + n, V0 + 2 * n, M0, S0};
+  for (int k = 0; k < 8; k++) launch_scatter_f64(cur[k], dst0[k], h->p.order, n, g, st);
+  const double* hy[3] = {yx, yy, yz};
+  for (int k = 0; k < 3; k++) CK(cudaMemcpyAsync(Y + k * n, hy[k], n * sizeof(double), cudaMemcpyHostToDevice, st));
+  auto copy3 = [&](double* d, const double* s) {
+    return cudaMemcpyAsync(d, s, 3 * n * sizeof(double), cudaMemcpyDeviceToDevice, st);
+  };
+  // one KDK step from (X, V) with A = a(X) on entry; A = a(X') on exit
+  auto kdk = [&]() -> int {
+    launch_axpy3(n, 0.5 * dt, A, A + n, A + 2 * n, V, V + n, V + 2 * n, g, st);
+    launch_axpy3(n, dt, V, V + n, V + 2 * n, X, X + n, X + 2 * n, g, st);
+    CKR(load_state(h, X, V, M0, S0));
+    CKR(chain_forces(h, A));
+    launch_axpy3(n, 0.5 * dt, A, A + n, A + 2 * n, V, V + n, V + 2 * n, g, st);
+    return PT_OK;
+  };
+
+  // forward, keeping (X, V) every C steps
+  CK(copy3(X, X0));
+  CK(copy3(V, V0));
+  CKR(load_state(h, X, V, M0, S0));
+  CKR(chain_forces(h, A));
+  for (int s = 0; s < K; s++) {
+    if (s % C == 0) {
+      CK(copy3(ck + (int64_t)(s / C) * 6 * n, X));
+      CK(copy3(ck + (int64_t)(s / C) * 6 * n + 3 * n, V));
+    }
+    CKR(kdk());
+  }
+  // loss = 0.5 sum |x_K - y|^2 and its gradient
+  {
+    std::vector<double> hx(3 * n);
+    CK(cudaMemcpyAsync(hx.data(), X, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    double L = 0.0;
+    for (int k = 0; k < 3; k++)
+      for (int64_t i = 0; i < n; i++) {
+        const double d = hx[k * n + i] - hy[k][i];
+        L += d * d;
+      }
+    if (loss) *loss = 0.5 * L;
+  }
+  CK(copy3(xb, X));
+  launch_axpy3(n, -1.0, Y, Y + n, Y + 2 * n, xb, xb + n, xb + 2 * n, g, st);
+  CK(cudaMemsetAsync(vb, 0, 3 * n * sizeof(double), st));
+  CK(cudaMemsetAsync(mb, 0, n * sizeof(double), st));
+  CK(cudaMemsetAsync(pd, 0, 3 * n * sizeof(double), st));
+
+  // backward, segment by segment, recomputing each segment's positions
+  for (int c = nck - 1; c >= 0; c--) {
+    const int s0 = c * C, s1 = std::min(s0 + C, K);
+    CK(copy3(X, ck + (int64_t)c * 6 * n));
+    CK(copy3(V, ck + (int64_t)c * 6 * n + 3 * n));
+    CK(copy3(seg, X));
+    CKR(load_state(h, X, V, M0, S0));
+    CKR(chain_forces(h, A));
+    for (int s = s0; s < s1; s++) {
+      CKR(kdk());
+      CK(copy3(seg + (int64_t)(s + 1 - s0) * 3 * n, X));
+    }
+    for (int s = s1 - 1; s >= s0; s--) {
+      // the point x_{s+1}: a(x_{s+1}) feeds v_{s+1} (and v_h of step s+1, already in pd)
+      launch_axpy3(n, 0.5 * dt, vb, vb + n, vb + 2 * n, pd, pd + n, pd + 2 * n, g, st);
+      if (s + 1 < K) {
+        CKR(load_state(h, seg + (int64_t)(s + 1 - s0) * 3 * n, V, M0, S0));
+        CKR(chain_forces(h, A));
+        CKR(adjoint_device(h, pd, pd + n, pd + 2 * n, xb, xb + n, xb + 2 * n, mb, true));
+      }
+      // x_{s+1} = x_s + dt v_h ; v_h = v_s + dt/2 a(x_s)
+      launch_axpy3(n, dt, xb, xb + n, xb + 2 * n, vb, vb + n, vb + 2 * n, g, st);
+      CK(cudaMemsetAsync(pd, 0, 3 * n * sizeof(double), st));
+      launch_axpy3(n, 0.5 * dt, vb, vb + n, vb + 2 * n, pd, pd + n, pd + 2 * n, g, st);
+    }
+  }
+  // the point x_0
+  CKR(load_state(h, X0, V0, M0, S0));
+  CKR(chain_forces(h, A));
+  CKR(adjoint_device(h, pd, pd + n, pd + 2 * n, xb, xb + n, xb + 2 * n, mb, true));
+  double* hout[7] = {gx, gy, gz, gvx, gvy, gvz, gm};
+  const double* dsrc[7] = {xb, xb + n, xb + 2 * n, vb, vb + n, vb + 2 * n, mb};
+  for (int k = 0; k < 7; k++)
+    if (hout[k]) CK(cudaMemcpyAsync(hout[k], dsrc[k], n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  // leave the handle at the initial state (with its force pass)
+  return PT_OK;
+}

@@ -20,6 +20,7 @@ enum : unsigned {
   kErrBucketTooBig = 1u << 2,
   kErrListOverflow = 1u << 3,
   kErrCapacity = 1u << 4,
+  kErrAdjointSoftened = 1u << 5,
 };
 
 // Particle state, structure of arrays, FP64, in key-sorted order after a build.
@@ -110,6 +111,25 @@ struct TravParams {
   unsigned long long* counters;  // n_pp, n_pc, n_open
   unsigned int* work;     // dynamic bucket counter
   unsigned int* status;
+};
+
+// Inputs and outputs of the adjoint force pass (k_adjoint.cu).
+struct AdjParams {
+  Particles p;  // sorted positions, masses, softening
+  const WalkRec* walk;
+  const QuadRec* quad;
+  const Mom* mom;
+  const int32_t* parent;
+  const int32_t* buckets;
+  int64_t nbuckets, nnodes;
+  const int64_t* list_off;
+  const int32_t* list_node;
+  const int8_t* list_kind;
+  const double *cax, *cay, *caz;  // cotangent, sorted order
+  double *gx, *gy, *gz, *gm;      // particle adjoints, sorted order (zeroed)
+  double* nadj;                   // 10 per node: cm x/y/z, M, Qxx, Qyy, Qzz, Qxy, Qxz, Qyz (zeroed)
+  unsigned* work;
+  unsigned* status;
 };
 
 }  // namespace pt

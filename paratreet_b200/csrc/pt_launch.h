@@ -41,6 +41,7 @@ void launch_leaf_moments(Nodes nd, int64_t nnodes, Particles p, cudaStream_t st)
 void launch_upward_level(Nodes nd, int64_t begin, int64_t count, cudaStream_t st);
 void launch_finalize(Nodes nd, int64_t nnodes, double gfac, int want_f32, cudaStream_t st);
 void launch_traverse_f64(const TravParams& P, const Mom* mom, int grid, cudaStream_t st);
+void launch_replay_f64(const TravParams& P, int grid, cudaStream_t st);
 void launch_kick_perturb(Particles p, int64_t n, double dt, int grid, cudaStream_t st);
 void launch_kick_half(Particles p, int64_t n, double dt, int grid, cudaStream_t st);
 void launch_drift(Particles p, int64_t n, double dt, int grid, cudaStream_t st);
@@ -52,6 +53,9 @@ void launch_prep_sources(const int32_t* buckets, int64_t nbuckets, const WalkRec
                          float* softf, cudaStream_t st);
 void launch_traverse_mixed(const TravParams& P, const Mom* mom, int grid, int variant, cudaStream_t st);
 
+// k_adjoint.cu
+void launch_adjoint(const AdjParams& A, int grid, cudaStream_t st);
+
 // k_util.cu
 void launch_scatter_f64(const double* in, double* out, const int32_t* order, int64_t n, int grid, cudaStream_t st);
 void launch_scatter_u64(const uint64_t* in, uint64_t* out, const int32_t* order, int64_t n, int grid,
@@ -59,5 +63,10 @@ void launch_scatter_u64(const uint64_t* in, uint64_t* out, const int32_t* order,
 void launch_iota_i32(int32_t* out, int64_t n, int grid, cudaStream_t st);
 void launch_inverse_perm(const int32_t* order, int32_t* inv, int64_t n, int grid, cudaStream_t st);
 void launch_map_index(const int32_t* inv, const int32_t* in, int32_t* out, int64_t n, cudaStream_t st);
+void launch_axpy1(int64_t n, double alpha, const double* x, double* y, int grid, cudaStream_t st);
+void launch_axpy3(int64_t n, double alpha, const double* x0, const double* x1, const double* x2, double* y0,
+                  double* y1, double* y2, int grid, cudaStream_t st);
+void launch_gather_by_order(const double* in, double* out, const int32_t* order, int64_t n, int grid,
+                            cudaStream_t st);
 
 }  // namespace pt

@@ -178,6 +178,7 @@ __device__ __forceinline__ bool walk_bucket(const WalkRec* __restrict__ walk, in
 }
 
 // Evaluator that only records / counts the interaction list of a bucket.
+// Stored kinds: 0 leaf() P2P, 1 node() quadrupole, 2 node() softened monopole.
 struct ListRecorder {
   int lane;
   int mode;  // 1 count, 2 record
@@ -189,8 +190,8 @@ struct ListRecorder {
     if (mode == 2 && lane == 0) { node_out[base + n] = node; kind_out[base + n] = 0; }
     ++n;
   }
-  __device__ void p2c(int node, bool) {
-    if (mode == 2 && lane == 0) { node_out[base + n] = node; kind_out[base + n] = 1; }
+  __device__ void p2c(int node, bool mono) {
+    if (mode == 2 && lane == 0) { node_out[base + n] = node; kind_out[base + n] = mono ? 2 : 1; }
     ++n;
   }
 };

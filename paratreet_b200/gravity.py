@@ -232,3 +232,29 @@ class GravitySimulation:
         out = [np.empty(t.size) for _ in range(4)]
         self._check(self._lib.pt_direct_sum(self._h, t.size, L.ptr(t), *[L.ptr(o) for o in out]))
         return out
+
+    # -- differentiation (needs record_lists) --------------------------------
+    def forces_frozen(self, x=None, y=None, z=None, m=None):
+        """Re-evaluate the recorded interaction lists (FP64) with new positions /
+        masses on the same tree; returns accelerations like accelerations()."""
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, m)]
+        self._check(self._lib.pt_forces_frozen(self._h, *[L.ptr(a) for a in arrs]))
+        return self.accelerations()
+
+    def adjoint(self, cax, cay, caz):
+        """Gradient of sum_i cot_i . a_i w.r.t. positions and masses (fixed lists)."""
+        c = [np.ascontiguousarray(a, dtype=np.float64) for a in (cax, cay, caz)]
+        out = [np.empty(self.n) for _ in range(4)]
+        self._check(self._lib.pt_adjoint(self._h, *[L.ptr(a) for a in c], *[L.ptr(o) for o in out]))
+        return {"gx": out[0], "gy": out[1], "gz": out[2], "gm": out[3]}
+
+    def chain_grad(self, nsteps: int, dt: float, targets, ckpt_every: int = 0):
+        """Loss 0.5 sum |x(T) - y|^2 after nsteps KDK steps and its gradient w.r.t.
+        the initial positions, velocities and masses (checkpointed adjoint)."""
+        y = [np.ascontiguousarray(t, dtype=np.float64) for t in targets]
+        out = [np.empty(self.n) for _ in range(7)]
+        loss = C.c_double()
+        self._check(self._lib.pt_chain_grad(self._h, int(nsteps), float(dt), int(ckpt_every),
+                                            *[L.ptr(a) for a in y], C.byref(loss), *[L.ptr(o) for o in out]))
+        keys = ("gx", "gy", "gz", "gvx", "gvy", "gvz", "gm")
+        return loss.value, dict(zip(keys, out))
