@@ -69,6 +69,8 @@ def _port_lib():
         lib.pto_forces.argtypes = [C.c_void_p, C.c_int]
         lib.pto_run.argtypes = [C.c_void_p, C.c_int]
         lib.pto_direct.argtypes = [C.c_int] + [_dp] * 5 + [C.c_int, _i32p] + [_dp] * 4 + [C.c_int]
+        lib.pto_set_periodic.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_double, C.c_double]
+        lib.pto_ewald_direct.argtypes = [C.c_int] + [_dp] * 5 + [C.c_double, C.c_int, _i32p] + [_dp] * 4 + [C.c_int]
         _port = lib
     return _port
 
@@ -82,6 +84,7 @@ def _ref_lib():
         lib.ptref_run.argtypes = [C.c_void_p, C.c_int]
         lib.ptref_set_record_lists.argtypes = [C.c_void_p, C.c_int]
         lib.ptref_forces_sample.argtypes = [C.c_void_p, C.c_double] + [C.POINTER(C.c_double)] * 3
+        lib.ptref_set_periodic.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int]
         _ref = lib
     return _ref
 
@@ -181,6 +184,10 @@ class PortSim(_Sim):
         h = lib.pto_create(n, *_arrs(p), bucket, theta, dt_max, threads)
         super().__init__(lib, h, n)
 
+    def set_periodic(self, period=1.0, n_replicas=1, rcut=2.6, hcut=2.8):
+        """Periodic cube: replica walks plus the Ewald correction."""
+        self._lib.pto_set_periodic(self._h, 1, period, n_replicas, rcut, hcut)
+
     def forces(self, record_lists=False):
         self._lib.pto_forces(self._h, 1 if record_lists else 0)
 
@@ -202,6 +209,10 @@ class RefSim(_Sim):
         n = p["x"].size
         h = lib.ptref_create(n, *_arrs(p), bucket, theta, dt_max, group, threads)
         super().__init__(lib, h, n)
+
+    def set_periodic(self, period=1.0, n_replicas=1):
+        """Periodic cube (the reference's fEwCut 2.6 and |h| <= 2.8)."""
+        self._lib.ptref_set_periodic(self._h, 1, period, n_replicas)
 
     def forces(self, record_lists=False):
         self._lib.ptref_set_record_lists(self._h, 1 if record_lists else 0)
@@ -231,6 +242,16 @@ def direct_sum(p: dict, targets: np.ndarray, threads: int = 1):
     out = [np.zeros(t.size) for _ in range(4)]
     a = _arrs(p)
     lib.pto_direct(p["x"].size, a[0], a[1], a[2], a[6], a[7], t.size, t, *out, threads)
+    return out
+
+
+def ewald_direct_sum(p: dict, targets: np.ndarray, period: float = 1.0, threads: int = 1):
+    """FP64 periodic (Ewald) direct sum at the given target indices."""
+    lib = _port_lib()
+    t = np.ascontiguousarray(targets, dtype=np.int32)
+    out = [np.zeros(t.size) for _ in range(4)]
+    a = _arrs(p)
+    lib.pto_ewald_direct(p["x"].size, a[0], a[1], a[2], a[6], a[7], period, t.size, t, *out, threads)
     return out
 
 

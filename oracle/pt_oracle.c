@@ -21,6 +21,9 @@
 #endif
 
 #define PTO_MAX_DEPTH 21 /* 63 key bits / 3 */
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
 
 typedef struct {
   double mass, cm[3], soft, radius;
@@ -52,6 +55,9 @@ struct pto_sim {
   long list_total, list_cap;
   unsigned long long n_pp, n_pc, n_open;
   double t_build, t_trav;
+  /* periodic cube (examples/Gravity.C:34-50, examples/Ewald.{h,C}) */
+  int periodic, n_replicas;
+  double period, ewald_rcut, ewald_hcut;
 };
 
 static double wall(void) {
@@ -461,34 +467,35 @@ static int box_sphere(const double lo[3], const double hi[3], const double c[3],
 }
 
 /* GravityVisitor::open, :162-182 (non-HEXADECAPOLE :180). */
-static int visit_open(const pto_sim* s, const pto_mom* src, const pto_mom* tgt, double gfac) {
+static int visit_open(const pto_mom* src, const pto_mom* tgt, double gfac, const double off[3]) {
   if (src->count <= 6) return 1;
   double rsq = src->radius * src->radius * gfac;
-  return box_sphere(tgt->lo, tgt->hi, src->cm, rsq);
-  (void)s;
+  double c[3] = {src->cm[0] + off[0], src->cm[1] + off[1], src->cm[2] + off[2]};
+  return box_sphere(tgt->lo, tgt->hi, c, rsq);
 }
 
 /* GravityVisitor::openSoftening, :122-128. */
-static int open_softening(const pto_mom* src, const pto_mom* tgt) {
+static int open_softening(const pto_mom* src, const pto_mom* tgt, const double off[3]) {
   double r1 = 2.0 * src->soft, r2 = 2.0 * tgt->soft;
-  double dx = src->cm[0] - tgt->cm[0], dy = src->cm[1] - tgt->cm[1], dz = src->cm[2] - tgt->cm[2];
+  double c[3] = {src->cm[0] + off[0], src->cm[1] + off[1], src->cm[2] + off[2]};
+  double dx = c[0] - tgt->cm[0], dy = c[1] - tgt->cm[1], dz = c[2] - tgt->cm[2];
   double rs = r1 + r2;
   if (dx * dx + dy * dy + dz * dz <= rs * rs) return 1;
-  return box_sphere(tgt->lo, tgt->hi, src->cm, r1 * r1);
+  return box_sphere(tgt->lo, tgt->hi, c, r1 * r1);
 }
 
 /* GravityVisitor::leaf, :144-160 -- P2P; the per-source-leaf sum is formed
  * first and then added (applyAcceleration).  pot_full additionally sums
  * -m_j * a (the reference's leaf() does not touch the potential). */
-static void visit_leaf(pto_sim* s, int src, int tgt) {
+static void visit_leaf(pto_sim* s, int src, int tgt, const double off[3]) {
   int s0 = s->npstart[src], sn = s->nnp[src];
   int t0 = s->npstart[tgt], tn = s->nnp[tgt];
   for (int i = t0; i < t0 + tn; i++) {
     double ax = 0.0, ay = 0.0, az = 0.0, pf = 0.0;
     for (int j = s0; j < s0 + sn; j++) {
-      double dx = (s->x[j] + 0.0) - s->x[i];
-      double dy = (s->y[j] + 0.0) - s->y[i];
-      double dz = (s->z[j] + 0.0) - s->z[i];
+      double dx = (s->x[j] + off[0]) - s->x[i];
+      double dy = (s->y[j] + off[1]) - s->y[i];
+      double dz = (s->z[j] + off[2]) - s->z[i];
       double rsq = dx * dx + dy * dy + dz * dz;
       double twoh = s->soft[j] + s->soft[i];
       if (rsq != 0) {
@@ -510,16 +517,16 @@ static void visit_leaf(pto_sim* s, int src, int tgt) {
 
 /* GravityVisitor::node, :184-224 (non-HEXADECAPOLE :207-221), with the
  * unsoftened monopole fallback addGravity, :130-139. */
-static void visit_node(pto_sim* s, int src, int tgt) {
+static void visit_node(pto_sim* s, int src, int tgt, const double off[3]) {
   const pto_mom* q = &s->mom[src];
   const pto_mom* t = &s->mom[tgt];
   if (q->count == 0) return;
   int t0 = s->npstart[tgt], tn = s->nnp[tgt];
-  if (open_softening(q, t)) {
+  if (open_softening(q, t, off)) {
     for (int i = t0; i < t0 + tn; i++) {
-      double dx = (q->cm[0] + 0.0) - s->x[i];
-      double dy = (q->cm[1] + 0.0) - s->y[i];
-      double dz = (q->cm[2] + 0.0) - s->z[i];
+      double dx = (q->cm[0] + off[0]) - s->x[i];
+      double dy = (q->cm[1] + off[1]) - s->y[i];
+      double dz = (q->cm[2] + off[2]) - s->z[i];
       double rsq = dx * dx + dy * dy + dz * dz;
       if (rsq != 0) {
         double f = q->mass / (rsq * sqrt(rsq));
@@ -532,9 +539,9 @@ static void visit_node(pto_sim* s, int src, int tgt) {
     return;
   }
   for (int i = t0; i < t0 + tn; i++) {
-    double rx = (s->x[i] - q->cm[0]) - 0.0;
-    double ry = (s->y[i] - q->cm[1]) - 0.0;
-    double rz = (s->z[i] - q->cm[2]) - 0.0;
+    double rx = (s->x[i] - q->cm[0]) - off[0];
+    double ry = (s->y[i] - q->cm[1]) - off[1];
+    double rz = (s->z[i] - q->cm[2]) - off[2];
     double rsq = rx * rx + ry * ry + rz * rz;
     double dir = 1.0 / sqrt(rsq);
     double twoh = q->soft + s->soft[i];
@@ -555,6 +562,110 @@ static void visit_node(pto_sim* s, int src, int tgt) {
   }
 }
 
+/* EwaldData::EwaldInit (examples/Ewald.C:80-163) and LeafEwaldFn
+ * (examples/Ewald.h:3-199), non-HEXADECAPOLE branch, restated: the root
+ * cell's monopole + quadrupole summed over real-space images (erfc; -erf for
+ * images inside the replica hole, which the tree walked) and over the
+ * reciprocal table; alpha = 2/L. */
+typedef struct { double h[3], c; } pto_ewt;
+
+static void ewald_correction(pto_sim* s) {
+  const pto_mom* R = &s->mom[0];
+  const double L = s->period;
+  const int hReps = (int)ceil(s->ewald_hcut);
+  const double alpha = 2.0 / L, alpha2 = alpha * alpha;
+  const double k4 = M_PI * M_PI / (alpha * alpha * L * L);
+  int cap = (2 * hReps + 1) * (2 * hReps + 1) * (2 * hReps + 1), nh = 0;
+  pto_ewt* ewt = (pto_ewt*)malloc(sizeof(pto_ewt) * (size_t)cap);
+  for (int hx = -hReps; hx <= hReps; ++hx)
+    for (int hy = -hReps; hy <= hReps; ++hy)
+      for (int hz = -hReps; hz <= hReps; ++hz) {
+        int h2 = hx * hx + hy * hy + hz * hz;
+        if (h2 == 0 || h2 > s->ewald_hcut * s->ewald_hcut) continue;
+        double g0 = exp(-k4 * h2) / (M_PI * h2 * L);
+        double g1 = 2 * M_PI / L * g0;
+        double g2 = -2 * M_PI / L * g1;
+        double qx = (1.0 / 1.0) * (R->xz * hz + R->xy * hy + R->xx * hx);
+        double qy = (1.0 / 1.0) * (R->yz * hz + R->xy * hx + R->yy * hy);
+        double qz = (1.0 / 1.0) * (R->yz * hy + R->xz * hx + R->zz * hz);
+        double qm = (1.0 / 2.0) * (qx * hx + qy * hy + qz * hz);
+        double c = 0.0;
+        c -= g2 * qm;
+        c -= g0 * R->mass;
+        ewt[nh].h[0] = 2 * M_PI / L * hx;
+        ewt[nh].h[1] = 2 * M_PI / L * hy;
+        ewt[nh].h[2] = 2 * M_PI / L * hz;
+        ewt[nh].c = c;
+        nh++;
+      }
+  const double Q2 = 0.5 * (R->xx + R->yy + R->zz);
+  int nEw = (int)ceil(s->ewald_rcut);
+  if (s->n_replicas > nEw) nEw = s->n_replicas;
+  const double cut2 = s->ewald_rcut * s->ewald_rcut * L * L, inner2 = 1.2e-3 * L * L;
+  const double k1 = M_PI / (alpha2 * L * L * L), ka = 2.0 * alpha / sqrt(M_PI);
+  const int nr = s->n_replicas;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) num_threads(s->threads)
+#endif
+  for (int i = 0; i < s->n; i++) {
+    double pot = R->mass * k1, ax = 0.0, ay = 0.0, az = 0.0;
+    double dx = s->x[i] - R->cm[0], dy = s->y[i] - R->cm[1], dz = s->z[i] - R->cm[2];
+    for (int ix = -nEw; ix <= nEw; ++ix)
+      for (int iy = -nEw; iy <= nEw; ++iy)
+        for (int iz = -nEw; iz <= nEw; ++iz) {
+          int hole = ix >= -nr && ix <= nr && iy >= -nr && iy <= nr && iz >= -nr && iz <= nr;
+          double x = dx + ix * L, y = dy + iy * L, z = dz + iz * L;
+          double r2 = x * x + y * y + z * z, g0, g1, g2, g3;
+          if (r2 > cut2 && !hole) continue;
+          if (r2 < inner2) {
+            double an = ka;
+            r2 *= alpha2;
+            g0 = an * ((1.0 / 3.0) * r2 - 1.0);
+            an *= 2 * alpha2;
+            g1 = an * ((1.0 / 5.0) * r2 - (1.0 / 3.0));
+            an *= 2 * alpha2;
+            g2 = an * ((1.0 / 7.0) * r2 - (1.0 / 5.0));
+            an *= 2 * alpha2;
+            g3 = an * ((1.0 / 9.0) * r2 - (1.0 / 7.0));
+          } else {
+            double dir = 1 / sqrt(r2), dir2 = dir * dir;
+            double a = exp(-r2 * alpha2);
+            a *= ka * dir2;
+            g0 = hole ? -erf(alpha / dir) : erfc(alpha / dir);
+            g0 *= dir;
+            g1 = g0 * dir2 + a;
+            double an = 2 * alpha2;
+            g2 = 3 * g1 * dir2 + an * a;
+            an *= 2 * alpha2;
+            g3 = 5 * g2 * dir2 + an * a;
+          }
+          double mx = R->xx * x + R->xy * y + R->xz * z;
+          double my = R->xy * x + R->yy * y + R->yz * z;
+          double mz = R->xz * x + R->yz * y + R->zz * z;
+          double mir = 0.5 * (mx * x + my * y + mz * z);
+          double qta = g1 * R->mass - g2 * Q2 + g3 * mir;
+          pot -= g0 * R->mass - g1 * Q2 + g2 * mir;
+          ax += g2 * (mx) - x * qta;
+          ay += g2 * (my) - y * qta;
+          az += g2 * (mz) - z * qta;
+        }
+    for (int h = 0; h < nh; ++h) {
+      double hx = ewt[h].h[0] * dx + ewt[h].h[1] * dy + ewt[h].h[2] * dz;
+      double c = cos(hx), sn = sin(hx);
+      pot += ewt[h].c * c;
+      ax += ewt[h].h[0] * (ewt[h].c * sn);
+      ay += ewt[h].h[1] * (ewt[h].c * sn);
+      az += ewt[h].h[2] * (ewt[h].c * sn);
+    }
+    s->pot[i] += pot;
+    s->potf[i] += pot;
+    s->ax[i] += ax;
+    s->ay[i] += ay;
+    s->az[i] += az;
+  }
+  free(ewt);
+}
+
 static void list_push(pto_sim* s, uint64_t key, int kind) {
   if (s->list_total == s->list_cap) {
     s->list_cap = s->list_cap ? 2 * s->list_cap : 4096;
@@ -569,7 +680,7 @@ static void list_push(pto_sim* s, uint64_t key, int kind) {
 /* src/Traverser.h:154-217 for one bucket: pre-order DFS; Leaf -> leaf()
  * (self included, CallSelfLeaf), Internal -> open() ? children : node(),
  * EmptyLeaf -> nothing. */
-static void walk(pto_sim* s, int tgt, double gfac, int record, unsigned long long* cnt) {
+static void walk(pto_sim* s, int tgt, double gfac, int record, unsigned long long* cnt, const double off[3]) {
   int stack[8 * (PTO_MAX_DEPTH + 2)];
   int sp = 0;
   stack[sp++] = 0;
@@ -577,16 +688,16 @@ static void walk(pto_sim* s, int tgt, double gfac, int record, unsigned long lon
     int nd = stack[--sp];
     int ty = s->ntype[nd];
     if (ty == PTO_LEAF) {
-      visit_leaf(s, nd, tgt);
+      visit_leaf(s, nd, tgt, off);
       cnt[0] += (unsigned long long)s->nnp[nd] * (unsigned long long)s->nnp[tgt];
       if (record) list_push(s, s->nkey[nd], 0);
     } else if (ty == PTO_INTERNAL) {
       cnt[2]++;
-      if (visit_open(s, &s->mom[nd], &s->mom[tgt], gfac)) {
+      if (visit_open(&s->mom[nd], &s->mom[tgt], gfac, off)) {
         int c0 = s->nchild[nd];
         for (int c = 7; c >= 0; c--) stack[sp++] = c0 + c;
       } else {
-        visit_node(s, nd, tgt);
+        visit_node(s, nd, tgt, off);
         cnt[1] += (unsigned long long)s->nnp[tgt];
         if (record) list_push(s, s->nkey[nd], 1);
       }
@@ -602,6 +713,7 @@ static void traverse(pto_sim* s, int record) {
   memset(s->pot, 0, sizeof(double) * s->n);
   memset(s->potf, 0, sizeof(double) * s->n);
   unsigned long long pp = 0, pc = 0, op = 0;
+  const double zero[3] = {0.0, 0.0, 0.0};
   if (record) {
     free(s->list_off);
     s->list_off = (long*)malloc(sizeof(long) * (s->nleaves + 1));
@@ -609,19 +721,27 @@ static void traverse(pto_sim* s, int record) {
     for (long b = 0; b < s->nleaves; b++) {
       unsigned long long c[3] = {0, 0, 0};
       s->list_off[b] = s->list_total;
-      walk(s, s->leaves[b], gfac, 1, c);
+      walk(s, s->leaves[b], gfac, 1, c, zero);
       pp += c[0]; pc += c[1]; op += c[2];
     }
     s->list_off[s->nleaves] = s->list_total;
   } else {
+    /* examples/Gravity.C:32-46: one walk, or (2n+1)^3 replica walks */
+    const int nr = s->periodic ? s->n_replicas : 0;
+    for (int X = -nr; X <= nr; X++)
+      for (int Y = -nr; Y <= nr; Y++)
+        for (int Z = -nr; Z <= nr; Z++) {
+          const double off[3] = {X * s->period, Y * s->period, Z * s->period};
 #ifdef _OPENMP
 #pragma omp parallel for schedule(dynamic, 16) reduction(+ : pp, pc, op) num_threads(s->threads)
 #endif
-    for (long b = 0; b < s->nleaves; b++) {
-      unsigned long long c[3] = {0, 0, 0};
-      walk(s, s->leaves[b], gfac, 0, c);
-      pp += c[0]; pc += c[1]; op += c[2];
-    }
+          for (long b = 0; b < s->nleaves; b++) {
+            unsigned long long c[3] = {0, 0, 0};
+            walk(s, s->leaves[b], gfac, 0, c, s->periodic ? off : zero);
+            pp += c[0]; pc += c[1]; op += c[2];
+          }
+        }
+    if (s->periodic) ewald_correction(s);
   }
   s->n_pp = pp;
   s->n_pc = pc;
@@ -633,6 +753,14 @@ static double* dup_d(const double* a, int n) {
   double* p = (double*)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
   if (n > 0) memcpy(p, a, sizeof(double) * (size_t)n);
   return p;
+}
+
+void pto_set_periodic(pto_sim* s, int periodic, double L, int n_replicas, double rcut, double hcut) {
+  s->periodic = periodic;
+  s->period = L;
+  s->n_replicas = n_replicas;
+  s->ewald_rcut = rcut;
+  s->ewald_hcut = hcut;
 }
 
 pto_sim* pto_create(int n, const double* x, const double* y, const double* z, const double* vx,
@@ -818,4 +946,93 @@ void pto_direct(int n, const double* x, const double* y, const double* z, const 
     ax[t] = sx; ay[t] = sy; az[t] = sz; pot[t] = sp;
   }
   (void)threads;
+}
+
+/* FP64 periodic (Ewald) direct sum with the spline kernel for the nearest
+ * image within soft_i + soft_j: alpha = 4/L, real-space images within 1.5 L,
+ * reciprocal |h|^2 <= 64, background and self terms in the potential. */
+void pto_ewald_direct(int n, const double* x, const double* y, const double* z, const double* m,
+                      const double* soft, double L, int nt, const int* targets, double* ax, double* ay,
+                      double* az, double* pot, int threads) {
+  const double V = L * L * L, alpha = 4.0 / L, rc = 1.5 * L, rc2 = rc * rc;
+  const double ka = 2.0 * alpha / sqrt(M_PI);
+  const int hmax = 8, nimg = 2;
+  int cap = (2 * hmax + 1) * (2 * hmax + 1) * (2 * hmax + 1), nk = 0;
+  double* kv = (double*)malloc(sizeof(double) * 4 * (size_t)cap);
+  for (int hx = -hmax; hx <= hmax; hx++)
+    for (int hy = -hmax; hy <= hmax; hy++)
+      for (int hz = -hmax; hz <= hmax; hz++) {
+        int h2 = hx * hx + hy * hy + hz * hz;
+        if (h2 == 0 || h2 > hmax * hmax) continue;
+        double kx = 2 * M_PI / L * hx, ky = 2 * M_PI / L * hy, kz = 2 * M_PI / L * hz;
+        double k2 = kx * kx + ky * ky + kz * kz;
+        kv[4 * nk] = kx; kv[4 * nk + 1] = ky; kv[4 * nk + 2] = kz;
+        kv[4 * nk + 3] = 4 * M_PI / V * exp(-k2 / (4 * alpha * alpha)) / k2;
+        nk++;
+      }
+  double* S = (double*)calloc(2 * (size_t)nk, sizeof(double));
+  double M = 0.0;
+  for (int j = 0; j < n; j++) M += m[j];
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) num_threads(threads > 0 ? threads : 1)
+#endif
+  for (int k = 0; k < nk; k++) {
+    double sc = 0.0, ss = 0.0;
+    for (int j = 0; j < n; j++) {
+      double ph = kv[4 * k] * x[j] + kv[4 * k + 1] * y[j] + kv[4 * k + 2] * z[j];
+      sc += m[j] * cos(ph);
+      ss += m[j] * sin(ph);
+    }
+    S[2 * k] = sc;
+    S[2 * k + 1] = ss;
+  }
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 4) num_threads(threads > 0 ? threads : 1)
+#endif
+  for (int t = 0; t < nt; t++) {
+    int i = targets[t];
+    double sx = 0.0, sy = 0.0, sz = 0.0, sp = 0.0;
+    for (int j = 0; j < n; j++) {
+      double d0x = x[j] - x[i], d0y = y[j] - y[i], d0z = z[j] - z[i];
+      d0x -= L * rint(d0x / L);
+      d0y -= L * rint(d0y / L);
+      d0z -= L * rint(d0z / L);
+      for (int a = -nimg; a <= nimg; a++)
+        for (int b = -nimg; b <= nimg; b++)
+          for (int c = -nimg; c <= nimg; c++) {
+            double dx = d0x + a * L, dy = d0y + b * L, dz = d0z + c * L;
+            double r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 > rc2 || r2 == 0.0) continue;
+            double r = sqrt(r2), ec = erfc(alpha * r);
+            double f = (ec + ka * r * exp(-alpha * alpha * r2)) / (r2 * r);
+            sx += m[j] * f * dx;
+            sy += m[j] * f * dy;
+            sz += m[j] * f * dz;
+            sp -= m[j] * ec / r;
+          }
+      double r2 = d0x * d0x + d0y * d0y + d0z * d0z, twoh = soft[j] + soft[i];
+      if (r2 != 0.0 && r2 < twoh * twoh) {
+        double a, b, r = sqrt(r2);
+        spline(r2, twoh, &a, &b);
+        double corr = b - 1.0 / (r2 * r);
+        sx += m[j] * corr * d0x;
+        sy += m[j] * corr * d0y;
+        sz += m[j] * corr * d0z;
+        sp -= m[j] * (a - 1.0 / r);
+      }
+    }
+    sp += M_PI * M / (alpha * alpha * V) + ka * m[i];
+    for (int k = 0; k < nk; k++) {
+      double ph = kv[4 * k] * x[i] + kv[4 * k + 1] * y[i] + kv[4 * k + 2] * z[i];
+      double sn = sin(ph), cs = cos(ph), w = kv[4 * k + 3];
+      double f = w * (sn * S[2 * k] - cs * S[2 * k + 1]);
+      sx -= f * kv[4 * k];
+      sy -= f * kv[4 * k + 1];
+      sz -= f * kv[4 * k + 2];
+      sp -= w * (cs * S[2 * k] + sn * S[2 * k + 1]);
+    }
+    ax[t] = sx; ay[t] = sy; az[t] = sz; pot[t] = sp;
+  }
+  free(kv);
+  free(S);
 }

@@ -46,6 +46,14 @@ void pto_get_bucket_keys(const pto_sim* s, uint64_t* keys);
 long pto_list_total(const pto_sim* s);
 void pto_get_lists(const pto_sim* s, long* offsets, uint64_t* keys, int* kinds);
 
+/* Periodic cube of side L: (2n+1)^3 replica walks and the reference's Ewald
+ * correction with real-space radius rcut*L and reciprocal cut |h| <= hcut. */
+void pto_set_periodic(pto_sim* s, int periodic, double L, int n_replicas, double rcut, double hcut);
+/* FP64 periodic (Ewald) direct sum; see pt_oracle.c. */
+void pto_ewald_direct(int n, const double* x, const double* y, const double* z, const double* m,
+                      const double* soft, double L, int nt, const int* targets, double* ax, double* ay,
+                      double* az, double* pot, int threads);
+
 /* FP64 direct sum (spline softening, twoh = soft_i + soft_j, G = 1) over
  * all n sources for nt target indices; isolated (no periodic images). */
 void pto_direct(int n, const double* x, const double* y, const double* z, const double* m,

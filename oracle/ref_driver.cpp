@@ -25,6 +25,11 @@
  *                     per Partition (src/Partition.h:129-134)
  *   step              src/Driver.h:183-251: forces -> kick -> perturb ->
  *                     new universe -> rekey; dt from examples/Gravity.C:63-67
+ *   periodic          examples/Gravity.C:19-50: EwaldInit on the root's data
+ *                     (examples/Ewald.C, compiled in ref_ewald.cpp), the
+ *                     (2n+1)^3 replica walks with GravityVisitor offsets, then
+ *                     the reference's own LeafEwaldFn (examples/Ewald.h) per
+ *                     leaf
  *
  * Deviation for degenerate input only: a node at depth 21 (all 63 key bits
  * used) is made a Leaf even when it holds more than `bucket` particles (the
@@ -49,6 +54,23 @@
 #include "CentroidData.h"
 #include "Node.h"
 #include "GravityVisitor.h"
+#include "EwaldData.h"
+
+// Readonly globals of examples/Main.C that Ewald.{h,C} read.
+Vector3D<Real> fPeriod(1.0, 1.0, 1.0);
+int nReplicas = 0;
+
+// ewaldProxy.ckLocalBranch() of the single-process run: the EwaldData that
+// EwaldInit filled.
+struct CProxy_EwaldData {
+  EwaldData* local = nullptr;
+  EwaldData* ckLocalBranch() const { return local; }
+};
+CProxy_EwaldData ewaldProxy;
+template <typename D>
+struct Partition;
+#define PARATREET_REGISTER_PER_LEAF_FN(name, data, fn) static auto name = fn;
+#include "Ewald.h"
 
 namespace {
 
@@ -71,6 +93,9 @@ struct RefSim {
   int group = 64;
   int record_lists = 0;
   int threads = 1;
+  int periodic = 0;
+  double period = 1.0;
+  int n_replicas = 0;
   // state
   std::vector<Particle> particles;  // sorted by key after each build
   OrientedBox<Real> universe;
@@ -180,8 +205,8 @@ struct GroupTrav {
   GravityVisitor v;
   size_t b0, nb;
   unsigned long long pp = 0, pc = 0, op = 0;
-  GroupTrav(RefSim& sim, size_t b0_, size_t nb_)
-      : s(sim), v(Vector3D<Real>(0, 0, 0), sim.theta), b0(b0_), nb(nb_) {}
+  GroupTrav(RefSim& sim, size_t b0_, size_t nb_, Vector3D<Real> offset = Vector3D<Real>(0, 0, 0))
+      : s(sim), v(offset, sim.theta), b0(b0_), nb(nb_) {}
 
   void recurse(RNode* node, const std::vector<char>& active) {
     std::vector<char> next(nb, 0);
@@ -228,18 +253,39 @@ void traverse(RefSim& s) {
   }
   size_t ngroups = (nb + s.group - 1) / s.group;
   unsigned long long pp = 0, pc = 0, op = 0;
+  EwaldData ewald;
+  if (s.periodic) {  // examples/Gravity.C:19-26 (preTraversalFn)
+    fPeriod = Vector3D<Real>(s.period, s.period, s.period);
+    nReplicas = s.n_replicas;
+    ewaldProxy.local = &ewald;
+    ewald.EwaldInit(s.root->data, CkCallback());
+  }
+  const int nr = s.periodic ? s.n_replicas : 0;
+  for (int X = -nr; X <= nr; X++)
+    for (int Y = -nr; Y <= nr; Y++)
+      for (int Z = -nr; Z <= nr; Z++) {
+        Vector3D<Real> offset(X * s.period, Y * s.period, Z * s.period);
+        if (!s.periodic) offset = Vector3D<Real>(0, 0, 0);
 #ifdef _OPENMP
 #pragma omp parallel for schedule(dynamic, 1) reduction(+ : pp, pc, op) num_threads(s.threads)
 #endif
-  for (long g = 0; g < (long)ngroups; g++) {
-    size_t b0 = (size_t)g * s.group;
-    size_t n = std::min((size_t)s.group, nb - b0);
-    GroupTrav t(s, b0, n);
-    std::vector<char> all(n, 1);
-    t.recurse(s.root, all);
-    pp += t.pp;
-    pc += t.pc;
-    op += t.op;
+        for (long g = 0; g < (long)ngroups; g++) {
+          size_t b0 = (size_t)g * s.group;
+          size_t n = std::min((size_t)s.group, nb - b0);
+          GroupTrav t(s, b0, n, offset);
+          std::vector<char> all(n, 1);
+          t.recurse(s.root, all);
+          pp += t.pp;
+          pc += t.pc;
+          op += t.op;
+        }
+      }
+  if (s.periodic) {  // examples/Gravity.C:45-48: callPerLeafFn(LeafEwaldFn)
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 16) num_threads(s.threads)
+#endif
+    for (long b = 0; b < (long)nb; b++) LeafEwaldFn(*s.leaves[b], (Partition<CentroidData>*)nullptr);
+    ewaldProxy.local = nullptr;
   }
   s.n_pp = pp;
   s.n_pc = pc;
@@ -409,6 +455,15 @@ int ptref_run(void* hp, int nsteps) {
     assignKeys(s);
   }
   return 0;
+}
+
+/* Periodic cube of side L with n replica shells walked by the tree and the
+ * reference's Ewald correction (fEwCut 2.6, |h| <= 2.8) for the rest. */
+void ptref_set_periodic(void* h, int periodic, double L, int n_replicas) {
+  RefSim* s = (RefSim*)h;
+  s->periodic = periodic;
+  s->period = L;
+  s->n_replicas = n_replicas;
 }
 
 void ptref_get_acc(void* h, double* ax, double* ay, double* az, double* pot) {

@@ -152,7 +152,7 @@ def lattice(ngrid: int = 256, seed: int = 11, box: float = 1.0, rms_cells: float
         amp = np.where(keep, 1.0 / k2, 0.0)  # |psi(k)|^2 ~ k^2 / k^4 = k^-2
     disp = []
     for kk in (kx, ky, kz):
-        comp = np.fft.irfftn(1j * kk * amp * wk, s=(ngrid, ngrid, ngrid))
+        comp = np.fft.irfftn(1j * kk * amp * wk, s=(ngrid, ngrid, ngrid), axes=(0, 1, 2))
         disp.append(comp)
     disp = np.stack(disp)
     rms = np.sqrt(np.mean(np.sum(disp * disp, axis=0)))

@@ -21,6 +21,13 @@ ref_<case>.json
     per-bucket interaction lists, accelerations, partial potentials, and the
     state after the configured number of kick/perturb steps.  The C oracle
     and the CUDA path must reproduce these bit for bit.
+periodic_<case>.json
+    The same sources in periodic mode (examples/Gravity.C replica walks plus
+    the Ewald correction of examples/Ewald.{h,C}) on a displaced lattice:
+    digests and samples of the accelerations and partial potentials.  The C
+    oracle reproduces them bit for bit (same host libm); the CUDA path is
+    compared with the C oracle within a tolerance, since the Ewald sums call
+    CUDA's erf/erfc/exp/sincos.
 """
 from __future__ import annotations
 
@@ -47,6 +54,12 @@ CASES = {
     "mixture_16k": (ics.mixture, dict(n=16384, seed=7, soft=1e-4), 16, 0.7, 1e-4, 3),
     "plummer_4k_b32_t05": (ics.plummer, dict(n=4096, seed=5, soft=1e-3), 32, 0.5, 0.01, 1),
     "hernquist_8k_t10": (ics.hernquist, dict(n=8192, seed=3, soft=0.01), 32, 1.0, 0.005, 2),
+}
+
+# name -> (lattice kwargs, bucket, theta, n_replicas)
+PERIODIC_CASES = {
+    "lattice_16_b32_r1": (dict(ngrid=16, seed=11, rms_cells=0.25, soft_cells=0.5), 32, 0.7, 1),
+    "lattice_12_b16_t05_r2": (dict(ngrid=12, seed=5, rms_cells=0.4, soft_cells=0.3), 16, 0.5, 2),
 }
 
 
@@ -109,6 +122,24 @@ def run_case(name):
     print(name, out["n_nodes"], out["n_buckets"], out["n_pp"], out["n_pc"])
 
 
+def run_periodic_case(name):
+    kw, bucket, theta, nrep = PERIODIC_CASES[name]
+    p = ics.lattice(**kw)
+    r = O.RefSim(p, bucket=bucket, theta=theta, threads=1)
+    r.set_periodic(1.0, nrep)
+    r.forces()
+    ax, ay, az, pot = r.acc()
+    idx = [0, 1, 2, int(p["x"].size // 2), int(p["x"].size - 1)]
+    out = {
+        "case": name, "kwargs": kw, "bucket": bucket, "theta": theta, "n_replicas": nrep, "period": 1.0,
+        "sha256": {"ax": digest(ax), "ay": digest(ay), "az": digest(az), "pot": digest(pot)},
+        "samples": {"idx": idx, "ax": [float(ax[i]) for i in idx], "pot": [float(pot[i]) for i in idx]},
+    }
+    with open(os.path.join(OUT, f"periodic_{name}.json"), "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+    print(name, p["x"].size)
+
+
 def read_tipsy_dark(path):
     with open(path, "rb") as f:
         buf = f.read()
@@ -147,12 +178,15 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
     ap.add_argument("--cases", nargs="*", default=list(CASES))
+    ap.add_argument("--periodic-cases", nargs="*", default=list(PERIODIC_CASES))
     a = ap.parse_args()
     if not O.ref_available():
         sys.exit("oracle/_ref/libptref.so is missing: run `make -C oracle` with the reference mounted")
     make_kat(a.reference)
     for c in a.cases:
         run_case(c)
+    for c in a.periodic_cases:
+        run_periodic_case(c)
 
 
 if __name__ == "__main__":
