@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define PT_ABI_VERSION 1
+#define PT_ABI_VERSION 2
 
 enum {
   PT_OK = 0,
@@ -71,6 +71,17 @@ typedef struct pt_config {
                         min(L / v_max / cbrt(N), dt_max), examples/Gravity.C:63-67 */
   int device;        /* CUDA device ordinal */
   int record_lists;  /* keep per-bucket interaction lists of every force pass */
+  /* Periodic cube (Configuration::periodic / fPeriod / nReplicas,
+     src/Configuration.h:118-148; examples/Gravity.C:32-48): the tree is walked
+     for (2 n_replicas + 1)^3 replica offsets, then the Ewald correction of
+     examples/Ewald.{h,C} (root monopole + quadrupole; real-space images within
+     ewald_rcut * period, reciprocal vectors |h| <= ewald_hcut) is added.
+     Excludes record_lists. */
+  int periodic;
+  int n_replicas;     /* 0..8 */
+  double period;      /* cube side L (> 0) */
+  double ewald_rcut;  /* fEwCut, examples/Ewald.h:26 (default 2.6) */
+  double ewald_hcut;  /* dEwhCut, examples/Ewald.C:86 (default 2.8) */
   int reserved[8];
 } pt_config;
 
@@ -96,7 +107,8 @@ typedef struct pt_counters {
 /* Library / handle ------------------------------------------------------- */
 int pt_abi_version(void);
 /* Fills the reference's defaults for the Gravity example with the octree:
- * theta 0.7, bucket 16, FP64, KKD, dt_max 1e-5, device 0. */
+ * theta 0.7, bucket 16, FP64, KKD, dt_max 1e-5, device 0; not periodic
+ * (period 1, 0 replica shells, Ewald cuts 2.6 and 2.8). */
 int pt_config_default(pt_config* cfg);
 /* Replaces paratreet::initialize<CentroidData> (src/Paratreet.h:220-239) for
  * this path: allocates the device state of one simulation. */
@@ -199,6 +211,14 @@ int pt_chain_grad(pt_handle* h, int nsteps, double dt, int ckpt_every, const dou
  * the kernel of examples/GravityVisitor.h:87-120 with twoh = soft_i + soft_j. */
 int pt_direct_sum(pt_handle* h, int64_t nt, const int32_t* targets, double* ax, double* ay,
                   double* az, double* pot);
+
+/* FP64 periodic (Ewald) direct sum, the yardstick of the periodic pass: the
+ * Ewald sum of the cube of side config.period (alpha = 4/L, real-space images
+ * within 1.5 L, reciprocal |h|^2 <= 64), with the spline kernel for the
+ * nearest image within soft_i + soft_j, for nt caller indices.  Potentials
+ * include the uniform-background and self terms.  No reference counterpart. */
+int pt_ewald_direct_sum(pt_handle* h, int64_t nt, const int32_t* targets, double* ax, double* ay,
+                        double* az, double* pot);
 
 /* No counterpart in the reference.  The same FP64 direct sum for callers that
  * cannot allocate device memory (their buffers come from a pool or budget of

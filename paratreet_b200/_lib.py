@@ -39,6 +39,11 @@ class PtConfig(C.Structure):
         ("dt_max", C.c_double),
         ("device", C.c_int),
         ("record_lists", C.c_int),
+        ("periodic", C.c_int),
+        ("n_replicas", C.c_int),
+        ("period", C.c_double),
+        ("ewald_rcut", C.c_double),
+        ("ewald_hcut", C.c_double),
         ("reserved", C.c_int * 8),
     ]
 
@@ -93,6 +98,7 @@ SIGNATURES = {
     "pt_get_lists": (C.c_int, [_vp, _vp, _vp, _vp]),
     "pt_get_counters": (C.c_int, [_vp, C.POINTER(PtCounters)]),
     "pt_direct_sum": (C.c_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp]),
+    "pt_ewald_direct_sum": (C.c_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp]),
     "pt_forces_frozen": (C.c_int, [_vp] + [_vp] * 4),
     "pt_adjoint": (C.c_int, [_vp] + [_vp] * 7),
     "pt_chain_grad": (C.c_int, [_vp, C.c_int, C.c_double, C.c_int] + [_vp] * 3 + [_vp] * 8),

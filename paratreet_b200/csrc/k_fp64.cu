@@ -395,6 +395,13 @@ __global__ void __launch_bounds__(kTravWarps * 32) traverse_f64(TravParams P, co
         ev.si = P.p.soft[t0 + lane];
       }
       ev.ax = ev.ay = ev.az = ev.pot = ev.potf = 0.0;
+      if (P.accumulate && lane < nt) {  // later replica walks continue each particle's sum
+        ev.ax = P.p.ax[t0 + lane];
+        ev.ay = P.p.ay[t0 + lane];
+        ev.az = P.p.az[t0 + lane];
+        ev.pot = P.p.pot[t0 + lane];
+        ev.potf = P.p.potf[t0 + lane];
+      }
       ev.ox = P.ox; ev.oy = P.oy; ev.oz = P.oz;
       ev.g = &g;
       ev.n_pp = 0; ev.n_pc = 0;

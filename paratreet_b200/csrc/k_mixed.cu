@@ -482,11 +482,18 @@ __global__ void __launch_bounds__(kMixWarps * 32, kMinBlocks) traverse_mixed(Tra
         for (int gg = 0; gg < x.G; gg++)
           for (int k = 0; k < 4; k++) v[k] += red[4 * (gg * nt + lane) + k];
         const int i = t0 + lane;
-        P.p.ax[i] = v[0];
-        P.p.ay[i] = v[1];
-        P.p.az[i] = v[2];
-        P.p.pot[i] = 0.0;
-        P.p.potf[i] = v[3];
+        if (P.accumulate) {  // later replica walks add to the stored sums
+          P.p.ax[i] += v[0];
+          P.p.ay[i] += v[1];
+          P.p.az[i] += v[2];
+          P.p.potf[i] += v[3];
+        } else {
+          P.p.ax[i] = v[0];
+          P.p.ay[i] = v[1];
+          P.p.az[i] = v[2];
+          P.p.pot[i] = 0.0;
+          P.p.potf[i] = v[3];
+        }
       }
       __syncwarp();
       c_pp += (unsigned long long)x.n_src * (unsigned long long)nt;

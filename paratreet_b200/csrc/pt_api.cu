@@ -66,6 +66,11 @@ struct pt_handle {
   double* dsum = nullptr;  // direct-sum scratch (caller-order copies + partials)
   int64_t dsum_cap = 0;
 
+  double4* d_htab = nullptr;  // Ewald reciprocal table (h vector, hCfac)
+  int htab_cap = 0;
+  double* ewd = nullptr;  // Ewald direct-sum scratch
+  int64_t ewd_cap = 0;
+
   cudaEvent_t ev[7]{};
   pt_counters last{};
   double last_dt = 0.0;
@@ -311,6 +316,79 @@ int upward(pt_handle* h) {
   return PT_OK;
 }
 
+// The Ewald correction of a periodic pass (examples/Gravity.C:45-48 calls
+// LeafEwaldFn on every leaf after the replica walks).  The host builds the
+// reciprocal table from the root's moments as EwaldData::EwaldInit does
+// (examples/Ewald.C:80-163, QEVAL at (hx, hy, hz) with the odd gamma terms
+// zeroed: hCfac = -g2 Qmir - g0 M, hSfac = 0), then one thread per particle of
+// the buckets [b0, b1) adds the real-space and reciprocal sums.
+int ewald_correction_pass(pt_handle* h, int64_t b0, int64_t b1) {
+  cudaStream_t st = h->stream;
+  Mom root;
+  CK(cudaMemcpyAsync(&root, h->nd.mom, sizeof(Mom), cudaMemcpyDeviceToHost, st));
+  int32_t pb[2] = {0, 0};
+  int32_t pe[2] = {0, 0};
+  if (b1 > b0) {
+    int32_t nb0 = 0, nb1 = 0;
+    CK(cudaMemcpyAsync(&nb0, h->buckets + b0, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&nb1, h->buckets + (b1 - 1), sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaMemcpyAsync(pb, &h->nd.walk[nb0].pstart, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(pe, &h->nd.walk[nb1].pstart, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  }
+  CK(cudaStreamSynchronize(st));
+  const double L = h->cfg.period;
+  const double hcut = h->cfg.ewald_hcut;
+  const int hReps = (int)std::ceil(hcut);
+  const double alpha = 2.0 / L;
+  const double k4 = M_PI * M_PI / (alpha * alpha * L * L);
+  std::vector<double4> tab;
+  for (int hx = -hReps; hx <= hReps; ++hx)
+    for (int hy = -hReps; hy <= hReps; ++hy)
+      for (int hz = -hReps; hz <= hReps; ++hz) {
+        const int h2 = hx * hx + hy * hy + hz * hz;
+        if (h2 == 0) continue;
+        if (h2 > hcut * hcut) continue;
+        const double g0 = std::exp(-k4 * h2) / (M_PI * h2 * L);
+        const double g1 = 2 * M_PI / L * g0;
+        const double g2 = -2 * M_PI / L * g1;
+        const double Qmirx = (1.0 / 1.0) * (root.xz * hz + root.xy * hy + root.xx * hx);
+        const double Qmiry = (1.0 / 1.0) * (root.yz * hz + root.xy * hx + root.yy * hy);
+        const double Qmirz = (1.0 / 1.0) * (root.yz * hy + root.xz * hx + root.zz * hz);
+        const double Qmir = (1.0 / 2.0) * (Qmirx * hx + Qmiry * hy + Qmirz * hz);
+        double mfacc = 0.0;
+        mfacc -= g2 * Qmir;
+        mfacc -= g0 * root.mass;
+        tab.push_back(make_double4(2 * M_PI / L * hx, 2 * M_PI / L * hy, 2 * M_PI / L * hz, mfacc));
+      }
+  if ((int)tab.size() > h->htab_cap) {
+    CKR(dalloc(h, &h->d_htab, tab.size()));
+    h->htab_cap = (int)tab.size();
+  }
+  if (!tab.empty())
+    CK(cudaMemcpyAsync(h->d_htab, tab.data(), tab.size() * sizeof(double4), cudaMemcpyHostToDevice, st));
+  EwaldRoot R{};
+  R.cm[0] = root.cm[0];
+  R.cm[1] = root.cm[1];
+  R.cm[2] = root.cm[2];
+  R.mass = root.mass;
+  R.xx = root.xx;
+  R.xy = root.xy;
+  R.xz = root.xz;
+  R.yy = root.yy;
+  R.yz = root.yz;
+  R.zz = root.zz;
+  R.L = L;
+  R.rcut = h->cfg.ewald_rcut;
+  R.n_replicas = h->cfg.n_replicas;
+  R.n_h = (int)tab.size();
+  const int64_t i0 = pb[0], i1 = (b1 > b0) ? (int64_t)pe[0] + pe[1] : i0;
+  launch_ewald_correction(h->p, i0, i1, R, h->d_htab, st);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(st));  // the host table must outlive the copy
+  return PT_OK;
+}
+
 int run_traversal(pt_handle* h, TravParams& P, int grid) {
   if (h->cfg.precision == PT_MIXED && P.mode != 1)
     launch_traverse_mixed(P, h->nd.mom, grid, h->mixed_variant, h->stream);
@@ -386,9 +464,25 @@ int traverse(pt_handle* h, int64_t b0, int64_t b1) {
   } else {
     P.mode = 0;
   }
-  CK(cudaMemsetAsync(h->d_work, 0, sizeof(unsigned), st));
   CK(cudaEventRecord(h->ev[5], st));
-  CKR(run_traversal(h, P, grid));
+  // examples/Gravity.C:32-46: one walk, or (2n+1)^3 replica walks with
+  // GravityVisitor offsets (X, Y, Z) * L in that loop order; every walk after
+  // the first continues each particle's sums
+  const int nr = h->cfg.periodic ? h->cfg.n_replicas : 0;
+  const double L = h->cfg.period;
+  bool first = true;
+  for (int X = -nr; X <= nr; X++)
+    for (int Y = -nr; Y <= nr; Y++)
+      for (int Z = -nr; Z <= nr; Z++) {
+        P.ox = X * L;
+        P.oy = Y * L;
+        P.oz = Z * L;
+        P.accumulate = first ? 0 : 1;
+        first = false;
+        CK(cudaMemsetAsync(h->d_work, 0, sizeof(unsigned), st));
+        CKR(run_traversal(h, P, grid));
+      }
+  if (h->cfg.periodic) CKR(ewald_correction_pass(h, b0, b1));
   CK(cudaEventRecord(h->ev[6], st));
   return PT_OK;
 }
@@ -490,6 +584,11 @@ int pt_config_default(pt_config* c) {
   c->dt_max = 1e-5;
   c->device = 0;
   c->record_lists = 0;
+  c->periodic = 0;
+  c->n_replicas = 0;
+  c->period = 1.0;
+  c->ewald_rcut = 2.6;  // fEwCut, examples/Ewald.h:26
+  c->ewald_hcut = 2.8;  // dEwhCut, examples/Ewald.C:86
   return PT_OK;
 }
 
@@ -499,6 +598,10 @@ int pt_create(const pt_config* cfg, pt_handle** out) {
   if (!(cfg->theta > 0.0) || cfg->bucket < 1 || cfg->bucket > 32) return PT_E_ARG;
   if (cfg->precision != PT_FP64 && cfg->precision != PT_MIXED) return PT_E_ARG;
   if (cfg->integrator != PT_KKD && cfg->integrator != PT_KDK) return PT_E_ARG;
+  if (cfg->periodic && (!(cfg->period > 0.0) || cfg->n_replicas < 0 || cfg->n_replicas > 8 ||
+                        !(cfg->ewald_rcut > 0.0) || cfg->ewald_rcut > 8.0 || !(cfg->ewald_hcut >= 0.0) ||
+                        cfg->ewald_hcut > 16.0 || cfg->record_lists))
+    return PT_E_ARG;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return PT_E_CUDA;
   if (cfg->device < 0 || cfg->device >= ndev) return PT_E_ARG;
@@ -545,7 +648,7 @@ int pt_destroy(pt_handle* h) {
   dfree(o.first_child); dfree(o.count); dfree(o.mom); dfree(o.walk); dfree(o.quad); dfree(o.quadf);
   dfree(o.fifo); dfree(o.nleaf_sub); dfree(o.nempty_sub); dfree(o.leaf_base); dfree(o.empty_base);
   dfree(h->flags); dfree(h->buckets); dfree(h->list_count); dfree(h->list_off); dfree(h->list_node);
-  dfree(h->list_kind); dfree(h->dsum); dfree(h->adj); dfree(h->nadj);
+  dfree(h->list_kind); dfree(h->dsum); dfree(h->adj); dfree(h->nadj); dfree(h->d_htab); dfree(h->ewd);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -830,6 +933,80 @@ int pt_direct_sum(pt_handle* h, int64_t nt, const int32_t* targets, double* ax, 
     if (ay) ay[t] = s[1];
     if (az) az[t] = s[2];
     if (pot) pot[t] = s[3];
+  }
+  return PT_OK;
+}
+
+// FP64 periodic (Ewald) direct sum: alpha = 4/L, real-space images within
+// 1.5 L (erfc(6) ~ 2e-17), reciprocal |h|^2 <= 64 (exp(-pi^2 64/16) ~ 7e-18),
+// the spline kernel for the nearest image within soft_i + soft_j, and the
+// background and self terms in the potential.
+int pt_ewald_direct_sum(pt_handle* h, int64_t nt, const int32_t* targets, double* ax, double* ay, double* az,
+                        double* pot) {
+  if (!h || nt < 0 || (nt > 0 && !targets)) return PT_E_ARG;
+  if (!h->p.x) return fail(h, PT_E_STATE, "no particles");
+  if (!(h->cfg.period > 0.0)) return fail(h, PT_E_ARG, "period must be positive");
+  const int64_t n = h->n;
+  if (nt == 0 || n == 0) return PT_OK;
+  for (int64_t t = 0; t < nt; t++)
+    if (targets[t] < 0 || targets[t] >= n) return fail(h, PT_E_ARG, "target index out of range");
+  cudaSetDevice(h->cfg.device);
+  cudaStream_t st = h->stream;
+  const double L = h->cfg.period, V = L * L * L;
+  const double alpha = 4.0 / L, rcut = 1.5 * L;
+  const int hmax = 8;
+  std::vector<double4> kv;
+  for (int hx = -hmax; hx <= hmax; hx++)
+    for (int hy = -hmax; hy <= hmax; hy++)
+      for (int hz = -hmax; hz <= hmax; hz++) {
+        const int h2 = hx * hx + hy * hy + hz * hz;
+        if (h2 == 0 || h2 > hmax * hmax) continue;
+        const double kx = 2 * M_PI / L * hx, ky = 2 * M_PI / L * hy, kz = 2 * M_PI / L * hz;
+        const double k2 = kx * kx + ky * ky + kz * kz;
+        kv.push_back(make_double4(kx, ky, kz, 4 * M_PI / V * std::exp(-k2 / (4 * alpha * alpha)) / k2));
+      }
+  const int nk = (int)kv.size();
+  kv.push_back(make_double4(0.0, 0.0, 0.0, 0.0));  // k = 0: total mass
+  const int tb = (int)((nt + 127) / 128);
+  int nsplit = std::max(1, std::min(256, (4 * h->sms + tb - 1) / tb));
+  if (n < 4096) nsplit = 1;
+  // doubles: caller-order x y z m soft (5n) | partials (4 nt nsplit) | recip out (4 nt) | S (2 nk + 2)
+  //          | k vectors (4 (nk + 1), 32-byte aligned) | targets (int32, nt / 2 + 1 doubles)
+  const int64_t off_part = 5 * n, off_rec = off_part + 4 * nt * nsplit, off_S = off_rec + 4 * nt;
+  const int64_t off_kv = (off_S + 2 * (nk + 1) + 3) / 4 * 4;
+  const int64_t off_tgt = off_kv + 4 * (nk + 1);
+  const int64_t need = off_tgt + nt / 2 + 1;
+  if (need > h->ewd_cap) {
+    CKR(dalloc(h, &h->ewd, need));
+    h->ewd_cap = need;
+  }
+  double* c = h->ewd;
+  const double* src[5] = {h->p.x, h->p.y, h->p.z, h->p.m, h->p.soft};
+  for (int k = 0; k < 5; k++) launch_scatter_f64(src[k], c + k * n, h->p.order, n, grid_for(h, n), st);
+  double* part = c + off_part;
+  double* rec = c + off_rec;
+  double* S = c + off_S;
+  double4* dkv = reinterpret_cast<double4*>(c + off_kv);
+  int32_t* dt = reinterpret_cast<int32_t*>(c + off_tgt);
+  CK(cudaMemcpyAsync(dkv, kv.data(), kv.size() * sizeof(double4), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dt, targets, nt * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  launch_ewald_structure(c, c + n, c + 2 * n, c + 3 * n, n, dkv, nk + 1, S, st);
+  launch_ewald_real(c, c + n, c + 2 * n, c + 3 * n, c + 4 * n, n, dt, nt, nsplit, L, alpha, rcut, part, st);
+  launch_ewald_recip(c, c + n, c + 2 * n, c + 3 * n, dt, nt, dkv, nk, S, alpha, V, rec, st);
+  CK(cudaGetLastError());
+  std::vector<double> hp((size_t)4 * nt * nsplit), hr((size_t)4 * nt);
+  CK(cudaMemcpyAsync(hp.data(), part, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(hr.data(), rec, hr.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  for (int64_t t = 0; t < nt; t++) {
+    double s4[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int sl = 0; sl < nsplit; sl++)
+      for (int k = 0; k < 4; k++) s4[k] += hp[((size_t)sl * nt + t) * 4 + k];
+    for (int k = 0; k < 4; k++) s4[k] += hr[4 * t + k];
+    if (ax) ax[t] = s4[0];
+    if (ay) ay[t] = s4[1];
+    if (az) az[t] = s4[2];
+    if (pot) pot[t] = s4[3];
   }
   return PT_OK;
 }

@@ -104,6 +104,7 @@ struct TravParams {
   double ox, oy, oz;      // GravityVisitor offset (periodic replicas; 0 otherwise)
   int64_t nnodes;
   int mode;               // 0 evaluate, 1 count lists only, 2 evaluate + record lists
+  int accumulate;         // add to the stored accelerations (replica walks after the first)
   int64_t* list_count;    // mode 1: entries per bucket
   const int64_t* list_off;// mode 2: CSR offsets
   int32_t* list_node;     // mode 2: node index per entry
@@ -111,6 +112,15 @@ struct TravParams {
   unsigned long long* counters;  // n_pp, n_pc, n_open
   unsigned int* work;     // dynamic bucket counter
   unsigned int* status;
+};
+
+// Root cell of the periodic cube for the Ewald correction (k_ewald.cu):
+// CentroidData of the root (mass, cm, quadrupole about cm) and the sums' cuts.
+struct EwaldRoot {
+  double cm[3], mass;
+  double xx, xy, xz, yy, yz, zz;
+  double L, rcut;
+  int n_replicas, n_h;
 };
 
 // Inputs and outputs of the adjoint force pass (k_adjoint.cu).

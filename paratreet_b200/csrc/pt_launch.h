@@ -53,6 +53,18 @@ void launch_prep_sources(const int32_t* buckets, int64_t nbuckets, const WalkRec
                          float* softf, cudaStream_t st);
 void launch_traverse_mixed(const TravParams& P, const Mom* mom, int grid, int variant, cudaStream_t st);
 
+// k_ewald.cu
+void launch_ewald_correction(Particles p, int64_t i0, int64_t i1, const EwaldRoot& R, const double4* htab,
+                             cudaStream_t st);
+void launch_ewald_structure(const double* x, const double* y, const double* z, const double* m, int64_t n,
+                            const double4* kv, int nk, double* S, cudaStream_t st);
+void launch_ewald_real(const double* x, const double* y, const double* z, const double* m, const double* soft,
+                       int64_t n, const int32_t* tgt, int64_t nt, int nsplit, double L, double alpha, double rcut,
+                       double* part, cudaStream_t st);
+void launch_ewald_recip(const double* x, const double* y, const double* z, const double* m, const int32_t* tgt,
+                        int64_t nt, const double4* kv, int nk, const double* S, double alpha, double V, double* out,
+                        cudaStream_t st);
+
 // k_adjoint.cu
 void launch_adjoint(const AdjParams& A, int grid, cudaStream_t st);
 

@@ -56,6 +56,11 @@ class Configuration:
     integrator: str = "kkd"
     device: int = 0
     record_lists: bool = False
+    periodic: bool = False        # Configuration::periodic
+    n_replicas: int = 0           # Configuration::nReplicas
+    period: float = 1.0           # Configuration::fPeriod (cubic)
+    ewald_rcut: float = 2.6       # fEwCut, examples/Ewald.h:26
+    ewald_hcut: float = 2.8       # dEwhCut, examples/Ewald.C:86
 
 
 @dataclass
@@ -94,6 +99,11 @@ class GravitySimulation:
         cfg.dt_max = conf.max_timestep
         cfg.device = conf.device
         cfg.record_lists = 1 if conf.record_lists else 0
+        cfg.periodic = 1 if conf.periodic else 0
+        cfg.n_replicas = conf.n_replicas
+        cfg.period = conf.period
+        cfg.ewald_rcut = conf.ewald_rcut
+        cfg.ewald_hcut = conf.ewald_hcut
         h = C.c_void_p()
         rc = self._lib.pt_create(C.byref(cfg), C.byref(h))
         if rc != L.PT_OK:
@@ -153,7 +163,8 @@ class GravitySimulation:
         """Partition::startDown<GravityVisitor>: one force evaluation."""
         if visitor is not None:
             if any(visitor.offset):
-                raise NotImplementedError("periodic replica offsets are not supported yet")
+                raise ValueError("replica offsets are generated by the periodic configuration "
+                                 "(periodic=True, n_replicas, period), as traversalFn does")
             if visitor.theta != self.conf.theta:
                 self.set_theta(visitor.theta)
         if buckets is None:
@@ -226,6 +237,13 @@ class GravitySimulation:
         c = L.PtCounters()
         self._check(self._lib.pt_get_counters(self._h, C.byref(c)))
         return {f: getattr(c, f) for f, _ in L.PtCounters._fields_ if f != "reserved"}
+
+    def ewald_direct_sum(self, targets):
+        """FP64 periodic (Ewald) direct sum in the configured cube at target indices."""
+        t = np.ascontiguousarray(targets, dtype=np.int32)
+        out = [np.empty(t.size) for _ in range(4)]
+        self._check(self._lib.pt_ewald_direct_sum(self._h, t.size, L.ptr(t), *[L.ptr(o) for o in out]))
+        return out
 
     def direct_sum(self, targets):
         t = np.ascontiguousarray(targets, dtype=np.int32)

@@ -37,7 +37,7 @@ def test_binding_covers_every_declared_symbol():
 
 def test_abi_version_and_defaults_without_gpu():
     lib = L.load()
-    assert lib.pt_abi_version() == 1
+    assert lib.pt_abi_version() == 2
     cfg = L.PtConfig()
     assert lib.pt_config_default(C.byref(cfg)) == 0
     assert cfg.theta == 0.7 and cfg.bucket == 16 and cfg.dt_max == 1e-5
@@ -54,6 +54,16 @@ def test_create_rejects_bad_config():
     cfg.bucket = 16
     cfg.theta = 0.0
     assert lib.pt_create(C.byref(cfg), C.byref(h)) == -1
+    cfg.theta = 0.7
+    # periodic: positive period, 0..8 replica shells, bounded cuts, no recorded lists
+    cfg.periodic = 1
+    assert (cfg.period, cfg.ewald_rcut, cfg.ewald_hcut) == (1.0, 2.6, 2.8)
+    for field, bad in (("period", 0.0), ("n_replicas", 9), ("n_replicas", -1), ("record_lists", 1),
+                       ("ewald_rcut", 0.0), ("ewald_rcut", 9.0), ("ewald_hcut", 17.0)):
+        keep = getattr(cfg, field)
+        setattr(cfg, field, bad)
+        assert lib.pt_create(C.byref(cfg), C.byref(h)) == -1, field
+        setattr(cfg, field, keep)
 
 
 def test_null_handle_calls_return_errors():
