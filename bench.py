@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-extras", action="store_true", help="skip e2e, fp64 comparison, errors, cpu baseline")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--sweep", default="0.5,0.7,1.0",
+                    help="theta values of the accuracy / throughput sweep ('' to skip)")
     return ap.parse_args()
 
 
@@ -306,6 +308,38 @@ def main():
     return 0
 
 
+def theta_sweep(a, sim, tgt, direct, stream):
+    """Force evaluations/s and errors vs the FP64 direct sum of both forms
+    over the theta values of --sweep (same particles and targets)."""
+    import torch
+    n = a.n
+    rows = []
+    for th in [float(v) for v in a.sweep.split(",") if v]:
+        sim.set_theta(th)
+        row = {"theta": th}
+        for prec, reps in (("mixed", 2), ("fp64", 1)):
+            sim.set_precision(prec)
+            sim.start_down()
+            ts = []
+            for _ in range(reps):
+                s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s0.record(stream)
+                sim.start_down()
+                s1.record(stream)
+                torch.cuda.synchronize()
+                ts.append(s0.elapsed_time(s1) / 1e3)
+            acc = sim.accelerations()
+            c = sim.counters()
+            row[prec] = {"force_evals_per_s": n / float(np.mean(ts)), "ms_per_pass": 1e3 * float(np.mean(ts)),
+                         "err_vs_direct": rel_errors((acc["ax"][tgt], acc["ay"][tgt], acc["az"][tgt]), direct),
+                         "interactions_per_particle": (c["n_pp"] + c["n_pc"]) / n}
+        row["ratio_mixed_over_fp64"] = row["mixed"]["force_evals_per_s"] / row["fp64"]["force_evals_per_s"]
+        rows.append(row)
+    sim.set_theta(a.theta)
+    sim.set_precision(a.precision)
+    return rows
+
+
 def gpu_launches(c):
     """Kernels of our library launched by one force pass (counted from the
     pass structure: keys 3, sort 8x(3 + scan) + 9 gathers, build per level,
@@ -372,6 +406,7 @@ def extras(a, sim, p, world, rank, stream, value):
     diff = rel_errors((am["ax"], am["ay"], am["az"]), (a64["ax"], a64["ay"], a64["az"]))
     sim.set_precision(a.precision)
     v_other = n / float(np.mean(t64))
+    res["theta_sweep"] = theta_sweep(a, sim, tgt, (dax, day, daz), stream) if a.sweep else []
     res["precision_comparison"] = {
         f"{a.precision}_force_evals_per_s": value, f"{other}_force_evals_per_s": v_other,
         "ratio_mixed_over_fp64": (value / v_other) if a.precision == "mixed" else (v_other / value),
