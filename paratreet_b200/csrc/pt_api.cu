@@ -34,7 +34,7 @@ struct pt_handle {
   int32_t* tmp_i = nullptr;
   uint64_t* key_alt = nullptr;
   uint32_t *idx = nullptr, *idx_alt = nullptr;
-  uint32_t* sort_hist = nullptr;
+  unsigned char* sort_scratch = nullptr;  // onesweep histograms, tile counters, look-back words
   uint32_t* scan_scratch = nullptr;
   size_t scan_scratch_elems = 0;
   uint32_t* d_total = nullptr;
@@ -143,8 +143,8 @@ int ensure_particles(pt_handle* h, int64_t n) {
   CKR(dalloc(h, &h->key_alt, c));
   CKR(dalloc(h, &h->idx, c));
   CKR(dalloc(h, &h->idx_alt, c));
-  CKR(dalloc(h, &h->sort_hist, sort_hist_elems(c)));
-  size_t ss = std::max(scan_scratch_bytes((int64_t)sort_hist_elems(c)), scan_scratch_bytes(8 * c + 64));
+  CKR(dalloc(h, &h->sort_scratch, sort_scratch_bytes(c)));
+  size_t ss = scan_scratch_bytes(8 * c + 64);
   h->scan_scratch_elems = ss / sizeof(uint32_t) + 1;
   CKR(dalloc(h, &h->scan_scratch, h->scan_scratch_elems));
   h->cap_n = c;
@@ -219,6 +219,7 @@ int read_status(pt_handle* h) {
     if (st & kErrListOverflow) m += " interaction list overflow;";
     if (st & kErrCapacity) m += " capacity exceeded;";
     if (st & kErrAdjointSoftened) m += " adjoint met a softened quadrupole term (not differentiated);";
+    if (st & kErrSort) m += " radix sort look-back timed out;";
     return fail(h, (st & kErrNonFinite) ? PT_E_NONFINITE : PT_E_DEVICE, m);
   }
   return PT_OK;
@@ -233,7 +234,8 @@ int keys_and_sort(pt_handle* h) {
   launch_keys(h->p.x, h->p.y, h->p.z, n, h->d_uni, h->p.key, h->idx, g, st);
   CK(cudaGetLastError());
   CK(cudaEventRecord(h->ev[1], st));
-  radix_sort_pairs(h->p.key, h->idx, h->key_alt, h->idx_alt, n, h->sort_hist, h->scan_scratch, h->d_total, st);
+  if (radix_sort_pairs(h->p.key, h->idx, h->key_alt, h->idx_alt, n, h->sort_scratch, h->d_status, h->sms, st))
+    return fail(h, PT_E_CUDA, "radix sort: could not set the shared-memory attribute");
   double** fields[] = {&h->p.x, &h->p.y, &h->p.z, &h->p.vx, &h->p.vy, &h->p.vz, &h->p.m, &h->p.soft};
   for (auto f : fields) {
     gather_f64(*f, h->tmp_d, h->idx, n, g, st);
@@ -641,7 +643,7 @@ int pt_destroy(pt_handle* h) {
                     &h->p.ax, &h->p.ay, &h->p.az, &h->p.pot, &h->p.potf, &h->tmp_d};
   for (auto pp : dbl) dfree(*pp);
   dfree(h->p.order); dfree(h->tmp_i); dfree(h->p.key); dfree(h->key_alt); dfree(h->idx); dfree(h->idx_alt);
-  dfree(h->sort_hist); dfree(h->scan_scratch); dfree(h->d_total); dfree(h->bbox_partial); dfree(h->d_uni);
+  dfree(h->sort_scratch); dfree(h->scan_scratch); dfree(h->d_total); dfree(h->bbox_partial); dfree(h->d_uni);
   dfree(h->d_status); dfree(h->d_counters); dfree(h->d_work); dfree(h->d_vmax2); dfree(h->srcf); dfree(h->softf);
   Nodes& o = h->nd;
   dfree(o.key); dfree(o.type); dfree(o.depth); dfree(o.pstart); dfree(o.pcount); dfree(o.parent);

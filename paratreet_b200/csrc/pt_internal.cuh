@@ -21,6 +21,7 @@ enum : unsigned {
   kErrListOverflow = 1u << 3,
   kErrCapacity = 1u << 4,
   kErrAdjointSoftened = 1u << 5,
+  kErrSort = 1u << 6,                 // radix sort look-back gave up waiting
 };
 
 // Particle state, structure of arrays, FP64, in key-sorted order after a build.

@@ -21,9 +21,10 @@ void launch_vmax2(const double* vx, const double* vy, const double* vz, int64_t 
 size_t scan_scratch_bytes(int64_t n);
 void scan_exclusive(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* scratch, uint32_t* total,
                     cudaStream_t st);
-size_t sort_hist_elems(int64_t n);
-void radix_sort_pairs(uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, int64_t n, uint32_t* hist,
-                      uint32_t* scratch, uint32_t* total, cudaStream_t st);
+size_t sort_scratch_bytes(int64_t n);
+// 0 on success, -1 if the kernel attribute could not be set
+int radix_sort_pairs(uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, int64_t n, void* scratch,
+                     unsigned* status, int sms, cudaStream_t st);
 void gather_f64(const double* in, double* out, const uint32_t* idx, int64_t n, int grid, cudaStream_t st);
 void gather_i32(const int32_t* in, int32_t* out, const uint32_t* idx, int64_t n, int grid, cudaStream_t st);
 
