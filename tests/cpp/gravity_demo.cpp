@@ -1,0 +1,62 @@
+// A C++ host written against the Visitor API, driving the device path through
+// include/paratreet_gpu.hpp (built and run by tests/test_cpp_facade.py).
+//
+//   gravity_demo copy  in.tipsy out.tipsy            read and write Tipsy (no GPU)
+//   gravity_demo forces in.tipsy out.acc theta bucket [mixed]
+//                                                    one force pass, .acc output
+//   gravity_demo steps in.tipsy out.tipsy theta bucket dt n
+//                                                    n Driver::run iterations
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+#include "paratreet_gpu.hpp"
+
+using namespace paratreet_gpu;
+
+int main(int argc, char** argv) {
+  if (argc < 4) {
+    std::fprintf(stderr, "usage: %s copy|forces|steps in out [theta bucket [dt n | mixed]]\n", argv[0]);
+    return 2;
+  }
+  const std::string mode = argv[1];
+  try {
+    TipsyHeader h;
+    Particles p = read_tipsy(argv[2], &h);
+    std::printf("read %d particles (gas %d, dark %d, star %d), time %.17g\n", h.nbodies, h.nsph, h.ndark,
+                h.nstar, h.time);
+    if (mode == "copy") {
+      write_tipsy(argv[3], p, h.time);
+      return 0;
+    }
+    Configuration conf;
+    conf.theta = argc > 4 ? std::atof(argv[4]) : 0.7;
+    conf.max_particles_per_leaf = argc > 5 ? std::atoi(argv[5]) : 16;
+    if (mode == "forces") {
+      if (argc > 6 && std::strcmp(argv[6], "mixed") == 0) conf.precision = PT_MIXED;
+      Gravity g(conf);
+      g.load(p);
+      Accelerations a = run_gravity(g, GravityVisitor(Vector3D{0, 0, 0}, conf.theta));
+      write_acc(argv[3], a);
+      const pt_counters c = g.counters();
+      std::printf("buckets %lld nodes %lld pp %llu pc %llu\n", (long long)c.n_buckets, (long long)c.n_nodes,
+                  (unsigned long long)c.n_pp, (unsigned long long)c.n_pc);
+      return 0;
+    }
+    if (mode == "steps" && argc > 7) {
+      conf.max_timestep = std::atof(argv[6]);
+      Gravity g(conf);
+      g.load(p);
+      g.run(std::atoi(argv[7]));
+      g.state(p);
+      write_tipsy(argv[3], p, h.time);
+      return 0;
+    }
+    std::fprintf(stderr, "unknown mode %s\n", mode.c_str());
+    return 2;
+  } catch (const Error& e) {
+    std::fprintf(stderr, "error %d: %s\n", e.code, e.what());
+    return 1;
+  }
+}
