@@ -234,15 +234,20 @@ def main():
     sim.set_stream(stream.cuda_stream)
     sim.set_particles(p)
 
+    shard = None
+    if world > 1:  # buckets cut by measured work; results summed over the ranks (NCCL)
+        from paratreet_b200.sharding import DeviceEngine, ShardedGravity
+        shard = ShardedGravity(DeviceEngine(sim), world, rank)
+
     def pass_range():
-        if world == 1:
+        if shard is None:
             sim.start_down()
         else:
-            nb = sim.counters()["n_buckets"] or 1
-            b0, b1 = rank * nb // world, (rank + 1) * nb // world
-            sim.start_down(buckets=(b0, b1))
+            shard.forces()
 
-    sim.start_down()  # establishes bucket count for sharding
+    sim.start_down()  # a full pass on every rank: bucket count and per-bucket work
+    if shard is not None:
+        shard.balance(sim.bucket_work().astype(np.int64))
     for _ in range(a.warmup):
         pass_range()
     torch.cuda.synchronize()
@@ -298,7 +303,7 @@ def main():
            "interactions_per_s": (cnts["n_pp"] + cnts["n_pc"]) / t_trav}
 
     if not a.no_extras:
-        out.update(extras(a, sim, p, world, rank, stream, value))
+        out.update(extras(a, sim, p, world, rank, stream, value, shard))
     sim.close()
     if rank == 0:
         print(json.dumps(out))
@@ -350,7 +355,7 @@ def gpu_launches(c):
     return n
 
 
-def extras(a, sim, p, world, rank, stream, value):
+def extras(a, sim, p, world, rank, stream, value, shard=None):
     import torch
     n = a.n
     res = {}
@@ -367,11 +372,10 @@ def extras(a, sim, p, world, rank, stream, value):
     e0.record(stream)
     for _ in range(steps):
         sim.set_particles(host)
-        if world == 1:
+        if shard is None:
             sim.start_down()
         else:
-            nb = sim.counters()["n_buckets"] or 1
-            sim.start_down(buckets=(rank * nb // world, (rank + 1) * nb // world))
+            shard.forces()
         sim.accelerations({"ax": hout["ax"], "ay": hout["ay"], "az": hout["az"], "pot": None,
                            "pot_full": hout["pot_full"]})
     e1.record(stream)

@@ -149,14 +149,25 @@ int pt_compute_forces_range(pt_handle* h, int64_t b0, int64_t b1);
  * (P2P spline, quadrupole, monopole).  Any pointer may be NULL. */
 int pt_get_accel(pt_handle* h, double* ax, double* ay, double* az, double* pot, double* pot_full);
 /* Device pointers (sorted order, FP64) of the last force pass, and the
- * sorted-to-caller permutation (int32 order[i] = caller index of sorted i). */
-int pt_device_accel(pt_handle* h, const double** ax, const double** ay, const double** az,
+ * sorted-to-caller permutation (int32 order[i] = caller index of sorted i).
+ * The arrays may be changed in place before pt_advance / pt_get_accel: the
+ * ranks of a sharded run, which build identical trees and so share the sorted
+ * order, sum their pt_compute_forces_range results there (outside the range
+ * every array is zero).  Any pointer may be NULL. */
+int pt_device_accel(pt_handle* h, double** ax, double** ay, double** az, double** pot, double** pot_full,
                     const int32_t** order);
 
 /* Integration ------------------------------------------------------------ */
 /* nsteps iterations of src/Driver.h:183-251 (PT_KKD) or leapfrog (PT_KDK).
  * dt = min(L / v_max / cbrt(N), dt_max) per step. */
 int pt_step(pt_handle* h, int nsteps);
+/* The integrator half of one Driver::run iteration without its force pass:
+ * dt = min(L / v_max / cbrt(N), dt_max), then Partition::kick + perturb
+ * (src/Partition.h:329-379, src/Particle.C:7-21) with the accelerations now on
+ * the device (pt_device_accel), e.g. after the ranks of a sharded run have
+ * summed their pt_compute_forces_range results.  Needs a force pass at the
+ * current positions; dt may be NULL. */
+int pt_advance(pt_handle* h, double* dt);
 int pt_get_state(pt_handle* h, double* x, double* y, double* z, double* vx, double* vy, double* vz);
 int pt_last_dt(const pt_handle* h, double* dt);
 
@@ -179,6 +190,11 @@ int pt_get_bucket_keys(pt_handle* h, uint64_t* keys);
 int pt_get_lists_size(pt_handle* h, int64_t* total);
 int pt_get_lists(pt_handle* h, int64_t* offsets, uint64_t* keys, int32_t* kinds);
 int pt_get_counters(pt_handle* h, pt_counters* c);
+/* P2P pairs + P2C evaluations of each bucket (DFS order, pt_get_tree_size
+ * buckets) in the last force pass, replicas included; 0 for buckets outside
+ * the traversed range.  The cost model for splitting buckets over ranks
+ * (the work the reference's decompositions balance, src/Decomposition.C). */
+int pt_get_bucket_work(pt_handle* h, uint64_t* work);
 
 /* Differentiation ---------------------------------------------------------
  * No reference counterpart (ParaTreeT has no gradients).  All three need a

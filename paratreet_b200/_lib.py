@@ -85,7 +85,7 @@ SIGNATURES = {
     "pt_compute_forces": (C.c_int, [_vp]),
     "pt_compute_forces_range": (C.c_int, [_vp, _i64, _i64]),
     "pt_get_accel": (C.c_int, [_vp] + [_vp] * 5),
-    "pt_device_accel": (C.c_int, [_vp] + [C.POINTER(_vp)] * 4),
+    "pt_device_accel": (C.c_int, [_vp] + [C.POINTER(_vp)] * 6),
     "pt_step": (C.c_int, [_vp, C.c_int]),
     "pt_get_state": (C.c_int, [_vp] + [_vp] * 6),
     "pt_last_dt": (C.c_int, [_vp, _dp]),
@@ -99,6 +99,8 @@ SIGNATURES = {
     "pt_get_counters": (C.c_int, [_vp, C.POINTER(PtCounters)]),
     "pt_direct_sum": (C.c_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp]),
     "pt_ewald_direct_sum": (C.c_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp]),
+    "pt_advance": (C.c_int, [_vp, _vp]),
+    "pt_get_bucket_work": (C.c_int, [_vp, _vp]),
     "pt_forces_frozen": (C.c_int, [_vp] + [_vp] * 4),
     "pt_adjoint": (C.c_int, [_vp] + [_vp] * 7),
     "pt_chain_grad": (C.c_int, [_vp, C.c_int, C.c_double, C.c_int] + [_vp] * 3 + [_vp] * 8),

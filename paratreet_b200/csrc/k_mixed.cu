@@ -372,6 +372,7 @@ __global__ void __launch_bounds__(kMixWarps * 32, kMinBlocks) traverse_mixed(Tra
     const int tbase = P.walk[tnode].pstart, ntot = P.walk[tnode].pcount;
     // more than 32 particles only in a depth-21 leaf of identical keys: its
     // targets are walked in chunks of 32 (decisions depend on the bucket only)
+    const unsigned long long work0 = c_pp + c_pc;
     for (int tc = 0; tc < ntot; tc += 32) {
       const int t0 = tbase + tc, nt = min(32, ntot - tc);
       unsigned long long opens = 0;
@@ -499,6 +500,10 @@ __global__ void __launch_bounds__(kMixWarps * 32, kMinBlocks) traverse_mixed(Tra
       c_pp += (unsigned long long)x.n_src * (unsigned long long)nt;
       c_pc += (unsigned long long)x.n_node * (unsigned long long)nt;
       if (tc == 0) c_open += opens;
+    }
+    if (P.bucket_work && lane == 0) {
+      const unsigned long long wk = c_pp + c_pc - work0;
+      P.bucket_work[b] = P.accumulate ? P.bucket_work[b] + wk : wk;
     }
   }
   if (lane == 0) {

@@ -54,6 +54,7 @@ struct pt_handle {
   uint32_t* flags = nullptr;
   std::vector<int64_t> lev;
   int32_t* buckets = nullptr;
+  unsigned long long* bucket_work = nullptr;  // interactions per bucket of the last pass
   int64_t nbuckets = 0, cap_buckets = 0;
 
   int64_t* list_count = nullptr;
@@ -288,6 +289,7 @@ int build_tree(pt_handle* h) {
   h->nbuckets = nl;
   if (nl > h->cap_buckets) {
     CKR(dalloc(h, &h->buckets, nl));
+    CKR(dalloc(h, &h->bucket_work, nl));
     h->cap_buckets = nl;
   }
   launch_assign_buckets(h->nd, h->nnodes, h->buckets, nl, st);
@@ -419,6 +421,8 @@ int traverse(pt_handle* h, int64_t b0, int64_t b1) {
   P.b_begin = b0;
   P.b_end = b1;
   P.ox = P.oy = P.oz = 0.0;
+  P.bucket_work = h->bucket_work;
+  if (h->nbuckets > 0) CK(cudaMemsetAsync(h->bucket_work, 0, h->nbuckets * sizeof(unsigned long long), st));
   P.nnodes = h->nnodes;
   P.counters = h->d_counters;
   P.work = h->d_work;
@@ -649,7 +653,7 @@ int pt_destroy(pt_handle* h) {
   dfree(o.key); dfree(o.type); dfree(o.depth); dfree(o.pstart); dfree(o.pcount); dfree(o.parent);
   dfree(o.first_child); dfree(o.count); dfree(o.mom); dfree(o.walk); dfree(o.quad); dfree(o.quadf);
   dfree(o.fifo); dfree(o.nleaf_sub); dfree(o.nempty_sub); dfree(o.leaf_base); dfree(o.empty_base);
-  dfree(h->flags); dfree(h->buckets); dfree(h->list_count); dfree(h->list_off); dfree(h->list_node);
+  dfree(h->flags); dfree(h->buckets); dfree(h->bucket_work); dfree(h->list_count); dfree(h->list_off); dfree(h->list_node);
   dfree(h->list_kind); dfree(h->dsum); dfree(h->adj); dfree(h->nadj); dfree(h->d_htab); dfree(h->ewd);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
@@ -725,12 +729,43 @@ int pt_get_accel(pt_handle* h, double* ax, double* ay, double* az, double* pot, 
   return PT_OK;
 }
 
-int pt_device_accel(pt_handle* h, const double** ax, const double** ay, const double** az, const int32_t** order) {
+int pt_device_accel(pt_handle* h, double** ax, double** ay, double** az, double** pot, double** pot_full,
+                    const int32_t** order) {
   if (!h) return PT_E_ARG;
   if (ax) *ax = h->p.ax;
   if (ay) *ay = h->p.ay;
   if (az) *az = h->p.az;
+  if (pot) *pot = h->p.pot;
+  if (pot_full) *pot_full = h->p.potf;
   if (order) *order = h->p.order;
+  return PT_OK;
+}
+
+int pt_get_bucket_work(pt_handle* h, uint64_t* work) {
+  if (!h || !work) return PT_E_ARG;
+  if (!h->have_forces) return fail(h, PT_E_STATE, "no force pass yet");
+  if (h->nbuckets == 0) return PT_OK;
+  cudaSetDevice(h->cfg.device);
+  CK(cudaMemcpyAsync(work, h->bucket_work, h->nbuckets * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return PT_OK;
+}
+
+int pt_advance(pt_handle* h, double* dt_out) {
+  if (!h) return PT_E_ARG;
+  if (!h->p.x) return fail(h, PT_E_STATE, "no particles");
+  if (!h->have_forces || !h->forces_current) return fail(h, PT_E_STATE, "no force pass at the current positions");
+  cudaSetDevice(h->cfg.device);
+  double dt = 0.0;
+  if (h->n > 0) {
+    CKR(timestep(h, &dt));
+    launch_kick_perturb(h->p, h->n, dt, grid_for(h, h->n), h->stream);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  h->last_dt = dt;
+  h->forces_current = false;
+  if (dt_out) *dt_out = dt;
   return PT_OK;
 }
 

@@ -184,6 +184,22 @@ class GravitySimulation:
         """Driver::run: num_iterations of forces, kick, perturb."""
         self._check(self._lib.pt_step(self._h, int(num_iterations)))
 
+    def advance(self) -> float:
+        """Kick + perturb with the accelerations now on the device (after a
+        force pass, possibly summed over ranks); returns dt."""
+        v = C.c_double()
+        self._check(self._lib.pt_advance(self._h, C.byref(v)))
+        return v.value
+
+    def bucket_work(self):
+        """P2P pairs + P2C evaluations per bucket (DFS order) of the last pass."""
+        nn, nb = C.c_int64(), C.c_int64()
+        self._check(self._lib.pt_get_tree_size(self._h, C.byref(nn), C.byref(nb)))
+        w = np.zeros(nb.value, np.uint64)
+        if nb.value:
+            self._check(self._lib.pt_get_bucket_work(self._h, L.ptr(w)))
+        return w
+
     def state(self):
         out = {k: np.empty(self.n) for k in ("x", "y", "z", "vx", "vy", "vz")}
         self._check(self._lib.pt_get_state(self._h, *[L.ptr(out[k]) for k in ("x", "y", "z", "vx", "vy", "vz")]))

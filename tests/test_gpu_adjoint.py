@@ -104,9 +104,10 @@ def test_autograd_function_wrapper():
         g = pos.grad.numpy()
         # the same gradient from the C ABI directly
         ref = s.adjoint(*w.numpy())
-    # the adjoint adds source terms with FP64 atomics: equal up to summation order
-    assert np.allclose(g[0], ref["gx"], rtol=1e-12, atol=1e-14)
-    assert np.allclose(mass.grad.numpy(), ref["gm"], rtol=1e-12, atol=1e-14)
+    # the adjoint adds source terms with FP64 atomics: equal up to summation
+    # order, so entries that cancel are compared against the array's scale
+    for got, want in ((g[0], ref["gx"]), (g[1], ref["gy"]), (g[2], ref["gz"]), (mass.grad.numpy(), ref["gm"])):
+        assert np.allclose(got, want, rtol=1e-12, atol=1e-12 * np.abs(want).max())
 
 
 def test_chain_gradient_matches_finite_differences():
