@@ -253,7 +253,7 @@ def main():
     torch.cuda.synchronize()
     barrier(world)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
-    trav_ms, cnts = [], None
+    trav_ms, cnts, launches = [], None, 0
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
         barrier(world)
@@ -263,6 +263,7 @@ def main():
             ev[k][1].record(stream)
             c = sim.counters()
             trav_ms.append(c["ms_traverse"])
+            launches += int(c["launches"])  # kernels the library launched for this pass
             cnts = c
         torch.cuda.synchronize()
     step_ms = [s.elapsed_time(e) for s, e in ev]
@@ -270,7 +271,6 @@ def main():
     t = max_over_ranks(t_local, world)
     barrier(world)
     value = n * a.steps / t
-    launches = gpu_launches(cnts)
 
     # roofline of the traversal (dominant kernel)
     flops = 20.0 * cnts["n_pp"] + 66.0 * cnts["n_pc"]
@@ -283,8 +283,14 @@ def main():
     lanes = 128 if a.precision == "mixed" else 64
     peak_tf = nsm * lanes * 2 * sm_max * 1e6 / 1e12
     achieved = flops / t_trav / 1e12
+    traffic = traversal_traffic(a)
+    hbm = peaks.get("hbm_gbs") or 6650.0
     roofline = {"bound": "fp32" if a.precision == "mixed" else "fp64", "achieved": achieved,
-                "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf, "traffic": None,
+                "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf, "traffic": traffic,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "
+                                  "(profiles/traffic_traverse_mixed_plummer_16m.md)" if traffic else None,
+                "dram_gbs": (traffic / t_trav / 1e9) if traffic else None,
+                "dram_frac_of_hbm": (traffic / t_trav / 1e9 / hbm) if traffic else None,
                 "kernel": f"traverse_{a.precision}", "flops_per_launch": flops,
                 "flop_model": "20 per P2P pair + 66 per P2C evaluation",
                 "peak_source": f"nominal: {nsm} SMs x {lanes} {'FP32' if lanes == 128 else 'FP64'} lanes x 2 x "
@@ -294,13 +300,14 @@ def main():
            "warmup": a.warmup, "ms_per_step": t * 1e3 / a.steps, "higher_is_better": True,
            "scaling": "strong", "vs_baseline": None, "dtype": "f32 interactions / f64 tree"
            if a.precision == "mixed" else "f64", "data": "synthetic (seeded Plummer sphere)",
-           "config": workload_config(a, world), "gpu_launches": launches * a.steps,
+           "config": workload_config(a, world), "gpu_launches": launches,
            "roofline": roofline, "clocks": clocks,
            "phases_ms": {k: cnts[k] for k in ("ms_keys", "ms_sort", "ms_build", "ms_upward", "ms_traverse",
                                               "ms_total")},
            "interactions": {"n_pp": cnts["n_pp"], "n_pc": cnts["n_pc"], "n_open": cnts["n_open"],
                             "n_nodes": cnts["n_nodes"], "n_buckets": cnts["n_buckets"]},
-           "interactions_per_s": (cnts["n_pp"] + cnts["n_pc"]) / t_trav}
+           "interactions_per_s": (cnts["n_pp"] + cnts["n_pc"]) / t_trav,
+           "phases_roofline": phase_rooflines(cnts, n, peaks)}
 
     if not a.no_extras:
         out.update(extras(a, sim, p, world, rank, stream, value, shard))
@@ -311,6 +318,40 @@ def main():
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0
+
+
+# DRAM bytes (read + write) of one traverse_mixed launch on the default
+# workload (Plummer N = 2^24, bucket 32, theta 0.7), from
+# ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum (1 pass);
+# profiles/traffic_traverse_mixed_plummer_16m.md holds the command and figures.
+TRAVERSE_MIXED_TRAFFIC_16M = 1479119104 + 677974784
+
+
+def traversal_traffic(a):
+    """Measured DRAM bytes per traversal launch, scaled by particles from the
+    captured workload; None for other workloads."""
+    if (a.workload, a.theta, a.bucket, a.precision, a.soft) == ("plummer", 0.7, 32, "mixed", 1e-3):
+        return TRAVERSE_MIXED_TRAFFIC_16M * a.n / float(1 << 24)
+    return None
+
+
+def phase_rooflines(c, n, peaks):
+    """HBM roofline of the bandwidth-bound phases of the last pass: their
+    algorithmic bytes (keys 36 B/particle; sort 8 + 8 x 24 B and permute of
+    the eight FP64 arrays + order 132 B per particle; build 8 B/particle +
+    32 B/node; upward 32 B/particle + 160 B/node) over the phase's event time,
+    against the measured copy bandwidth."""
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    nodes = c["n_nodes"]
+    rows = {"keys": (36.0 * n, c["ms_keys"]), "sort_permute": ((200.0 + 132.0) * n, c["ms_sort"]),
+            "build": (8.0 * n + 32.0 * nodes, c["ms_build"]), "upward": (32.0 * n + 160.0 * nodes, c["ms_upward"])}
+    out = {}
+    for k, (b, ms) in rows.items():
+        gbs = b / (ms / 1e3) / 1e9 if ms > 0 else None
+        out[k] = {"bytes": b, "ms": ms, "achieved_gbs": gbs, "frac": (gbs / hbm) if gbs else None}
+    out["peak_gbs"] = hbm
+    out["peak_source"] = "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks.get("hbm_gbs") else "fallback 6650 GB/s"
+    return out
 
 
 def theta_sweep(a, sim, tgt, direct, stream):
@@ -343,16 +384,6 @@ def theta_sweep(a, sim, tgt, direct, stream):
     sim.set_theta(a.theta)
     sim.set_precision(a.precision)
     return rows
-
-
-def gpu_launches(c):
-    """Kernels of our library launched by one force pass (counted from the
-    pass structure: keys 3, sort 8x(3 + scan) + 9 gathers, build per level,
-    upward per level, traversal 1)."""
-    levels = int(c["depth"]) + 2
-    scan_kernels = 3
-    n = 3 + 8 * (2 + scan_kernels + 1) + 9 + 1 + levels * (1 + scan_kernels + 1) + 2 * levels + 1 + 1 + levels + 1 + 1
-    return n
 
 
 def extras(a, sim, p, world, rank, stream, value, shard=None):

@@ -94,7 +94,7 @@ typedef struct pt_counters {
   int64_t n_nodes;
   int64_t n_buckets;
   int32_t depth;       /* deepest level */
-  int32_t reserved;
+  int32_t launches;    /* kernels this library launched for the pass */
   /* device milliseconds of the last force pass, by phase */
   float ms_keys;       /* bbox + universe + keys */
   float ms_sort;       /* radix sort + permute */

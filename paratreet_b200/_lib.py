@@ -56,7 +56,7 @@ class PtCounters(C.Structure):
         ("n_nodes", C.c_int64),
         ("n_buckets", C.c_int64),
         ("depth", C.c_int32),
-        ("reserved", C.c_int32),
+        ("launches", C.c_int32),
         ("ms_keys", C.c_float),
         ("ms_sort", C.c_float),
         ("ms_build", C.c_float),

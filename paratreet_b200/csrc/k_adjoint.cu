@@ -244,9 +244,12 @@ __global__ void __launch_bounds__(kAdjWarps * 32) adjoint_upward(AdjParams A) {
 }
 
 void launch_adjoint(const AdjParams& A, int grid, cudaStream_t st) {
+  note_launch();
   adjoint_lists<<<grid, kAdjWarps * 32, 0, st>>>(A);
-  if (A.nbuckets > 0)
+  if (A.nbuckets > 0) {
+    note_launch();
     adjoint_upward<<<(unsigned)((A.nbuckets * 32 + kAdjWarps * 32 - 1) / (kAdjWarps * 32)), kAdjWarps * 32, 0, st>>>(A);
+  }
 }
 
 }  // namespace pt

@@ -135,28 +135,33 @@ __global__ void __launch_bounds__(256) assign_buckets(Nodes nd, int64_t nnodes, 
 
 static inline unsigned blocks_for(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
 
-void launch_init_root(Nodes nd, int64_t n, int bucket, cudaStream_t st) { init_root<<<1, 32, 0, st>>>(nd, n, bucket); }
+void launch_init_root(Nodes nd, int64_t n, int bucket, cudaStream_t st) {
+  note_launch();
+  init_root<<<1, 32, 0, st>>>(nd, n, bucket);
+}
 
 void launch_flag_internal(const int32_t* type, int64_t begin, int64_t count, uint32_t* flags, cudaStream_t st) {
-  if (count > 0) flag_internal<<<blocks_for(count), 256, 0, st>>>(type, begin, count, flags);
+  if (count > 0) { note_launch(); flag_internal<<<blocks_for(count), 256, 0, st>>>(type, begin, count, flags); }
 }
 
 void launch_build_children(Nodes nd, const uint64_t* keys, int64_t begin, int64_t count, const uint32_t* rank,
                            int64_t next_begin, int bucket, int64_t cap, unsigned* status, cudaStream_t st) {
-  if (count > 0)
+  if (count > 0) {
+    note_launch();
     build_children<<<blocks_for(count), 256, 0, st>>>(nd, keys, begin, count, rank, next_begin, bucket, cap, status);
+  }
 }
 
 void launch_count_subtree(Nodes nd, int64_t begin, int64_t count, cudaStream_t st) {
-  if (count > 0) count_subtree<<<blocks_for(count), 256, 0, st>>>(nd, begin, count);
+  if (count > 0) { note_launch(); count_subtree<<<blocks_for(count), 256, 0, st>>>(nd, begin, count); }
 }
 
 void launch_base_topdown(Nodes nd, int64_t begin, int64_t count, cudaStream_t st) {
-  if (count > 0) base_topdown<<<blocks_for(count), 256, 0, st>>>(nd, begin, count);
+  if (count > 0) { note_launch(); base_topdown<<<blocks_for(count), 256, 0, st>>>(nd, begin, count); }
 }
 
 void launch_assign_buckets(Nodes nd, int64_t nnodes, int32_t* buckets, int nleaves, cudaStream_t st) {
-  if (nnodes > 0) assign_buckets<<<blocks_for(nnodes), 256, 0, st>>>(nd, nnodes, buckets, nleaves);
+  if (nnodes > 0) { note_launch(); assign_buckets<<<blocks_for(nnodes), 256, 0, st>>>(nd, nnodes, buckets, nleaves); }
 }
 
 }  // namespace pt

@@ -251,23 +251,25 @@ __global__ void __launch_bounds__(128) ewald_recip(const double* __restrict__ x,
 
 void launch_ewald_correction(Particles p, int64_t i0, int64_t i1, const EwaldRoot& R, const double4* htab,
                              cudaStream_t st) {
-  if (i1 > i0) ewald_correction<<<(unsigned)((i1 - i0 + 127) / 128), 128, 0, st>>>(p, i0, i1, R, htab);
+  if (i1 > i0) { note_launch(); ewald_correction<<<(unsigned)((i1 - i0 + 127) / 128), 128, 0, st>>>(p, i0, i1, R, htab); }
 }
 void launch_ewald_structure(const double* x, const double* y, const double* z, const double* m, int64_t n,
                             const double4* kv, int nk, double* S, cudaStream_t st) {
-  if (nk > 0) ewald_structure<<<nk, 256, 0, st>>>(x, y, z, m, n, kv, nk, S);
+  if (nk > 0) { note_launch(); ewald_structure<<<nk, 256, 0, st>>>(x, y, z, m, n, kv, nk, S); }
 }
 void launch_ewald_real(const double* x, const double* y, const double* z, const double* m, const double* soft,
                        int64_t n, const int32_t* tgt, int64_t nt, int nsplit, double L, double alpha, double rcut,
                        double* part, cudaStream_t st) {
   dim3 grid((unsigned)((nt + kEwTile - 1) / kEwTile), nsplit);
-  if (nt > 0) ewald_real<<<grid, kEwTile, 0, st>>>(x, y, z, m, soft, n, tgt, nt, nsplit, L, alpha, rcut, part);
+  if (nt > 0) { note_launch(); ewald_real<<<grid, kEwTile, 0, st>>>(x, y, z, m, soft, n, tgt, nt, nsplit, L, alpha, rcut, part); }
 }
 void launch_ewald_recip(const double* x, const double* y, const double* z, const double* m, const int32_t* tgt,
                         int64_t nt, const double4* kv, int nk, const double* S, double alpha, double V, double* out,
                         cudaStream_t st) {
-  if (nt > 0)
+  if (nt > 0) {
+    note_launch();
     ewald_recip<<<(unsigned)((nt + 127) / 128), 128, 0, st>>>(x, y, z, m, tgt, nt, kv, nk, S, alpha, V, out);
+  }
 }
 
 }  // namespace pt

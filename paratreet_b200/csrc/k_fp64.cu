@@ -584,32 +584,38 @@ __global__ void __launch_bounds__(kDirTile) direct_sum_f64(const double* __restr
 static inline unsigned blocks_for(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
 
 void launch_leaf_moments(Nodes nd, int64_t nnodes, Particles p, cudaStream_t st) {
-  if (nnodes > 0) leaf_moments<<<blocks_for(nnodes), 256, 0, st>>>(nd, nnodes, p);
+  if (nnodes > 0) { note_launch(); leaf_moments<<<blocks_for(nnodes), 256, 0, st>>>(nd, nnodes, p); }
 }
 void launch_upward_level(Nodes nd, int64_t begin, int64_t count, cudaStream_t st) {
-  if (count > 0) upward_level<<<blocks_for(count, 128), 128, 0, st>>>(nd, begin, count);
+  if (count > 0) { note_launch(); upward_level<<<blocks_for(count, 128), 128, 0, st>>>(nd, begin, count); }
 }
 void launch_finalize(Nodes nd, int64_t nnodes, double gfac, int want_f32, cudaStream_t st) {
-  if (nnodes > 0) finalize_records<<<blocks_for(nnodes), 256, 0, st>>>(nd, nnodes, gfac, want_f32);
+  if (nnodes > 0) { note_launch(); finalize_records<<<blocks_for(nnodes), 256, 0, st>>>(nd, nnodes, gfac, want_f32); }
 }
 void launch_traverse_f64(const TravParams& P, const Mom* mom, int grid, cudaStream_t st) {
+  note_launch();
   traverse_f64<<<grid, kTravWarps * 32, 0, st>>>(P, mom);
 }
 void launch_replay_f64(const TravParams& P, int grid, cudaStream_t st) {
+  note_launch();
   replay_f64<<<grid, kTravWarps * 32, 0, st>>>(P);
 }
 void launch_kick_perturb(Particles p, int64_t n, double dt, int grid, cudaStream_t st) {
+  note_launch();
   kick_perturb<<<grid, 256, 0, st>>>(p, n, dt);
 }
 void launch_kick_half(Particles p, int64_t n, double dt, int grid, cudaStream_t st) {
+  note_launch();
   kick_half<<<grid, 256, 0, st>>>(p, n, dt);
 }
 void launch_drift(Particles p, int64_t n, double dt, int grid, cudaStream_t st) {
+  note_launch();
   drift<<<grid, 256, 0, st>>>(p, n, dt);
 }
 void launch_direct_sum(const double* x, const double* y, const double* z, const double* m, const double* soft,
                        int64_t n, const int32_t* tgt, int64_t nt, int nsplit, double* part, cudaStream_t st) {
   dim3 grid(blocks_for(nt, kDirTile), nsplit);
+  note_launch();
   direct_sum_f64<<<grid, kDirTile, 0, st>>>(x, y, z, m, soft, n, tgt, nt, nsplit, part);
 }
 

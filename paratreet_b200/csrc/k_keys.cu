@@ -127,17 +127,21 @@ __global__ void __launch_bounds__(256) vmax2_kernel(const double* __restrict__ v
 
 void launch_bbox(const double* x, const double* y, const double* z, int64_t n, double* partial, int nblocks,
                  double* uni, unsigned* status, cudaStream_t st) {
+  note_launch();
   bbox_partial<<<nblocks, 256, 0, st>>>(x, y, z, n, partial, status);
+  note_launch();
   bbox_final<<<1, 32, 0, st>>>(partial, nblocks, uni);
 }
 
 void launch_keys(const double* x, const double* y, const double* z, int64_t n, const double* uni, uint64_t* key,
                  uint32_t* idx, int grid, cudaStream_t st) {
+  note_launch();
   make_keys<<<grid, 256, 0, st>>>(x, y, z, n, uni, key, idx);
 }
 
 void launch_vmax2(const double* vx, const double* vy, const double* vz, int64_t n, unsigned long long* out,
                   int grid, cudaStream_t st) {
+  note_launch();
   vmax2_kernel<<<grid, 256, 0, st>>>(vx, vy, vz, n, out);
 }
 

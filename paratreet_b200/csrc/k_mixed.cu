@@ -533,13 +533,14 @@ void launch_prep_sources(const int32_t* buckets, int64_t nbuckets, const WalkRec
                          float* softf, cudaStream_t st) {
   if (nbuckets <= 0) return;
   int64_t threads = nbuckets * 32;
+  note_launch();
   prep_sources<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(buckets, nbuckets, walk, p, srcf, softf);
 }
 
 // variant: 0 = at most 6 CTAs/SM (80 registers), 1 = 5 CTAs/SM (no spills)
 void launch_traverse_mixed(const TravParams& P, const Mom* mom, int grid, int variant, cudaStream_t st) {
-  if (variant == 1) traverse_mixed<5><<<grid, kMixWarps * 32, 0, st>>>(P, mom);
-  else traverse_mixed<6><<<grid, kMixWarps * 32, 0, st>>>(P, mom);
+  if (variant == 1) { note_launch(); traverse_mixed<5><<<grid, kMixWarps * 32, 0, st>>>(P, mom); }
+  else { note_launch(); traverse_mixed<6><<<grid, kMixWarps * 32, 0, st>>>(P, mom); }
 }
 
 }  // namespace pt

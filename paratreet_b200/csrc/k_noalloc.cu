@@ -179,7 +179,9 @@ extern "C" int pt_direct_sum_noalloc(int64_t n, const double* x, const double* y
     return PT_E_CUDA;
   }
   dim3 grid((unsigned)tb, (unsigned)nsplit);
+  note_launch();
   noalloc_direct<<<grid, kNoAllocTile, 0, st>>>(x, y, z, m, soft, n, targets, nt, (int)nsplit, part, status);
+  note_launch();
   noalloc_reduce<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(part, (int)nsplit, nt, ax, ay, az, pot);
   unsigned h_status = 0;
   cudaError_t e = cudaGetLastError();

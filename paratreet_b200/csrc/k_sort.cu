@@ -281,11 +281,14 @@ void scan_exclusive(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* scra
   cudaMemcpyAsync(last, in + (n - 1), sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
   uint32_t* sums = scratch + 16;
   int64_t tiles = (n + kScanTile - 1) / kScanTile;
+  note_launch();
   scan_tiles<<<(unsigned)tiles, kScanThreads, 0, st>>>(in, out, n, sums);
   if (tiles > 1) {
     scan_exclusive(sums, sums, tiles, sums + tiles + 1, sums + tiles, st);
+    note_launch();
     scan_add<<<(unsigned)tiles, kScanThreads, 0, st>>>(out, n, sums);
   }
+  note_launch();
   scan_total<<<1, 32, 0, st>>>(last, out + (n - 1), 1, total);
 }
 
@@ -318,12 +321,15 @@ int radix_sort_pairs(uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, int
                            (int)sizeof(OnesweepShared)) != cudaSuccess)
     return -1;
   cudaMemsetAsync(ghist, 0, align256(8 * 256 * sizeof(uint32_t)) + align256(8 * sizeof(uint32_t)), st);
+  note_launch();
   radix_histograms<<<sms * 4, kSortThreads, 0, st>>>(k0, n, ghist);
+  note_launch();
   radix_digit_offsets<<<8, 256, 0, st>>>(ghist);
   uint64_t *ka = k0, *kb = k1;
   uint32_t *va = v0, *vb = v1;
   for (int pass = 0; pass < 8; pass++) {
     cudaMemsetAsync(look, 0, look_bytes, st);
+    note_launch();
     radix_onesweep<<<tiles, kSortThreads, sizeof(OnesweepShared), st>>>(
         ka, va, kb, vb, n, 8 * pass, ghist + 256 * pass, counters + pass, look, status);
     uint64_t* tk = ka; ka = kb; kb = tk;
@@ -342,9 +348,11 @@ __global__ void __launch_bounds__(256) gather_kernel(const T* __restrict__ in, T
 }
 
 void gather_f64(const double* in, double* out, const uint32_t* idx, int64_t n, int grid, cudaStream_t st) {
+  note_launch();
   gather_kernel<double><<<grid, 256, 0, st>>>(in, out, idx, n);
 }
 void gather_i32(const int32_t* in, int32_t* out, const uint32_t* idx, int64_t n, int grid, cudaStream_t st) {
+  note_launch();
   gather_kernel<int32_t><<<grid, 256, 0, st>>>(in, out, idx, n);
 }
 

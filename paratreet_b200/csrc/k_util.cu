@@ -53,32 +53,32 @@ __global__ void __launch_bounds__(256) axpy1_kernel(int64_t n, double alpha, con
 }
 
 void launch_axpy1(int64_t n, double alpha, const double* x, double* y, int grid, cudaStream_t st) {
-  if (n > 0) axpy1_kernel<<<grid, 256, 0, st>>>(n, alpha, x, y);
+  if (n > 0) { note_launch(); axpy1_kernel<<<grid, 256, 0, st>>>(n, alpha, x, y); }
 }
 void launch_axpy3(int64_t n, double alpha, const double* x0, const double* x1, const double* x2, double* y0,
                   double* y1, double* y2, int grid, cudaStream_t st) {
-  if (n > 0) axpy3_kernel<<<grid, 256, 0, st>>>(n, alpha, x0, x1, x2, y0, y1, y2);
+  if (n > 0) { note_launch(); axpy3_kernel<<<grid, 256, 0, st>>>(n, alpha, x0, x1, x2, y0, y1, y2); }
 }
 void launch_gather_by_order(const double* in, double* out, const int32_t* order, int64_t n, int grid,
                             cudaStream_t st) {
-  if (n > 0) gather_by_order<<<grid, 256, 0, st>>>(in, out, order, n);
+  if (n > 0) { note_launch(); gather_by_order<<<grid, 256, 0, st>>>(in, out, order, n); }
 }
 
 void launch_scatter_f64(const double* in, double* out, const int32_t* order, int64_t n, int grid, cudaStream_t st) {
-  if (n > 0) scatter_kernel<double><<<grid, 256, 0, st>>>(in, out, order, n);
+  if (n > 0) { note_launch(); scatter_kernel<double><<<grid, 256, 0, st>>>(in, out, order, n); }
 }
 void launch_scatter_u64(const uint64_t* in, uint64_t* out, const int32_t* order, int64_t n, int grid,
                         cudaStream_t st) {
-  if (n > 0) scatter_kernel<uint64_t><<<grid, 256, 0, st>>>(in, out, order, n);
+  if (n > 0) { note_launch(); scatter_kernel<uint64_t><<<grid, 256, 0, st>>>(in, out, order, n); }
 }
 void launch_iota_i32(int32_t* out, int64_t n, int grid, cudaStream_t st) {
-  if (n > 0) iota_kernel<<<grid, 256, 0, st>>>(out, n);
+  if (n > 0) { note_launch(); iota_kernel<<<grid, 256, 0, st>>>(out, n); }
 }
 void launch_inverse_perm(const int32_t* order, int32_t* inv, int64_t n, int grid, cudaStream_t st) {
-  if (n > 0) inverse_kernel<<<grid, 256, 0, st>>>(order, inv, n);
+  if (n > 0) { note_launch(); inverse_kernel<<<grid, 256, 0, st>>>(order, inv, n); }
 }
 void launch_map_index(const int32_t* inv, const int32_t* in, int32_t* out, int64_t n, cudaStream_t st) {
-  if (n > 0) map_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(inv, in, out, n);
+  if (n > 0) { note_launch(); map_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(inv, in, out, n); }
 }
 
 }  // namespace pt

@@ -9,6 +9,7 @@
 // The host reads back one 4-byte count per tree level (to size the next
 // level) and the status word at the end; everything else stays on the device.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -85,6 +86,14 @@ struct pt_handle {
   double* nadj = nullptr;  // 10 adjoint values per node
   int64_t nadj_cap = 0;
 };
+
+namespace pt {
+namespace {
+std::atomic<unsigned long long> g_launches{0};
+}
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+unsigned long long launches_so_far() { return g_launches.load(std::memory_order_relaxed); }
+}  // namespace pt
 
 namespace {
 
@@ -495,6 +504,7 @@ int traverse(pt_handle* h, int64_t b0, int64_t b1) {
 
 int forces(pt_handle* h, int64_t b0, int64_t b1) {
   if (!h->p.x) return fail(h, PT_E_STATE, "no particles: call pt_set_particles first");
+  const unsigned long long launches0 = launches_so_far();
   cudaStream_t st = h->stream;
   CK(cudaEventRecord(h->ev[0], st));
   if (h->n == 0) {
@@ -519,6 +529,7 @@ int forces(pt_handle* h, int64_t b0, int64_t b1) {
   k.n_nodes = h->nnodes;
   k.n_buckets = h->nbuckets;
   k.depth = (int32_t)h->lev.size() - 2;
+  k.launches = (int32_t)(launches_so_far() - launches0);
   CK(cudaEventElapsedTime(&k.ms_keys, h->ev[0], h->ev[1]));
   CK(cudaEventElapsedTime(&k.ms_sort, h->ev[1], h->ev[2]));
   CK(cudaEventElapsedTime(&k.ms_build, h->ev[2], h->ev[3]));

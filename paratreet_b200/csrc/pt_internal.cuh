@@ -7,6 +7,12 @@
 
 namespace pt {
 
+// Host-side count of this library's kernel launches (process-wide); every
+// launch site calls note_launch() right before it launches.
+void note_launch();
+unsigned long long launches_so_far();
+
+
 constexpr int kMaxDepth = 21;          // 63 key bits / 3 (src/common.h:29-31)
 constexpr int kTypeLeaf = 1;           // Node<Data>::Type numbering, src/Node.h:82-95
 constexpr int kTypeEmpty = 2;
