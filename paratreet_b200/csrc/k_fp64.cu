@@ -377,7 +377,6 @@ __global__ void __launch_bounds__(kTravWarps * 32) traverse_f64(TravParams P, co
     // A bucket holds more than 32 particles only when more than `bucket`
     // particles share one 63-bit key (depth-21 leaf); its targets are then
     // walked in chunks of 32 (the decisions depend on the bucket only).
-    const unsigned long long work0 = c_pp + c_pc;
     for (int tc = 0; tc < ntot; tc += 32) {
       const int t0 = tbase + tc, nt = min(32, ntot - tc);
       unsigned long long opens = 0;
@@ -425,10 +424,11 @@ __global__ void __launch_bounds__(kTravWarps * 32) traverse_f64(TravParams P, co
       }
       c_pp += ev.n_pp;
       c_pc += ev.n_pc;
-    }
-    if (P.bucket_work && lane == 0) {
-      const unsigned long long wk = c_pp + c_pc - work0;
-      P.bucket_work[b] = P.accumulate ? P.bucket_work[b] + wk : wk;
+      if (P.bucket_work && lane == 0) {  // this chunk's interactions, added to the bucket's
+        unsigned long long wk = ev.n_pp + ev.n_pc;
+        if (tc > 0 || P.accumulate) wk += P.bucket_work[b];
+        P.bucket_work[b] = wk;
+      }
     }
   }
   if (lane == 0) {

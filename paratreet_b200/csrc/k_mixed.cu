@@ -22,13 +22,18 @@
 //           appended to shared-memory buffers with their FP32 offsets, opened
 //           nodes to a per-warp LIFO.  The interaction order is not the
 //           reference's (only the FP64 form keeps it).
-//  eval     the bucket's n_t targets are replicated over G = 32 / T lane
-//           groups (T = next power of two >= n_t); group g takes every G-th
-//           source / node of a 32-entry chunk staged in shared memory, so a
-//           10-particle bucket keeps all 32 lanes busy.  Leaves whose nearest
+//  eval     the bucket's n_t targets are replicated over G = floor(32 / n_t)
+//           lane groups; group g takes every G-th source pair / node pair of
+//           a 64-entry chunk staged in shared memory as interleaved pairs, so
+//           a 10-particle bucket keeps 30 lanes busy and each lane evaluates
+//           two interactions per packed FP32 instruction (f32x2 add / mul /
+//           fma, two operations per issue slot).  Leaves whose nearest
 //           particle pair is provably beyond the softening length take a
-//           branch-free Newtonian loop (rsqrt on the SFU).
-//  reduce   per-lane Kahan sums -> FP64, butterfly over the G groups.
+//           branch-free Newtonian loop (rsqrt on the SFU).  The flushes are
+//           out-of-line functions (targets in, partial sums out by value) so
+//           that their loops get the register budget the walk state would
+//           otherwise hold.
+//  reduce   per-lane Kahan sums -> FP64, sum over the G groups.
 #include "pt_internal.cuh"
 #include "pt_walk.cuh"
 
@@ -59,12 +64,11 @@ struct MixWarp {
   float kahan[8][32];       // per-lane compensated sums (s, c) of ax, ay, az, pot
   int32_t pre[kMixBuf + 1]; // prefix of leaf sizes during a P2P flush
   int32_t ps0[kMixBuf];     // first particle of each buffered leaf
-  float4 src[32];           // staged sources: x, y, z (rel. bucket), m
-  float ssoft[32];
-  float sreach2[32];        // (soft_j + max bucket softening)^2: beyond it a pair is unsoftened
-  float4 qa[32];            // staged P2C: offset xyz, mass
-  float4 qb[32];            // xx, xy, xz, yy
-  float4 qc[32];            // yz, zz, soft (< 0: monopole), trace/2
+  float4 px[32];            // staged source pairs: x_a, x_b, y_a, y_b (rel. bucket)
+  float4 pz[32];            // z_a, z_b, m_a, m_b
+  float4 pr[32];            // near leaves: reach2_a, reach2_b, soft_a, soft_b; beyond
+                            // reach2 = (soft_j + max bucket softening)^2 a pair is unsoftened
+  float4 qp[6][32];         // staged P2C node pairs (see flush_p2c)
 };
 
 // SPLINE in FP32, softened branch (r < twoh): kept out of line so that the
@@ -151,11 +155,44 @@ struct MixCtx {
   }
 };
 
+// One source of a near leaf: Newtonian beyond the softening reach, the spline
+// inside it, nothing for the particle itself (r2 == 0).  pp sums +m a.
+__device__ __forceinline__ void near_pair(float m, float dx, float dy, float dz, float r2, float reach2,
+                                          float ssoft, float ts, float& ax, float& ay, float& az, float& pp) {
+  if (r2 > reach2) {
+    const float rinv = rsqrtf(r2);
+    const float mr = m * rinv;
+    const float mr3 = mr * rinv * rinv;
+    ax += dx * mr3;
+    ay += dy * mr3;
+    az += dz * mr3;
+    pp += mr;
+  } else if (r2 > 0.f) {
+    const float rinv = rsqrtf(r2);
+    float a, b;
+    spline_f32(r2, rinv, ssoft + ts, a, b);
+    const float bm = b * m;
+    ax += dx * bm;
+    ay += dy * bm;
+    az += dz * bm;
+    pp += m * a;
+  }
+}
+
 // Evaluate all buffered P2P leaves of one kind (far: no pair can be softened).
+// Sources are staged 64 per chunk as 32 interleaved pairs, px = (x_a, x_b,
+// y_a, y_b), pz = (z_a, z_b, m_a, m_b): each half of a 128-bit shared load is
+// an aligned register pair, so a lane evaluates two sources against its
+// target with the packed FP32 instructions (two FP32 operations per issue).
+// Missing sources of the last pair have zero mass at a far position.
+struct FlushIn {
+  float tx, ty, tz, ts;
+  int lane, grp, G;
+};
 template <bool kFar>
-__device__ __forceinline__ void flush_p2p(MixWarp& w, const float4* __restrict__ buf, int nleaves,
-                                          const WalkRec* __restrict__ walk, const float4* __restrict__ srcf,
-                                          const float* __restrict__ softf, MixCtx& x) {
+__device__ __noinline__ float4 flush_p2p_nl(MixWarp& w, const float4* __restrict__ buf, int nleaves,
+                                            const WalkRec* __restrict__ walk, const float4* __restrict__ srcf,
+                                            const float* __restrict__ softf, const FlushIn x, int& total_out) {
   // prefix of leaf sizes (nleaves <= 64: two entries per lane)
   int s0a = 0, s0b = 0, na = 0, nb = 0;
   if (x.lane < nleaves) { const WalkRec& r = walk[entry_node(buf[x.lane])]; s0a = r.pstart; na = r.pcount; }
@@ -172,101 +209,90 @@ __device__ __forceinline__ void flush_p2p(MixWarp& w, const float4* __restrict__
   if (x.lane + 32 < nleaves) { w.pre[x.lane + 32] = tota + incb - nb; w.ps0[x.lane + 32] = s0b; }
   if (x.lane == 0) w.pre[nleaves] = total;
   __syncwarp();
-  // Chunks of 32 sources; the loads of chunk k+1 are issued before chunk k is
-  // evaluated so that their L2 latency overlaps the arithmetic.
+  const float kPadPos = 1.0e10f;
   int base_leaf = 0;  // leaf holding the next chunk's first source
-  float4 nraw = make_float4(0.f, 0.f, 0.f, 0.f), noff = nraw;
-  float nsoft = 0.f;
+  float4 ra, rb, oa, ob;
+  float sa = 0.f, sb = 0.f;
   auto fetch = [&](int cs) {
-    const int q = cs + x.lane;
+    const int q0 = cs + 2 * x.lane;
     int lo = base_leaf;  // last leaf with pre <= q: a chunk spans few leaves
-    while (lo + 1 < nleaves && w.pre[lo + 1] <= q) lo++;
-    base_leaf = __shfl_sync(kFull, lo, 31);
-    if (q < total) {
-      noff = buf[lo];
-      const int j = w.ps0[lo] + (q - w.pre[lo]);
-      nraw = srcf[j];
-      if (!kFar) nsoft = softf[j];
+    while (lo + 1 < nleaves && w.pre[lo + 1] <= q0) lo++;
+    int lo1 = lo;
+    while (lo1 + 1 < nleaves && w.pre[lo1 + 1] <= q0 + 1) lo1++;
+    base_leaf = __shfl_sync(kFull, lo1, 31);
+    ra = rb = make_float4(kPadPos, kPadPos, kPadPos, 0.f);
+    oa = ob = make_float4(0.f, 0.f, 0.f, 0.f);
+    sa = sb = 0.f;
+    if (q0 < total) {
+      oa = buf[lo];
+      const int j = w.ps0[lo] + (q0 - w.pre[lo]);
+      ra = srcf[j];
+      if (!kFar) sa = softf[j];
+    }
+    if (q0 + 1 < total) {
+      ob = buf[lo1];
+      const int j = w.ps0[lo1] + (q0 + 1 - w.pre[lo1]);
+      rb = srcf[j];
+      if (!kFar) sb = softf[j];
     }
   };
   fetch(0);
-  for (int cs = 0; cs < total; cs += 32) {
-    if (cs + x.lane < total) {
-      w.src[x.lane] = make_float4(nraw.x + noff.x, nraw.y + noff.y, nraw.z + noff.z, nraw.w);
-      if (!kFar) {
-        w.ssoft[x.lane] = nsoft;
-        const float rr = nsoft + (float)w.geom.soft_max;
-        w.sreach2[x.lane] = rr * rr;
-      }
+  const float2 ntx = make_float2(-x.tx, -x.tx), nty = make_float2(-x.ty, -x.ty), ntz = make_float2(-x.tz, -x.tz);
+  float2 ax2 = make_float2(0.f, 0.f), ay2 = ax2, az2 = ax2, pp2 = ax2;  // pp2 sums +m/r
+  for (int cs = 0; cs < total; cs += 64) {
+    w.px[x.lane] = make_float4(ra.x + oa.x, rb.x + ob.x, ra.y + oa.y, rb.y + ob.y);
+    w.pz[x.lane] = make_float4(ra.z + oa.z, rb.z + ob.z, ra.w, rb.w);
+    if (!kFar) {
+      const float gs = (float)w.geom.soft_max;
+      const float qa = sa + gs, qb = sb + gs;
+      // a padded source (zero mass) takes the Newtonian branch
+      w.pr[x.lane] = make_float4(ra.w != 0.f ? qa * qa : -1.f, rb.w != 0.f ? qb * qb : -1.f, sa, sb);
     }
     __syncwarp();
-    if (cs + 32 < total) fetch(cs + 32);
-    const int cnt = min(32, total - cs);
-    if (kFar && x.grp < x.G) {
-      float bx = 0.f, by = 0.f, bz = 0.f, bp = 0.f;  // second chain
-      int jj = x.grp;
-      for (; jj + x.G < cnt; jj += 2 * x.G) {
-        const float4 s = w.src[jj];
-        const float4 u = w.src[jj + x.G];
-        const float dx = s.x - x.tx, dy = s.y - x.ty, dz = s.z - x.tz;
-        const float ex = u.x - x.tx, ey = u.y - x.ty, ez = u.z - x.tz;
-        const float r2 = dx * dx + dy * dy + dz * dz;
-        const float q2 = ex * ex + ey * ey + ez * ez;
-        const float rinv = rsqrtf(r2), qinv = rsqrtf(q2);
-        const float mr = s.w * rinv, mq = u.w * qinv;
-        const float mr3 = mr * rinv * rinv, mq3 = mq * qinv * qinv;
-        x.pax += dx * mr3;
-        x.pay += dy * mr3;
-        x.paz += dz * mr3;
-        x.ppf -= mr;
-        bx += ex * mq3;
-        by += ey * mq3;
-        bz += ez * mq3;
-        bp -= mq;
-      }
-      if (jj < cnt) {
-        const float4 s = w.src[jj];
-        const float dx = s.x - x.tx, dy = s.y - x.ty, dz = s.z - x.tz;
-        const float r2 = dx * dx + dy * dy + dz * dz;
-        const float rinv = rsqrtf(r2);
-        const float mr = s.w * rinv;
-        const float mr3 = mr * rinv * rinv;
-        x.pax += dx * mr3;
-        x.pay += dy * mr3;
-        x.paz += dz * mr3;
-        x.ppf -= mr;
-      }
-      x.pax += bx;
-      x.pay += by;
-      x.paz += bz;
-      x.ppf += bp;
-    } else if (!kFar && x.grp < x.G) {
-      for (int jj = x.grp; jj < cnt; jj += x.G) {
-        const float4 s = w.src[jj];
-        const float dx = s.x - x.tx, dy = s.y - x.ty, dz = s.z - x.tz;
-        const float r2 = dx * dx + dy * dy + dz * dz;
-        if (r2 > w.sreach2[jj]) {  // r > soft_i + soft_j: Newtonian, and r > 0
-          const float rinv = rsqrtf(r2);
-          const float mr = s.w * rinv;
-          const float mr3 = mr * rinv * rinv;
-          x.pax += dx * mr3;
-          x.pay += dy * mr3;
-          x.paz += dz * mr3;
-          x.ppf -= mr;
-        } else if (r2 > 0.f) {
-          const float rinv = rsqrtf(r2);
-          float a, b;
-          spline_f32(r2, rinv, w.ssoft[jj] + x.ts, a, b);
-          const float bm = b * s.w;
-          x.pax += dx * bm;
-          x.pay += dy * bm;
-          x.paz += dz * bm;
-          x.ppf -= s.w * a;
+    if (cs + 64 < total) fetch(cs + 64);
+    const int np = (min(64, total - cs) + 1) >> 1;
+    if (x.grp < x.G) {
+      for (int k = x.grp; k < np; k += x.G) {
+        const float4 X = w.px[k], Z = w.pz[k];
+        const float2 dx = __fadd2_rn(make_float2(X.x, X.y), ntx);
+        const float2 dy = __fadd2_rn(make_float2(X.z, X.w), nty);
+        const float2 dz = __fadd2_rn(make_float2(Z.x, Z.y), ntz);
+        float2 r2 = __fmul2_rn(dx, dx);
+        r2 = __ffma2_rn(dy, dy, r2);
+        r2 = __ffma2_rn(dz, dz, r2);
+        bool fast = true;
+        float4 R;
+        if (!kFar) {
+          R = w.pr[k];
+          fast = (r2.x > R.x) && (r2.y > R.y);
+        }
+        if (fast) {
+          const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+          const float2 mr = __fmul2_rn(make_float2(Z.z, Z.w), ri);
+          const float2 mr3 = __fmul2_rn(mr, __fmul2_rn(ri, ri));
+          ax2 = __ffma2_rn(dx, mr3, ax2);
+          ay2 = __ffma2_rn(dy, mr3, ay2);
+          az2 = __ffma2_rn(dz, mr3, az2);
+          pp2 = __fadd2_rn(pp2, mr);
+        } else {
+          near_pair(Z.z, dx.x, dy.x, dz.x, r2.x, R.x, R.z, x.ts, ax2.x, ay2.x, az2.x, pp2.x);
+          near_pair(Z.w, dx.y, dy.y, dz.y, r2.y, R.y, R.w, x.ts, ax2.y, ay2.y, az2.y, pp2.y);
         }
       }
     }
     __syncwarp();
   }
+  total_out = total;
+  return make_float4(ax2.x + ax2.y, ay2.x + ay2.y, az2.x + az2.y, -(pp2.x + pp2.y));
+}
+template <bool kFar>
+__device__ __forceinline__ void flush_p2p(MixWarp& w, const float4* __restrict__ buf, int nleaves,
+                                          const WalkRec* __restrict__ walk, const float4* __restrict__ srcf,
+                                          const float* __restrict__ softf, MixCtx& x) {
+  int total = 0;
+  const float4 v = flush_p2p_nl<kFar>(w, buf, nleaves, walk, srcf, softf,
+                                      FlushIn{x.tx, x.ty, x.tz, x.ts, x.lane, x.grp, x.G}, total);
+  x.pax += v.x; x.pay += v.y; x.paz += v.z; x.ppf += v.w;
   x.n_src += (unsigned)total;
   x.commit();
 }
@@ -302,41 +328,123 @@ __device__ __forceinline__ void p2c_term(const float4 A, const float4 B, const f
   az += -qir3 * rz + c * qz;
 }
 
-// Evaluate all buffered P2C nodes.
-__device__ __forceinline__ void flush_p2c(MixWarp& w, int nent, const QuadRecF* __restrict__ quadf, MixCtx& x) {
+// Both terms of a staged node pair in scalar form (the rare softened case);
+// out of line so that it adds no registers to the packed loop.
+__device__ __noinline__ float4 p2c_pair_scalar(const MixWarp& w, int k, float tx, float ty, float tz, float ts) {
+  const float4 P0 = w.qp[0][k], P1 = w.qp[1][k], P2 = w.qp[2][k], P3 = w.qp[3][k], P4 = w.qp[4][k],
+               P5 = w.qp[5][k];
+  float ax = 0.f, ay = 0.f, az = 0.f, pf = 0.f;
+  p2c_term(make_float4(P0.x, P0.z, P1.x, P1.z), make_float4(P2.x, P2.z, P3.x, P3.z),
+           make_float4(P4.x, P4.z, P5.x, P5.z), tx, ty, tz, ts, ax, ay, az, pf);
+  p2c_term(make_float4(P0.y, P0.w, P1.y, P1.w), make_float4(P2.y, P2.w, P3.y, P3.w),
+           make_float4(P4.y, P4.w, P5.y, P5.w), tx, ty, tz, ts, ax, ay, az, pf);
+  return make_float4(ax, ay, az, pf);
+}
+
+// Evaluate all buffered P2C nodes.  Nodes are staged 64 per chunk as 32
+// interleaved pairs (six float4: offsets, masses, the six second moments,
+// softening and half trace, each as (node a, node b)) and a lane evaluates
+// two nodes against its target with the packed FP32 instructions.  The
+// offsets are o = cm_node - cm_bucket and the expression is written for
+// r' = o - t = -r (q' = -q, so the acceleration reads qir3 r' - c q').
+// A pair with a softened term falls back to the scalar p2c_term for both.
+// Missing nodes of the last pair have zero mass and moments at a far offset.
+__device__ __noinline__ float4 flush_p2c_nl(MixWarp& w, int nent, const QuadRecF* __restrict__ quadf, const FlushIn x) {
   const float qnan = __int_as_float(0x7fc00000);
-  float4 ne = make_float4(0.f, 0.f, 0.f, 0.f), nq0 = ne, nq1 = ne;  // next chunk's entry and record
-  auto fetch = [&](int cs) {
-    const int q = cs + x.lane;
+  const float kPad = 1.0e10f;
+  float4 a0, a1, b0, b1;  // next chunk: records of this lane's two nodes
+  auto load_node = [&](int q, float4& r0, float4& r1) {
+    r0 = make_float4(0.f, 0.f, 0.f, 0.f);
+    r1 = r0;
     if (q < nent) {
-      ne = w.cbuf[q];
-      const float4* rec = reinterpret_cast<const float4*>(quadf + entry_node(ne));
-      nq0 = rec[0];  // mass, soft, xx, xy
-      nq1 = rec[1];  // xz, yy, yz, zz
+      const float4* rec = reinterpret_cast<const float4*>(quadf + entry_node(w.cbuf[q]));
+      r0 = rec[0];  // mass, soft, xx, xy
+      r1 = rec[1];  // xz, yy, yz, zz
     }
   };
+  auto fetch = [&](int cs) {
+    load_node(cs + 2 * x.lane, a0, a1);
+    load_node(cs + 2 * x.lane + 1, b0, b1);
+  };
   fetch(0);
-  for (int cs = 0; cs < nent; cs += 32) {
-    if (cs + x.lane < nent) {
-      w.qa[x.lane] = make_float4(ne.x, ne.y, ne.z, nq0.x);
-      if (entry_flag(ne)) {
-        w.qb[x.lane] = make_float4(0.f, 0.f, 0.f, 0.f);
-        w.qc[x.lane] = make_float4(0.f, 0.f, qnan, 0.f);
-      } else {
-        w.qb[x.lane] = make_float4(nq0.z, nq0.w, nq1.x, nq1.y);
-        w.qc[x.lane] = make_float4(nq1.z, nq1.w, nq0.y, 0.5f * (nq0.z + nq1.y + nq1.w));
+  const float2 ntx = make_float2(-x.tx, -x.tx), nty = make_float2(-x.ty, -x.ty), ntz = make_float2(-x.tz, -x.tz);
+  const float2 three = make_float2(3.f, 3.f), five = make_float2(5.f, 5.f), half = make_float2(0.5f, 0.5f);
+  float2 ax2 = make_float2(0.f, 0.f), ay2 = ax2, az2 = ax2, pf2 = ax2;
+  for (int cs = 0; cs < nent; cs += 64) {
+    // (ox, oy) (oz, M) (xx, xy) (xz, yy) (yz, zz) (soft, tr/2), each for nodes a and b
+    {
+      const int qa = cs + 2 * x.lane, qb = qa + 1;
+      const float4 pad = make_float4(kPad, kPad, kPad, 0.f);
+      const float4 ea = qa < nent ? w.cbuf[qa] : pad, eb = qb < nent ? w.cbuf[qb] : pad;
+      if (qa < nent && entry_flag(ea)) {  // monopole: no second moments, NaN softening
+        a0 = make_float4(a0.x, qnan, 0.f, 0.f);
+        a1 = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+      if (qb < nent && entry_flag(eb)) {
+        b0 = make_float4(b0.x, qnan, 0.f, 0.f);
+        b1 = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    w.qp[0][x.lane] = make_float4(ea.x, eb.x, ea.y, eb.y);
+    w.qp[1][x.lane] = make_float4(ea.z, eb.z, a0.x, b0.x);
+    w.qp[2][x.lane] = make_float4(a0.z, b0.z, a0.w, b0.w);
+    w.qp[3][x.lane] = make_float4(a1.x, b1.x, a1.y, b1.y);
+    w.qp[4][x.lane] = make_float4(a1.z, b1.z, a1.w, b1.w);
+    w.qp[5][x.lane] = make_float4(a0.y, b0.y, 0.5f * (a0.z + a1.y + a1.w), 0.5f * (b0.z + b1.y + b1.w));
+    }
+    __syncwarp();
+    if (cs + 64 < nent) fetch(cs + 64);
+    const int np = (min(64, nent - cs) + 1) >> 1;
+    if (x.grp < x.G) {
+      for (int k = x.grp; k < np; k += x.G) {
+        const float4 P0 = w.qp[0][k], P1 = w.qp[1][k];
+        const float2 rx = __fadd2_rn(make_float2(P0.x, P0.y), ntx);  // r' = o - t
+        const float2 ry = __fadd2_rn(make_float2(P0.z, P0.w), nty);
+        const float2 rz = __fadd2_rn(make_float2(P1.x, P1.y), ntz);
+        float2 r2 = __fmul2_rn(rx, rx);
+        r2 = __ffma2_rn(ry, ry, r2);
+        r2 = __ffma2_rn(rz, rz, r2);
+        const float4 P5 = w.qp[5][k];
+        const float twa = P5.x + x.ts, twb = P5.y + x.ts;
+        const float4 P2 = w.qp[2][k], P3 = w.qp[3][k], P4 = w.qp[4][k];
+        if (r2.x < twa * twa || r2.y < twb * twb) {  // softened: both terms in scalar form
+          const float4 v = p2c_pair_scalar(w, k, x.tx, x.ty, x.tz, x.ts);
+          ax2.x += v.x;
+          ay2.x += v.y;
+          az2.x += v.z;
+          pf2.x += v.w;
+          continue;
+        }
+        const float2 a = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+        const float2 d2 = __fmul2_rn(a, a);
+        const float2 b = __fmul2_rn(a, d2);
+        const float2 c = __fmul2_rn(__fmul2_rn(b, d2), three);
+        const float2 d = __fmul2_rn(__fmul2_rn(c, d2), five);
+        const float2 xx = make_float2(P2.x, P2.y), xy = make_float2(P2.z, P2.w);
+        const float2 xz = make_float2(P3.x, P3.y), yy = make_float2(P3.z, P3.w);
+        const float2 yz = make_float2(P4.x, P4.y), zz = make_float2(P4.z, P4.w);
+        const float2 qx = __ffma2_rn(xz, rz, __ffma2_rn(xy, ry, __fmul2_rn(xx, rx)));
+        const float2 qy = __ffma2_rn(yz, rz, __ffma2_rn(yy, ry, __fmul2_rn(xy, rx)));
+        const float2 qz = __ffma2_rn(zz, rz, __ffma2_rn(yz, ry, __fmul2_rn(xz, rx)));
+        const float2 qir = __fmul2_rn(half, __ffma2_rn(qz, rz, __ffma2_rn(qy, ry, __fmul2_rn(qx, rx))));
+        const float2 M = make_float2(P1.z, P1.w), tr = make_float2(P5.z, P5.w);
+        const float2 ctr = __fmul2_rn(c, tr);
+        // qir3 = b M + d qir - c tr ; pot += b tr - M a - c qir
+        const float2 qir3 = __fadd2_rn(__ffma2_rn(d, qir, __fmul2_rn(b, M)), make_float2(-ctr.x, -ctr.y));
+        const float2 pt = __ffma2_rn(b, tr, make_float2(-(M.x * a.x), -(M.y * a.y)));
+        pf2 = __fadd2_rn(pf2, __ffma2_rn(make_float2(-c.x, -c.y), qir, pt));
+        const float2 nc = make_float2(-c.x, -c.y);
+        ax2 = __ffma2_rn(nc, qx, __ffma2_rn(qir3, rx, ax2));
+        ay2 = __ffma2_rn(nc, qy, __ffma2_rn(qir3, ry, ay2));
+        az2 = __ffma2_rn(nc, qz, __ffma2_rn(qir3, rz, az2));
       }
     }
     __syncwarp();
-    if (cs + 32 < nent) fetch(cs + 32);
-    const int cnt = min(32, nent - cs);
-    if (x.grp < x.G) {
-      // one P2C term has enough independent work; a 2-way unroll measured slower
-      for (int ee = x.grp; ee < cnt; ee += x.G)
-        p2c_term(w.qa[ee], w.qb[ee], w.qc[ee], x.tx, x.ty, x.tz, x.ts, x.pax, x.pay, x.paz, x.ppf);
-    }
-    __syncwarp();
   }
+  return make_float4(ax2.x + ax2.y, ay2.x + ay2.y, az2.x + az2.y, pf2.x + pf2.y);
+}
+__device__ __forceinline__ void flush_p2c(MixWarp& w, int nent, const QuadRecF* __restrict__ quadf, MixCtx& x) {
+  const float4 v = flush_p2c_nl(w, nent, quadf, FlushIn{x.tx, x.ty, x.tz, x.ts, x.lane, x.grp, x.G});
+  x.pax += v.x; x.pay += v.y; x.paz += v.z; x.ppf += v.w;
   x.n_node += (unsigned)nent;
   x.commit();
 }
@@ -372,7 +480,6 @@ __global__ void __launch_bounds__(kMixWarps * 32, kMinBlocks) traverse_mixed(Tra
     const int tbase = P.walk[tnode].pstart, ntot = P.walk[tnode].pcount;
     // more than 32 particles only in a depth-21 leaf of identical keys: its
     // targets are walked in chunks of 32 (decisions depend on the bucket only)
-    const unsigned long long work0 = c_pp + c_pc;
     for (int tc = 0; tc < ntot; tc += 32) {
       const int t0 = tbase + tc, nt = min(32, ntot - tc);
       unsigned long long opens = 0;
@@ -473,7 +580,7 @@ __global__ void __launch_bounds__(kMixWarps * 32, kMinBlocks) traverse_mixed(Tra
       }
 
       // sum the G lane groups of each target (staging area reused as FP64 scratch)
-      double* red = reinterpret_cast<double*>(w.qa);
+      double* red = reinterpret_cast<double*>(&w.qp[0][0]);
       __syncwarp();
 #pragma unroll
       for (int k = 0; k < 4; k++) red[4 * lane + k] = (double)w.kahan[2 * k][lane] - (double)w.kahan[2 * k + 1][lane];
@@ -500,10 +607,11 @@ __global__ void __launch_bounds__(kMixWarps * 32, kMinBlocks) traverse_mixed(Tra
       c_pp += (unsigned long long)x.n_src * (unsigned long long)nt;
       c_pc += (unsigned long long)x.n_node * (unsigned long long)nt;
       if (tc == 0) c_open += opens;
-    }
-    if (P.bucket_work && lane == 0) {
-      const unsigned long long wk = c_pp + c_pc - work0;
-      P.bucket_work[b] = P.accumulate ? P.bucket_work[b] + wk : wk;
+      if (P.bucket_work && lane == 0) {  // this chunk's interactions, added to the bucket's
+        unsigned long long wk = (unsigned long long)(x.n_src + x.n_node) * (unsigned long long)nt;
+        if (tc > 0 || P.accumulate) wk += P.bucket_work[b];
+        P.bucket_work[b] = wk;
+      }
     }
   }
   if (lane == 0) {
@@ -539,8 +647,9 @@ void launch_prep_sources(const int32_t* buckets, int64_t nbuckets, const WalkRec
 
 // variant: 0 = at most 6 CTAs/SM (80 registers), 1 = 5 CTAs/SM (no spills)
 void launch_traverse_mixed(const TravParams& P, const Mom* mom, int grid, int variant, cudaStream_t st) {
-  if (variant == 1) { note_launch(); traverse_mixed<5><<<grid, kMixWarps * 32, 0, st>>>(P, mom); }
-  else { note_launch(); traverse_mixed<6><<<grid, kMixWarps * 32, 0, st>>>(P, mom); }
+  // 5 CTAs per SM (96 registers) by default; PT_MIXED_VARIANT=1 selects 6 CTAs (80 registers)
+  if (variant == 1) { note_launch(); traverse_mixed<6><<<grid, kMixWarps * 32, 0, st>>>(P, mom); }
+  else { note_launch(); traverse_mixed<5><<<grid, kMixWarps * 32, 0, st>>>(P, mom); }
 }
 
 }  // namespace pt
