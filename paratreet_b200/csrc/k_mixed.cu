@@ -36,6 +36,7 @@
 //  reduce   per-lane Kahan sums -> FP64, sum over the G groups.
 #include "pt_internal.cuh"
 #include "pt_walk.cuh"
+#include "pt_f32.cuh"
 
 namespace pt {
 
@@ -70,63 +71,6 @@ struct MixWarp {
                             // reach2 = (soft_j + max bucket softening)^2 a pair is unsoftened
   float4 qp[6][32];         // staged P2C node pairs (see flush_p2c)
 };
-
-// SPLINE in FP32, softened branch (r < twoh): kept out of line so that the
-// rarely taken polynomial does not raise register pressure in the hot loops.
-__device__ __noinline__ void spline_f32_soft(float r2, float rinv, float twoh, float& a, float& b) {
-  float r = r2 * rinv;
-  float dih = 2.0f / twoh;
-  float u = r * dih;
-  float u2 = u * u;
-  if (u < 1.0f) {
-    a = dih * (7.0f / 5.0f - 2.0f / 3.0f * u2 + 3.0f / 10.0f * u2 * u2 - 1.0f / 10.0f * u2 * u2 * u);
-    b = dih * dih * dih * (4.0f / 3.0f - 6.0f / 5.0f * u2 + 1.0f / 2.0f * u2 * u);
-  } else {
-    a = -1.0f / 15.0f * rinv +
-        dih * (8.0f / 5.0f - 4.0f / 3.0f * u2 + u2 * u - 3.0f / 10.0f * u2 * u2 + 1.0f / 30.0f * u2 * u2 * u);
-    b = -1.0f / 15.0f * rinv * rinv * rinv +
-        dih * dih * dih * (8.0f / 3.0f - 3.0f * u + 6.0f / 5.0f * u2 - 1.0f / 6.0f * u2 * u);
-  }
-}
-
-// SPLINE in FP32 (r2 > 0): force term b, potential term a.
-__device__ __forceinline__ void spline_f32(float r2, float rinv, float twoh, float& a, float& b) {
-  if (r2 < twoh * twoh) {
-    spline_f32_soft(r2, rinv, twoh, a, b);
-  } else {
-    a = rinv;
-    b = rinv * rinv * rinv;
-  }
-}
-
-// SPLINEQ in FP32 with the reference's grouping (examples/GravityVisitor.h:37-80);
-// only the softened branch is called (out of line, rarely taken).
-__device__ __noinline__ void splineq_f32(float dir, float r2, float twoh, float& a, float& b, float& c, float& d) {
-  if (r2 < twoh * twoh) {
-    float dih = 2.0f / twoh;
-    float u = dih / dir;
-    float u2 = u * u;
-    float d2 = dih * dih, d3 = d2 * dih, d4 = d3 * dih, d5 = d4 * dih, d6 = d5 * dih;
-    if (u < 1.0f) {
-      a = dih * 7.0f / 5.0f - 2.0f / 3.0f * u2 + 3.0f / 10.0f * u2 * u2 - 1.0f / 10.0f * u2 * u2 * u;
-      b = d3 * 4.0f / 3.0f - 6.0f / 5.0f * u2 + 1.0f / 2.0f * u2 * u;
-      c = d5 * 12.0f / 5.0f - 3.0f / 2.0f * u;
-      d = 3.0f / 2.0f * d6 * dir;
-    } else {
-      float r3 = dir * dir * dir;
-      a = -1.0f / 15.0f * dir + dih * (8.0f / 5.0f) - 4.0f / 3.0f * u2 + u2 * u - 3.0f / 10.0f * u2 * u2 +
-          1.0f / 30.0f * u2 * u2 * u;
-      b = -1.0f / 15.0f * r3 + d3 * 8.0f / 3.0f - 3.0f * u + 6.0f / 5.0f * u2 - 1.0f / 6.0f * u2 * u;
-      c = -1.0f / 5.0f * r3 * dir * dir + 3.0f * d4 * dir + d5 * (-12.0f) / 5.0f + 1.0f / 2.0f * u;
-      d = -r3 * r3 * dir + 3.0f * d4 * r3 - 1.0f / 2.0f * d6 * dir;
-    }
-  } else {
-    a = dir;
-    b = a * a * a;
-    c = 3.0f * b * a * a;
-    d = 5.0f * c * a * a;
-  }
-}
 
 __device__ __forceinline__ float4 pack_entry(float ox, float oy, float oz, int node, bool flag) {
   return make_float4(ox, oy, oz, __int_as_float(node | (flag ? (int)0x80000000 : 0)));

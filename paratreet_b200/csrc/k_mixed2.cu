@@ -1,0 +1,656 @@
+// k_mixed2.cu -- K7 mixed-precision traversal in two phases.
+//
+// Phase A (walk_lists): one warp per bucket walks the tree exactly as the
+// fused traversal does (FP64 opening and softening tests, GravityVisitor::
+// open / openSoftening, so the same leaf() and node() interactions) and
+// writes the bucket's interaction list to HBM: P2C node indices (bit 31 =
+// monopole, addGravity; bit 30 = near: a target may lie inside the node's
+// softening sphere) and P2P leaf indices (bit 31 = near: some pair may be
+// softened).  Each warp appends to regions it reserves from two global pools
+// at bucket boundaries, so every bucket's list is contiguous; a bucket that
+// outgrows what is left of its region sets kErrPool and the host repeats the
+// walk with larger regions.
+//
+// Phase B (eval_p2c, eval_p2p): one warp per bucket streams its list in
+// chunks of 64 entries and evaluates them with the packed FP32 instructions
+// (two interactions per issue slot) on offsets relative to the bucket's
+// centre of mass, as the fused kernel does, but without the walk's state in
+// registers, so more warps fit on an SM.  eval_p2c stores (or, for replica
+// walks after the first, adds) and eval_p2p adds.
+#include "pt_internal.cuh"
+#include "pt_walk.cuh"
+#include "pt_f32.cuh"
+
+namespace pt {
+
+constexpr int kWlWarps = 4;
+constexpr int kWlStack = 640;  // opened nodes pending (as the fused walk)
+constexpr int kWlBuf = 64;
+
+struct WalkWarp {
+  BucketGeom geom;
+  int32_t stack[kWlStack];
+  int32_t pcbuf[kWlBuf];  // P2C entries waiting to be written
+  int32_t ppbuf[kWlBuf];  // P2P entries waiting to be written
+};
+
+// Per-warp region of one pool: [cur, end).
+struct Region {
+  unsigned long long cur, end;
+};
+
+// Reserve a new region when less than `thresh` entries are left (lane 0 calls
+// the atomic; the result is broadcast).  Returns false if the pool is full.
+__device__ __forceinline__ bool ensure_region(Region& r, unsigned long long* cursor, unsigned long long cap,
+                                              unsigned region, unsigned thresh, int lane) {
+  if (r.end - r.cur >= thresh) return true;
+  unsigned long long s = 0;
+  if (lane == 0) s = atomicAdd(cursor, (unsigned long long)region);
+  s = __shfl_sync(kFull, s, 0);
+  if (s + region > cap) {
+    r.cur = r.end = cap;
+    return false;
+  }
+  r.cur = s;
+  r.end = s + region;
+  return true;
+}
+
+// Write n buffered entries at the region cursor (false if they do not fit).
+__device__ __forceinline__ bool drain(const int32_t* buf, int n, Region& r, int32_t* __restrict__ pool, int lane) {
+  if (n == 0) return true;
+  if (r.cur + (unsigned long long)n > r.end) return false;
+  for (int k = lane; k < n; k += 32) pool[r.cur + k] = buf[k];
+  r.cur += (unsigned long long)n;
+  return true;
+}
+
+__global__ void __launch_bounds__(kWlWarps * 32, 8) walk_lists(TravParams P, ListParams L, const Mom* __restrict__ mom) {
+  __shared__ WalkWarp warps[kWlWarps];
+  WalkWarp& w = warps[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  unsigned long long c_pp = 0, c_pc = 0, c_open = 0;
+  unsigned max_len = 0;
+  Region rpc{0, 0}, rpp{0, 0};
+  bool pool_ok = true;
+  while (true) {
+    unsigned bi = 0;
+    if (lane == 0) bi = atomicAdd(P.work, 1u);
+    bi = __shfl_sync(kFull, bi, 0);
+    const int64_t b = P.b_begin + (int64_t)bi;
+    if (b >= P.b_end) break;
+    const int64_t lb = b - P.b_begin;
+    const int tnode = P.buckets[b];
+    if (tnode < 0 || tnode >= P.nnodes) {
+      if (lane == 0) atomicOr(P.status, kErrCapacity);
+      continue;
+    }
+    pool_ok = pool_ok && ensure_region(rpc, L.cursor + 0, L.cap_pc, L.region, L.thresh, lane) &&
+              ensure_region(rpp, L.cursor + 1, L.cap_pp, L.region, L.thresh, lane);
+    if (!pool_ok) {
+      if (lane == 0) {
+        atomicOr(P.status, kErrPool);
+        L.pc_count[lb] = 0;
+        L.pp_count[lb] = 0;
+      }
+      continue;
+    }
+    __syncwarp();
+    if (lane == 0) load_bucket_geom(mom, tnode, w.geom);
+    __syncwarp();
+    const BucketGeom& g = w.geom;
+    const int ntot = P.walk[tnode].pcount;
+    const unsigned long long pc0 = rpc.cur, pp0 = rpp.cur;
+    unsigned long long opens = 0, nsrc = 0;
+    int sp = 0, nc = 0, np = 0;
+    int nexp = 1, pop = -1;
+    bool ok = true, fits = true;
+    while (true) {
+      const int e = lane >> 3, c = lane & 7;
+      int node = -1;
+      if (pop < 0) {
+        if (lane == 0) node = 0;
+      } else if (e < nexp) {
+        node = w.stack[pop + e] + c;
+      }
+      int cls = kClsNone;
+      WalkRec r;
+      if (node >= 0) {
+        if (node >= P.nnodes) {
+          atomicOr(P.status, kErrCapacity);
+        } else {
+          r = P.walk[node];
+          cls = classify_node(r, g, P.ox, P.oy, P.oz);
+        }
+      }
+      opens += (unsigned long long)__popc(__ballot_sync(kFull, node >= 0 && node < P.nnodes &&
+                                                                    r.type == kTypeInternal));
+      bool near = false;
+      if (cls == kClsP2P || cls == kClsQuad) {
+        // P2P: a pair may be softened; P2C: a target may be inside twoh of
+        // the centre (SPLINEQ's softened branch), with a relative margin
+        const double cx = r.cm[0] + P.ox, cy = r.cm[1] + P.oy, cz = r.cm[2] + P.oz;
+        const double reach = (cls == kClsP2P) ? r.reach + r.soft_max + g.soft_max
+                                              : (r.soft + g.soft_max) * (1.0 + 1e-5);
+        near = !(box_dist2(g.lo, g.hi, cx, cy, cz) > reach * reach);
+      }
+      {
+        const bool pc = (cls == kClsQuad || cls == kClsMono);
+        const unsigned m = __ballot_sync(kFull, pc);
+        if (pc)
+          w.pcbuf[nc + __popc(m & ((1u << lane) - 1u))] =
+              node | (cls == kClsMono ? (int)0x80000000 : 0) | (near ? 0x40000000 : 0);
+        nc += __popc(m);
+      }
+      {
+        const bool pp = (cls == kClsP2P);
+        const unsigned m = __ballot_sync(kFull, pp);
+        if (pp) w.ppbuf[np + __popc(m & ((1u << lane) - 1u))] = node | (near ? (int)0x80000000 : 0);
+        np += __popc(m);
+        nsrc += (unsigned long long)__reduce_add_sync(kFull, pp ? (unsigned)r.pcount : 0u);
+      }
+      {
+        const bool op = (cls == kClsOpen);
+        const unsigned m = __ballot_sync(kFull, op);
+        if (sp + __popc(m) > kWlStack) {
+          ok = false;
+          break;
+        }
+        if (op) w.stack[sp + __popc(m & ((1u << lane) - 1u))] = r.first_child;
+        sp += __popc(m);
+      }
+      __syncwarp();
+      const bool last = (sp == 0);
+      if (nc >= 32 || last) {
+        fits = drain(w.pcbuf, nc, rpc, L.pc_pool, lane) && fits;
+        nc = 0;
+      }
+      if (np >= 32 || last) {
+        fits = drain(w.ppbuf, np, rpp, L.pp_pool, lane) && fits;
+        np = 0;
+      }
+      __syncwarp();
+      if (last) break;
+      nexp = sp < 4 ? sp : 4;
+      sp -= nexp;
+      pop = sp;
+    }
+    if (!ok && lane == 0) atomicOr(P.status, kErrStack);
+    if (!fits && lane == 0) atomicOr(P.status, kErrPool);
+    const unsigned npc = (unsigned)(rpc.cur - pc0), npp = (unsigned)(rpp.cur - pp0);
+    if (lane == 0) {
+      const bool good = ok && fits;
+      L.pc_start[lb] = (int64_t)pc0;
+      L.pc_count[lb] = good ? (int32_t)npc : 0;
+      L.pp_start[lb] = (int64_t)pp0;
+      L.pp_count[lb] = good ? (int32_t)npp : 0;
+    }
+    max_len = max(max_len, max(npc, npp));
+    c_pc += (unsigned long long)npc * (unsigned long long)ntot;
+    c_pp += nsrc * (unsigned long long)ntot;
+    c_open += opens;
+    if (P.bucket_work && lane == 0) {
+      unsigned long long wk = ((unsigned long long)npc + nsrc) * (unsigned long long)ntot;
+      if (P.accumulate) wk += P.bucket_work[b];
+      P.bucket_work[b] = wk;
+    }
+  }
+  if (lane == 0) {
+    atomicAdd(&P.counters[0], c_pp);
+    atomicAdd(&P.counters[1], c_pc);
+    atomicAdd(&P.counters[2], c_open);
+    atomicMax(L.max_len, max_len);
+  }
+}
+
+// ---------------------------------------------------------------- phase B
+constexpr int kEvWarps = 4;
+
+struct EvalWarp {
+  BucketGeom geom;
+  float4 st[6][32];            // staged pairs: P2C six rows; P2P px, pz, pr
+  int32_t pre[kWlBuf + 1];     // P2P: prefix of leaf sizes in a leaf block
+  int32_t ps0[kWlBuf];         // P2P: first particle of each leaf
+  float4 lof[kWlBuf];          // P2P: leaf offsets cm_leaf - cm_bucket (FP32)
+  int32_t lsel[kWlBuf];        // P2P: leaves of the current kind in a block
+};
+
+// Per-lane target of a 32-target chunk, replicated over G lane groups.
+struct EvTarget {
+  int t, grp, G, nt;
+  float tx, ty, tz, ts;
+};
+
+__device__ __forceinline__ EvTarget ev_target(const Particles& p, const BucketGeom& g, int t0, int nt, int lane) {
+  EvTarget x;
+  x.nt = nt;
+  x.t = lane % nt;
+  x.grp = lane / nt;
+  x.G = 32 / nt;
+  x.tx = x.ty = x.tz = x.ts = 0.f;
+  if (x.grp < x.G) {
+    const int i = t0 + x.t;
+    x.tx = (float)(p.x[i] - g.cm[0]);
+    x.ty = (float)(p.y[i] - g.cm[1]);
+    x.tz = (float)(p.z[i] - g.cm[2]);
+    x.ts = (float)p.soft[i];
+  }
+  return x;
+}
+
+struct Kahan4 {
+  float s[4], c[4];
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int k = 0; k < 4; k++) s[k] = c[k] = 0.f;
+  }
+  __device__ __forceinline__ void add(int k, float v) {
+    const float y = v - c[k];
+    const float t = s[k] + y;
+    c[k] = (t - s[k]) - y;
+    s[k] = t;
+  }
+};
+
+// Sum the G lane groups of each target and store or add the result.
+__device__ __forceinline__ void ev_finish(EvalWarp& w, const Kahan4& K, const EvTarget& x, const TravParams& P,
+                                          int t0, int lane, bool store) {
+  double* red = reinterpret_cast<double*>(&w.st[0][0]);
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < 4; k++) red[4 * lane + k] = (double)K.s[k] - (double)K.c[k];
+  __syncwarp();
+  if (lane < x.nt) {
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int gg = 0; gg < x.G; gg++)
+      for (int k = 0; k < 4; k++) v[k] += red[4 * (gg * x.nt + lane) + k];
+    const int i = t0 + lane;
+    if (store) {
+      P.p.ax[i] = v[0];
+      P.p.ay[i] = v[1];
+      P.p.az[i] = v[2];
+      P.p.pot[i] = 0.0;
+      P.p.potf[i] = v[3];
+    } else {
+      P.p.ax[i] += v[0];
+      P.p.ay[i] += v[1];
+      P.p.az[i] += v[2];
+      P.p.potf[i] += v[3];
+    }
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ bool next_bucket(const TravParams& P, int lane, int64_t& b, int& tnode) {
+  unsigned bi = 0;
+  if (lane == 0) bi = atomicAdd(P.work, 1u);
+  bi = __shfl_sync(kFull, bi, 0);
+  b = P.b_begin + (int64_t)bi;
+  if (b >= P.b_end) return false;
+  tnode = P.buckets[b];
+  return true;
+}
+
+// FP32 offset of a node's centre of mass (plus the replica offset) from the
+// bucket's, computed in FP64 as the walk computes it.
+__device__ __forceinline__ float4 node_offset(const WalkRec* __restrict__ walk, int node, const TravParams& P,
+                                              const BucketGeom& g) {
+  const double2* r = reinterpret_cast<const double2*>(walk + node);
+  const double2 c01 = r[0];
+  const double c2 = r[1].x;
+  return make_float4((float)((c01.x + P.ox) - g.cm[0]), (float)((c01.y + P.oy) - g.cm[1]),
+                     (float)((c2 + P.oz) - g.cm[2]), 0.f);
+}
+
+// Both terms of a staged node pair in scalar form (the rare softened case).
+__device__ __noinline__ float4 ev_p2c_pair_scalar(const EvalWarp& w, int k, float tx, float ty, float tz, float ts) {
+  const float4 P0 = w.st[0][k], P1 = w.st[1][k], P2 = w.st[2][k], P3 = w.st[3][k], P4 = w.st[4][k],
+               P5 = w.st[5][k];
+  float ax = 0.f, ay = 0.f, az = 0.f, pf = 0.f;
+  // rows: (ox, oy, oz, M), (xx, xy, xz, yy), (yz, zz, soft, half trace)
+  const float4 t[2][3] = {{make_float4(P0.x, P0.z, P1.x, P1.z), make_float4(P2.x, P2.z, P3.x, P3.z),
+                           make_float4(P4.x, P4.z, P5.z, fabsf(P5.x))},
+                          {make_float4(P0.y, P0.w, P1.y, P1.w), make_float4(P2.y, P2.w, P3.y, P3.w),
+                           make_float4(P4.y, P4.w, P5.w, fabsf(P5.y))}};
+  for (int s = 0; s < 2; s++) {
+    // r = t - o (GravityVisitor::node, examples/GravityVisitor.h:207-220, FP32)
+    const float4 A = t[s][0], B = t[s][1], Cc = t[s][2];
+    const float rx = tx - A.x, ry = ty - A.y, rz = tz - A.z;
+    const float r2 = rx * rx + ry * ry + rz * rz;
+    const float dir = rsqrtf(r2);
+    float a, b, c, d;
+    splineq_f32(dir, r2, Cc.z + ts, a, b, c, d);
+    const float qx = B.x * rx + B.y * ry + B.z * rz;
+    const float qy = B.y * rx + B.w * ry + Cc.x * rz;
+    const float qz = B.z * rx + Cc.x * ry + Cc.y * rz;
+    const float qir = 0.5f * (qx * rx + qy * ry + qz * rz);
+    const float qir3 = b * A.w + d * qir - c * Cc.w;
+    pf += -A.w * a - c * qir + b * Cc.w;
+    ax += -qir3 * rx + c * qx;
+    ay += -qir3 * ry + c * qy;
+    az += -qir3 * rz + c * qz;
+  }
+  return make_float4(ax, ay, az, pf);
+}
+
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams P, ListParams L,
+                                                                     const Mom* __restrict__ mom) {
+  __shared__ EvalWarp warps[kEvWarps];
+  EvalWarp& w = warps[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const float qnan = __int_as_float(0x7fc00000);
+  const float kPad = 1.0e10f;
+  const float2 mthree = make_float2(-3.f, -3.f), mfive = make_float2(-5.f, -5.f), half = make_float2(0.5f, 0.5f);
+  int64_t b;
+  int tnode;
+  while (next_bucket(P, lane, b, tnode)) {
+    if (tnode < 0 || tnode >= P.nnodes) continue;
+    const int64_t lb = b - P.b_begin;
+    const int64_t start = L.pc_start[lb];
+    const int count = L.pc_count[lb];
+    __syncwarp();
+    if (lane == 0) load_bucket_geom(mom, tnode, w.geom);
+    __syncwarp();
+    const int tbase = P.walk[tnode].pstart, ntot = P.walk[tnode].pcount;
+    for (int tc = 0; tc < ntot; tc += 32) {
+      const int t0 = tbase + tc, nt = min(32, ntot - tc);
+      const EvTarget x = ev_target(P.p, w.geom, t0, nt, lane);
+      const float2 ntx = make_float2(-x.tx, -x.tx), nty = make_float2(-x.ty, -x.ty), ntz = make_float2(-x.tz, -x.tz);
+      Kahan4 K;
+      K.zero();
+      for (int cs = 0; cs < count; cs += 64) {
+        // stage this lane's two nodes as a pair
+        float4 o[2], r0[2], r1[2];
+        bool near[2] = {false, false};
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int q = cs + 2 * lane + h;
+          o[h] = make_float4(kPad, kPad, kPad, 0.f);
+          r0[h] = make_float4(0.f, 0.f, 0.f, 0.f);
+          r1[h] = r0[h];
+          if (q < count) {
+            const int e = L.pc_pool[start + q];
+            const int node = e & 0x3fffffff;
+            near[h] = (e & 0x40000000) != 0;
+            const float4* rec = reinterpret_cast<const float4*>(P.quadf + node);
+            o[h] = node_offset(P.walk, node, P, w.geom);
+            r0[h] = rec[0];  // mass, soft, xx, xy
+            r1[h] = rec[1];  // xz, yy, yz, zz
+            if (e < 0) {     // monopole: no second moments, NaN softening (never softened)
+              r0[h] = make_float4(r0[h].x, qnan, 0.f, 0.f);
+              r1[h] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+          }
+        }
+        __syncwarp();
+        w.st[0][lane] = make_float4(o[0].x, o[1].x, o[0].y, o[1].y);
+        w.st[1][lane] = make_float4(o[0].z, o[1].z, r0[0].x, r0[1].x);
+        w.st[2][lane] = make_float4(r0[0].z, r0[1].z, r0[0].w, r0[1].w);
+        w.st[3][lane] = make_float4(r1[0].x, r1[1].x, r1[0].y, r1[1].y);
+        w.st[4][lane] = make_float4(r1[0].z, r1[1].z, r1[0].w, r1[1].w);
+        {  // (tr_a, tr_b, soft_a, soft_b); a near node carries its half trace negated
+          const float tra = 0.5f * (r0[0].z + r1[0].y + r1[0].w), trb = 0.5f * (r0[1].z + r1[1].y + r1[1].w);
+          w.st[5][lane] = make_float4(near[0] ? -tra : tra, near[1] ? -trb : trb, r0[0].y, r0[1].y);
+        }
+        __syncwarp();
+        const int npair = (min(64, count - cs) + 1) >> 1;
+        float2 ax2 = make_float2(0.f, 0.f), ay2 = ax2, az2 = ax2, pp2 = ax2, mm2 = ax2;
+        if (x.grp < x.G) {
+          for (int k = x.grp; k < npair; k += x.G) {
+            const float4 P5 = w.st[5][k];
+            if ((__float_as_int(P5.x) | __float_as_int(P5.y)) < 0) {  // a near node: scalar, softening tested
+              const float4 v = ev_p2c_pair_scalar(w, k, x.tx, x.ty, x.tz, x.ts);
+              ax2.x += v.x;
+              ay2.x += v.y;
+              az2.x += v.z;
+              pp2.x += v.w;
+              continue;
+            }
+            const float4 P0 = w.st[0][k], P1 = w.st[1][k];
+            const float2 rx = __fadd2_rn(make_float2(P0.x, P0.y), ntx);  // r' = o - t = -r
+            const float2 ry = __fadd2_rn(make_float2(P0.z, P0.w), nty);
+            const float2 rz = __fadd2_rn(make_float2(P1.x, P1.y), ntz);
+            float2 r2 = __fmul2_rn(rx, rx);
+            r2 = __ffma2_rn(ry, ry, r2);
+            r2 = __ffma2_rn(rz, rz, r2);
+            const float4 P2 = w.st[2][k], P3 = w.st[3][k], P4 = w.st[4][k];
+            const float2 a = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+            const float2 d2 = __fmul2_rn(a, a);
+            const float2 bb = __fmul2_rn(a, d2);                       // b = 1/r^3
+            const float2 nc = __fmul2_rn(__fmul2_rn(bb, d2), mthree);  // -c = -3/r^5
+            const float2 d = __fmul2_rn(__fmul2_rn(nc, d2), mfive);    // d = 15/r^7
+            const float2 xx = make_float2(P2.x, P2.y), xy = make_float2(P2.z, P2.w);
+            const float2 xz = make_float2(P3.x, P3.y), yy = make_float2(P3.z, P3.w);
+            const float2 yz = make_float2(P4.x, P4.y), zz = make_float2(P4.z, P4.w);
+            const float2 qx = __ffma2_rn(xz, rz, __ffma2_rn(xy, ry, __fmul2_rn(xx, rx)));  // q' = -q
+            const float2 qy = __ffma2_rn(yz, rz, __ffma2_rn(yy, ry, __fmul2_rn(xy, rx)));
+            const float2 qz = __ffma2_rn(zz, rz, __ffma2_rn(yz, ry, __fmul2_rn(xz, rx)));
+            const float2 qir = __fmul2_rn(half, __ffma2_rn(qz, rz, __ffma2_rn(qy, ry, __fmul2_rn(qx, rx))));
+            const float2 M = make_float2(P1.z, P1.w), tr = make_float2(P5.x, P5.y);
+            // qir3 = b M + d qir - c tr; acc += qir3 r' - c q'; pot += b tr - c qir - M a
+            const float2 qir3 = __ffma2_rn(nc, tr, __ffma2_rn(d, qir, __fmul2_rn(bb, M)));
+            ax2 = __ffma2_rn(nc, qx, __ffma2_rn(qir3, rx, ax2));
+            ay2 = __ffma2_rn(nc, qy, __ffma2_rn(qir3, ry, ay2));
+            az2 = __ffma2_rn(nc, qz, __ffma2_rn(qir3, rz, az2));
+            pp2 = __ffma2_rn(nc, qir, __ffma2_rn(bb, tr, pp2));
+            mm2 = __ffma2_rn(M, a, mm2);
+          }
+        }
+        K.add(0, ax2.x + ax2.y);
+        K.add(1, ay2.x + ay2.y);
+        K.add(2, az2.x + az2.y);
+        K.add(3, (pp2.x + pp2.y) - (mm2.x + mm2.y));
+      }
+      ev_finish(w, K, x, P, t0, lane, P.accumulate == 0);
+    }
+  }
+}
+
+// One source of a near leaf: Newtonian beyond the softening reach, the spline
+// inside it, nothing for the particle itself (r2 == 0).  pp sums +m a.
+__device__ __forceinline__ void ev_near_source(float m, float dx, float dy, float dz, float r2, float reach2,
+                                               float ssoft, float ts, float& ax, float& ay, float& az, float& pp) {
+  if (r2 > reach2) {
+    const float rinv = rsqrtf(r2);
+    const float mr = m * rinv;
+    const float mr3 = mr * rinv * rinv;
+    ax += dx * mr3;
+    ay += dy * mr3;
+    az += dz * mr3;
+    pp += mr;
+  } else if (r2 > 0.f) {
+    const float rinv = rsqrtf(r2);
+    float a, b;
+    spline_f32(r2, rinv, ssoft + ts, a, b);
+    const float bm = b * m;
+    ax += dx * bm;
+    ay += dy * bm;
+    az += dz * bm;
+    pp += m * a;
+  }
+}
+
+// P2P of the selected leaves w.lsel[0..nleaves) (GravityVisitor::leaf,
+// examples/GravityVisitor.h:144-160, in FP32): their sources are staged 64
+// per chunk as 32 interleaved pairs px = (x_a, x_b, y_a, y_b), pz = (z_a,
+// z_b, m_a, m_b), relative to the bucket, and evaluated with packed FP32.
+template <bool kFar>
+__device__ __forceinline__ void ev_p2p_leaves(EvalWarp& w, int nleaves, const TravParams& P, const EvTarget& x,
+                                              int lane, Kahan4& K) {
+  int s0a = 0, s0b = 0, na = 0, nb = 0;
+  if (lane < nleaves) {
+    const int nd = w.lsel[lane];
+    s0a = P.walk[nd].pstart;
+    na = P.walk[nd].pcount;
+    w.lof[lane] = node_offset(P.walk, nd, P, w.geom);
+  }
+  if (lane + 32 < nleaves) {
+    const int nd = w.lsel[lane + 32];
+    s0b = P.walk[nd].pstart;
+    nb = P.walk[nd].pcount;
+    w.lof[lane + 32] = node_offset(P.walk, nd, P, w.geom);
+  }
+  int inca = na, incb = nb;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int ya = __shfl_up_sync(kFull, inca, o), yb = __shfl_up_sync(kFull, incb, o);
+    if (lane >= o) {
+      inca += ya;
+      incb += yb;
+    }
+  }
+  const int tota = __shfl_sync(kFull, inca, 31);
+  const int total = tota + __shfl_sync(kFull, incb, 31);
+  if (lane < nleaves) {
+    w.pre[lane] = inca - na;
+    w.ps0[lane] = s0a;
+  }
+  if (lane + 32 < nleaves) {
+    w.pre[lane + 32] = tota + incb - nb;
+    w.ps0[lane + 32] = s0b;
+  }
+  if (lane == 0) w.pre[nleaves] = total;
+  __syncwarp();
+  const float kPadPos = 1.0e10f;
+  const float gs = (float)w.geom.soft_max;
+  const float2 ntx = make_float2(-x.tx, -x.tx), nty = make_float2(-x.ty, -x.ty), ntz = make_float2(-x.tz, -x.tz);
+  int base_leaf = 0;
+  for (int cs = 0; cs < total; cs += 64) {
+    {  // stage this lane's two sources
+      const int q0 = cs + 2 * lane;
+      int lo = base_leaf;  // last leaf with pre <= q: a chunk spans few leaves
+      while (lo + 1 < nleaves && w.pre[lo + 1] <= q0) lo++;
+      int lo1 = lo;
+      while (lo1 + 1 < nleaves && w.pre[lo1 + 1] <= q0 + 1) lo1++;
+      base_leaf = __shfl_sync(kFull, lo1, 31);
+      float4 ra = make_float4(kPadPos, kPadPos, kPadPos, 0.f), rb = ra;
+      float4 oa = make_float4(0.f, 0.f, 0.f, 0.f), ob = oa;
+      float sa = 0.f, sb = 0.f;
+      if (q0 < total) {
+        oa = w.lof[lo];
+        const int j = w.ps0[lo] + (q0 - w.pre[lo]);
+        ra = P.srcf[j];
+        if (!kFar) sa = P.softf[j];
+      }
+      if (q0 + 1 < total) {
+        ob = w.lof[lo1];
+        const int j = w.ps0[lo1] + (q0 + 1 - w.pre[lo1]);
+        rb = P.srcf[j];
+        if (!kFar) sb = P.softf[j];
+      }
+      __syncwarp();
+      w.st[0][lane] = make_float4(ra.x + oa.x, rb.x + ob.x, ra.y + oa.y, rb.y + ob.y);
+      w.st[1][lane] = make_float4(ra.z + oa.z, rb.z + ob.z, ra.w, rb.w);
+      if (!kFar) {
+        const float qa = sa + gs, qb = sb + gs;
+        // a padded source (zero mass) takes the Newtonian branch
+        w.st[2][lane] = make_float4(ra.w != 0.f ? qa * qa : -1.f, rb.w != 0.f ? qb * qb : -1.f, sa, sb);
+      }
+      __syncwarp();
+    }
+    const int np = (min(64, total - cs) + 1) >> 1;
+    float2 ax2 = make_float2(0.f, 0.f), ay2 = ax2, az2 = ax2, pp2 = ax2;  // pp2 sums +m/r
+    if (x.grp < x.G) {
+      for (int k = x.grp; k < np; k += x.G) {
+        const float4 X = w.st[0][k], Z = w.st[1][k];
+        const float2 dx = __fadd2_rn(make_float2(X.x, X.y), ntx);
+        const float2 dy = __fadd2_rn(make_float2(X.z, X.w), nty);
+        const float2 dz = __fadd2_rn(make_float2(Z.x, Z.y), ntz);
+        float2 r2 = __fmul2_rn(dx, dx);
+        r2 = __ffma2_rn(dy, dy, r2);
+        r2 = __ffma2_rn(dz, dz, r2);
+        bool fast = true;
+        float4 R = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (!kFar) {
+          R = w.st[2][k];
+          fast = (r2.x > R.x) && (r2.y > R.y);
+        }
+        if (fast) {
+          const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+          const float2 mr = __fmul2_rn(make_float2(Z.z, Z.w), ri);
+          const float2 mr3 = __fmul2_rn(mr, __fmul2_rn(ri, ri));
+          ax2 = __ffma2_rn(dx, mr3, ax2);
+          ay2 = __ffma2_rn(dy, mr3, ay2);
+          az2 = __ffma2_rn(dz, mr3, az2);
+          pp2 = __fadd2_rn(pp2, mr);
+        } else {
+          ev_near_source(Z.z, dx.x, dy.x, dz.x, r2.x, R.x, R.z, x.ts, ax2.x, ay2.x, az2.x, pp2.x);
+          ev_near_source(Z.w, dx.y, dy.y, dz.y, r2.y, R.y, R.w, x.ts, ax2.y, ay2.y, az2.y, pp2.y);
+        }
+      }
+    }
+    K.add(0, ax2.x + ax2.y);
+    K.add(1, ay2.x + ay2.y);
+    K.add(2, az2.x + az2.y);
+    K.add(3, -(pp2.x + pp2.y));
+  }
+  __syncwarp();
+}
+
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2p(TravParams P, ListParams L,
+                                                                     const Mom* __restrict__ mom) {
+  __shared__ EvalWarp warps[kEvWarps];
+  EvalWarp& w = warps[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  int64_t b;
+  int tnode;
+  while (next_bucket(P, lane, b, tnode)) {
+    if (tnode < 0 || tnode >= P.nnodes) continue;
+    const int64_t lb = b - P.b_begin;
+    const int64_t start = L.pp_start[lb];
+    const int count = L.pp_count[lb];
+    __syncwarp();
+    if (lane == 0) load_bucket_geom(mom, tnode, w.geom);
+    __syncwarp();
+    const int tbase = P.walk[tnode].pstart, ntot = P.walk[tnode].pcount;
+    for (int tc = 0; tc < ntot; tc += 32) {
+      const int t0 = tbase + tc, nt = min(32, ntot - tc);
+      const EvTarget x = ev_target(P.p, w.geom, t0, nt, lane);
+      Kahan4 K;
+      K.zero();
+      for (int blk = 0; blk < count; blk += 64) {
+        const bool va = blk + lane < count, vb = blk + lane + 32 < count;
+        const int ea = va ? L.pp_pool[start + blk + lane] : 0;
+        const int eb = vb ? L.pp_pool[start + blk + lane + 32] : 0;
+#pragma unroll
+        for (int kind = 0; kind < 2; kind++) {  // far leaves, then near leaves
+          const bool sa = va && ((ea < 0) == (kind == 1)), sb = vb && ((eb < 0) == (kind == 1));
+          const unsigned ma = __ballot_sync(kFull, sa), mb = __ballot_sync(kFull, sb);
+          const unsigned lt = (1u << lane) - 1u;
+          __syncwarp();
+          if (sa) w.lsel[__popc(ma & lt)] = ea & 0x7fffffff;
+          if (sb) w.lsel[__popc(ma) + __popc(mb & lt)] = eb & 0x7fffffff;
+          __syncwarp();
+          const int n = __popc(ma) + __popc(mb);
+          if (n) {
+            if (kind == 0) ev_p2p_leaves<true>(w, n, P, x, lane, K);
+            else ev_p2p_leaves<false>(w, n, P, x, lane, K);
+          }
+        }
+      }
+      ev_finish(w, K, x, P, t0, lane, false);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- launchers
+int walk_lists_grid(int sms) { return sms * 8; }
+
+void launch_walk_lists(const TravParams& P, const ListParams& L, const Mom* mom, int grid, cudaStream_t st) {
+  note_launch();
+  walk_lists<<<grid, kWlWarps * 32, 0, st>>>(P, L, mom);
+}
+// eval_p2c keeps 80 registers (6 CTAs per SM; at 64 it spills), eval_p2p
+// fits 64 (8 CTAs per SM)
+void launch_eval_lists(const TravParams& P, const ListParams& L, const Mom* mom, int grid, cudaStream_t st,
+                       unsigned* work2) {
+  TravParams Q = P;
+  Q.work = work2;
+  note_launch();
+  eval_p2c<6><<<grid, kEvWarps * 32, 0, st>>>(P, L, mom);
+  note_launch();
+  eval_p2p<8><<<grid, kEvWarps * 32, 0, st>>>(Q, L, mom);
+}
+
+}  // namespace pt

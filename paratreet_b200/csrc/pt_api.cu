@@ -68,6 +68,18 @@ struct pt_handle {
   double* dsum = nullptr;  // direct-sum scratch (caller-order copies + partials)
   int64_t dsum_cap = 0;
 
+  // two-phase mixed traversal: list pools and per-bucket list descriptors
+  bool two_phase = true;  // PT_MIXED_FUSED=1 selects the fused walk + evaluate kernel
+  int32_t *pool_pc = nullptr, *pool_pp = nullptr;
+  unsigned long long cap_pc = 0, cap_pp = 0;    // allocated entries of each pool
+  unsigned long long want_pc = 0, want_pp = 0;  // entries the next pass should have
+  int64_t *l_pc_start = nullptr, *l_pp_start = nullptr;
+  int32_t *l_pc_count = nullptr, *l_pp_count = nullptr;
+  int64_t l_nb_cap = 0;
+  unsigned long long* d_lcur = nullptr;  // [0] P2C cursor, [1] P2P cursor, [2] longest list
+  unsigned* d_work3 = nullptr;           // bucket queues of the three kernels
+  unsigned l_thresh = 4096;
+
   double4* d_htab = nullptr;  // Ewald reciprocal table (h vector, hCfac)
   int htab_cap = 0;
   double* ewd = nullptr;  // Ewald direct-sum scratch
@@ -230,6 +242,7 @@ int read_status(pt_handle* h) {
     if (st & kErrCapacity) m += " capacity exceeded;";
     if (st & kErrAdjointSoftened) m += " adjoint met a softened quadrupole term (not differentiated);";
     if (st & kErrSort) m += " radix sort look-back timed out;";
+    if (st & kErrPool) m += " interaction-list pools exhausted;";
     return fail(h, (st & kErrNonFinite) ? PT_E_NONFINITE : PT_E_DEVICE, m);
   }
   return PT_OK;
@@ -402,7 +415,105 @@ int ewald_correction_pass(pt_handle* h, int64_t b0, int64_t b1) {
   return PT_OK;
 }
 
+// Two-phase mixed evaluation: walk_lists writes every bucket's interaction
+// list to the pools, then eval_p2c and eval_p2p evaluate them.  Pools are
+// sized from the previous pass; a pass whose lists outgrow their regions or
+// pools is repeated (counters restored) with larger ones.
+int run_two_phase(pt_handle* h, TravParams& P) {
+  cudaStream_t st = h->stream;
+  const int64_t nb = P.b_end - P.b_begin;
+  if (nb <= 0) return PT_OK;
+  if (nb > h->l_nb_cap) {
+    CKR(dalloc(h, &h->l_pc_start, nb));
+    CKR(dalloc(h, &h->l_pp_start, nb));
+    CKR(dalloc(h, &h->l_pc_count, nb));
+    CKR(dalloc(h, &h->l_pp_count, nb));
+    h->l_nb_cap = nb;
+  }
+  if (!h->d_lcur) CKR(dalloc(h, &h->d_lcur, 3));
+  if (!h->d_work3) CKR(dalloc(h, &h->d_work3, 3));
+  const int wgrid = (int)std::max<int64_t>(1, std::min<int64_t>(walk_lists_grid(h->sms), (nb + 3) / 4));
+  unsigned long long c0[3];
+  CK(cudaMemcpyAsync(c0, h->d_counters, sizeof(c0), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  ListParams L{};
+  for (int attempt = 0;; attempt++) {
+    const unsigned region = 2 * h->l_thresh;
+    const unsigned long long slack = (unsigned long long)wgrid * 4 * region;
+    const unsigned long long need_pc =
+        std::max<unsigned long long>(h->want_pc ? h->want_pc + slack : 0, 1024ull * nb + slack);
+    const unsigned long long need_pp =
+        std::max<unsigned long long>(h->want_pp ? h->want_pp + slack : 0, 256ull * nb + slack);
+    if (need_pc > h->cap_pc || need_pp > h->cap_pp) {
+      dfree(h->pool_pc);
+      dfree(h->pool_pp);
+      h->cap_pc = h->cap_pp = 0;
+      if (cudaMalloc((void**)&h->pool_pc, need_pc * sizeof(int32_t)) != cudaSuccess ||
+          cudaMalloc((void**)&h->pool_pp, need_pp * sizeof(int32_t)) != cudaSuccess) {
+        // no room for the lists: this handle evaluates with the fused kernel from now on
+        cudaGetLastError();
+        dfree(h->pool_pc);
+        dfree(h->pool_pp);
+        h->two_phase = false;
+        CK(cudaMemcpyAsync(h->d_counters, c0, sizeof(c0), cudaMemcpyHostToDevice, st));
+        launch_traverse_mixed(P, h->nd.mom, h->sms * 16, h->mixed_variant, st);
+        CK(cudaGetLastError());
+        return PT_OK;
+      }
+      h->cap_pc = need_pc;
+      h->cap_pp = need_pp;
+    }
+    L.pc_pool = h->pool_pc;
+    L.pp_pool = h->pool_pp;
+    L.cursor = h->d_lcur;
+    L.cap_pc = h->cap_pc;
+    L.cap_pp = h->cap_pp;
+    L.region = region;
+    L.thresh = h->l_thresh;
+    L.pc_start = h->l_pc_start;
+    L.pc_count = h->l_pc_count;
+    L.pp_start = h->l_pp_start;
+    L.pp_count = h->l_pp_count;
+    L.max_len = reinterpret_cast<unsigned*>(h->d_lcur + 2);
+    CK(cudaMemsetAsync(h->d_lcur, 0, 3 * sizeof(unsigned long long), st));
+    CK(cudaMemsetAsync(h->d_work3, 0, 3 * sizeof(unsigned), st));
+    TravParams A = P;
+    A.work = h->d_work3;
+    launch_walk_lists(A, L, h->nd.mom, wgrid, st);
+    CK(cudaGetLastError());
+    unsigned status = 0;
+    unsigned long long cur[3];
+    CK(cudaMemcpyAsync(&status, h->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(cur, h->d_lcur, sizeof(cur), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    // the cursors count reserved regions (also refused ones): at most the pool size is used
+    const unsigned long long used_pc = std::min(cur[0], h->cap_pc), used_pp = std::min(cur[1], h->cap_pp);
+    if (!(status & kErrPool)) {
+      // next pass: room for this pass's lists and a quarter more
+      h->want_pc = std::max<unsigned long long>(h->want_pc, used_pc + used_pc / 4);
+      h->want_pp = std::max<unsigned long long>(h->want_pp, used_pp + used_pp / 4);
+      break;
+    }
+    if (attempt >= 4) return fail(h, PT_E_NOMEM, "interaction lists outgrow their pools");
+    // repeat the walk with larger regions and pools
+    status &= ~kErrPool;
+    CK(cudaMemcpyAsync(h->d_status, &status, sizeof(unsigned), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(h->d_counters, c0, sizeof(c0), cudaMemcpyHostToDevice, st));
+    const unsigned longest = (unsigned)cur[2];
+    while (h->l_thresh < 2 * longest + 64) h->l_thresh *= 2;
+    h->l_thresh *= 2;
+    h->want_pc = 2 * h->cap_pc;
+    h->want_pp = 2 * h->cap_pp;
+  }
+  TravParams E = P;
+  E.work = h->d_work3 + 1;
+  launch_eval_lists(E, L, h->nd.mom, h->sms * 16, st, h->d_work3 + 2);
+  CK(cudaGetLastError());
+  return PT_OK;
+}
+
 int run_traversal(pt_handle* h, TravParams& P, int grid) {
+  if (h->cfg.precision == PT_MIXED && P.mode == 0 && h->two_phase) return run_two_phase(h, P);
   if (h->cfg.precision == PT_MIXED && P.mode != 1)
     launch_traverse_mixed(P, h->nd.mom, grid, h->mixed_variant, h->stream);
   else launch_traverse_f64(P, h->nd.mom, grid, h->stream);
@@ -633,6 +744,7 @@ int pt_create(const pt_config* cfg, pt_handle** out) {
   if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess) return bail(PT_E_CUDA);
   h->sms = prop.multiProcessorCount;
   if (const char* v = std::getenv("PT_MIXED_VARIANT")) h->mixed_variant = std::atoi(v);
+  if (const char* v = std::getenv("PT_MIXED_FUSED")) h->two_phase = std::atoi(v) == 0;
   if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) return bail(PT_E_CUDA);
   h->stream = h->own_stream;
   for (auto& e : h->ev)
@@ -666,6 +778,8 @@ int pt_destroy(pt_handle* h) {
   dfree(o.fifo); dfree(o.nleaf_sub); dfree(o.nempty_sub); dfree(o.leaf_base); dfree(o.empty_base);
   dfree(h->flags); dfree(h->buckets); dfree(h->bucket_work); dfree(h->list_count); dfree(h->list_off); dfree(h->list_node);
   dfree(h->list_kind); dfree(h->dsum); dfree(h->adj); dfree(h->nadj); dfree(h->d_htab); dfree(h->ewd);
+  dfree(h->pool_pc); dfree(h->pool_pp); dfree(h->l_pc_start); dfree(h->l_pp_start); dfree(h->l_pc_count);
+  dfree(h->l_pp_count); dfree(h->d_lcur); dfree(h->d_work3);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);

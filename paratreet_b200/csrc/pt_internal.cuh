@@ -28,6 +28,7 @@ enum : unsigned {
   kErrCapacity = 1u << 4,
   kErrAdjointSoftened = 1u << 5,
   kErrSort = 1u << 6,                 // radix sort look-back gave up waiting
+  kErrPool = 1u << 7,                 // two-phase traversal: a list outgrew its region or pool (retried)
 };
 
 // Particle state, structure of arrays, FP64, in key-sorted order after a build.
@@ -120,6 +121,23 @@ struct TravParams {
   unsigned long long* counters;  // n_pp, n_pc, n_open
   unsigned int* work;     // dynamic bucket counter
   unsigned int* status;
+};
+
+// Interaction lists of the two-phase mixed traversal (k_mixed2.cu): two pools
+// of node indices (bit 31 = monopole for P2C, near for P2P), per-warp regions
+// reserved from the cursors, and per bucket (index b - b_begin) the start and
+// length of its contiguous list in each pool.
+struct ListParams {
+  int32_t* pc_pool;
+  int32_t* pp_pool;
+  unsigned long long* cursor;  // [0] P2C pool, [1] P2P pool
+  unsigned long long cap_pc, cap_pp;
+  unsigned region, thresh;     // region size; least space left before a bucket starts
+  int64_t* pc_start;
+  int32_t* pc_count;
+  int64_t* pp_start;
+  int32_t* pp_count;
+  unsigned* max_len;           // longest list of the pass
 };
 
 // Root cell of the periodic cube for the Ewald correction (k_ewald.cu):

@@ -66,6 +66,14 @@ void launch_ewald_recip(const double* x, const double* y, const double* z, const
                         int64_t nt, const double4* kv, int nk, const double* S, double alpha, double V, double* out,
                         cudaStream_t st);
 
+// k_mixed2.cu
+int walk_lists_grid(int sms);
+void launch_walk_lists(const TravParams& P, const ListParams& L, const Mom* mom, int grid, cudaStream_t st);
+// eval_p2c (store or add per P.accumulate) then eval_p2p (add); each takes its
+// bucket queue from P.work and work2 respectively (zeroed by the caller)
+void launch_eval_lists(const TravParams& P, const ListParams& L, const Mom* mom, int grid, cudaStream_t st,
+                       unsigned* work2);
+
 // k_adjoint.cu
 void launch_adjoint(const AdjParams& A, int grid, cudaStream_t st);
 
