@@ -291,7 +291,8 @@ def main():
                                   "(profiles/traffic_traverse_mixed_plummer_16m.md)" if traffic else None,
                 "dram_gbs": (traffic / t_trav / 1e9) if traffic else None,
                 "dram_frac_of_hbm": (traffic / t_trav / 1e9 / hbm) if traffic else None,
-                "kernel": f"traverse_{a.precision}", "flops_per_launch": flops,
+                "kernel": "walk_lists + eval_p2c + eval_p2p" if a.precision == "mixed" else "traverse_f64",
+                "flops_per_launch": flops,
                 "flop_model": "20 per P2P pair + 66 per P2C evaluation",
                 "peak_source": f"nominal: {nsm} SMs x {lanes} {'FP32' if lanes == 128 else 'FP64'} lanes x 2 x "
                                f"{sm_max:.0f} MHz (no measured FP32/FP64 figure in MEASURED_PEAKS.json)"}
@@ -320,11 +321,11 @@ def main():
     return 0
 
 
-# DRAM bytes (read + write) of one traverse_mixed launch on the default
-# workload (Plummer N = 2^24, bucket 32, theta 0.7), from
-# ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum (1 pass);
+# DRAM bytes (read + write) of one mixed traversal on the default workload
+# (Plummer N = 2^24, bucket 32, theta 0.7): walk_lists + eval_p2c + eval_p2p,
+# from ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum (1 pass);
 # profiles/traffic_traverse_mixed_plummer_16m.md holds the command and figures.
-TRAVERSE_MIXED_TRAFFIC_16M = 1479119104 + 677974784
+TRAVERSE_MIXED_TRAFFIC_16M = (517378560 + 8313764352) + (8061403904 + 662865664) + (3190561280 + 539555840)
 
 
 def traversal_traffic(a):
