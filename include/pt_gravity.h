@@ -222,6 +222,19 @@ int pt_chain_grad(pt_handle* h, int nsteps, double dt, int ckpt_every, const dou
                   const double* yz, double* loss, double* gx, double* gy, double* gz, double* gvx,
                   double* gvy, double* gvz, double* gm);
 
+/* SPH density ---------------------------------------------------------------
+ * The density pass of the reference's SPH example on the same tree:
+ * startUpAndDown<DensityVisitor> (examples/SPH.C:77-86, examples/
+ * DensityVisitor.h: the k = 32 nearest neighbours of every particle, the
+ * particle itself included) and DensityFn (examples/SPH.C:11-37): ball_sq =
+ * the 32nd smallest d2, density = sum_j kernelM4(4 d2_j / ball_sq) m_j /
+ * (pi/8 ball_sq^1.5) with kernelM4 of examples/SPHUtils.h.  FP64; the tree is
+ * rebuilt from the current positions (an earlier force pass's results are
+ * dropped).  Caller order; any output may be NULL except that nbr and nbr_d2
+ * go together: 32 neighbours per particle (caller indices, -1 past N) sorted
+ * by (d2, index), and their d2. */
+int pt_sph_density(pt_handle* h, double* density, double* ball_sq, int32_t* nbr, double* nbr_d2);
+
 /* FP64 direct sum (the force-error yardstick) ------------------------------
  * Isolated spline-softened sum over all particles for nt caller indices,
  * the kernel of examples/GravityVisitor.h:87-120 with twoh = soft_i + soft_j. */

@@ -69,6 +69,7 @@ def _port_lib():
         lib.pto_forces.argtypes = [C.c_void_p, C.c_int]
         lib.pto_run.argtypes = [C.c_void_p, C.c_int]
         lib.pto_direct.argtypes = [C.c_int] + [_dp] * 5 + [C.c_int, _i32p] + [_dp] * 4 + [C.c_int]
+        lib.pto_sph_density.argtypes = [C.c_int] + [_dp] * 4 + [C.c_int, C.c_int, _dp, _dp, _i32p, _dp]
         lib.pto_set_periodic.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_double, C.c_double]
         lib.pto_ewald_direct.argtypes = [C.c_int] + [_dp] * 5 + [C.c_double, C.c_int, _i32p] + [_dp] * 4 + [C.c_int]
         _port = lib
@@ -85,6 +86,7 @@ def _ref_lib():
         lib.ptref_set_record_lists.argtypes = [C.c_void_p, C.c_int]
         lib.ptref_forces_sample.argtypes = [C.c_void_p, C.c_double] + [C.POINTER(C.c_double)] * 3
         lib.ptref_set_periodic.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int]
+        lib.ptref_sph_density.argtypes = [C.c_void_p, _dp, _dp, _i32p, _dp]
         _ref = lib
     return _ref
 
@@ -214,6 +216,15 @@ class RefSim(_Sim):
         """Periodic cube (the reference's fEwCut 2.6 and |h| <= 2.8)."""
         self._lib.ptref_set_periodic(self._h, 1, period, n_replicas)
 
+    def sph_density(self):
+        """The reference's DensityVisitor + DensityFn (k = 32): density, ball^2,
+        neighbours (caller order, sorted by (d2, index)) and their d2."""
+        n, k = self.n, 32
+        d, b, nd2 = np.zeros(n), np.zeros(n), np.zeros(n * k)
+        nbr = np.zeros(n * k, np.int32)
+        self._lib.ptref_sph_density(self._h, d, b, nbr, nd2)
+        return d, b, nbr.reshape(n, k), nd2.reshape(n, k)
+
     def forces(self, record_lists=False):
         self._lib.ptref_set_record_lists(self._h, 1 if record_lists else 0)
         self._lib.ptref_run(self._h, 0)
@@ -253,6 +264,17 @@ def ewald_direct_sum(p: dict, targets: np.ndarray, period: float = 1.0, threads:
     a = _arrs(p)
     lib.pto_ewald_direct(p["x"].size, a[0], a[1], a[2], a[6], a[7], period, t.size, t, *out, threads)
     return out
+
+
+def sph_density(p: dict, k: int = 32, threads: int = 1):
+    """Brute-force k-nearest-neighbour SPH density (the C restatement)."""
+    lib = _port_lib()
+    n = p["x"].size
+    a = _arrs(p)
+    d, b, nd2 = np.zeros(n), np.zeros(n), np.zeros(n * k)
+    nbr = np.zeros(n * k, np.int32)
+    lib.pto_sph_density(n, a[0], a[1], a[2], a[6], k, threads, d, b, nbr, nd2)
+    return d, b, nbr.reshape(n, k), nd2.reshape(n, k)
 
 
 def sort_tree(t: Tree) -> Tree:

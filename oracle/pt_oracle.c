@@ -1036,3 +1036,53 @@ void pto_ewald_direct(int n, const double* x, const double* y, const double* z, 
   free(kv);
   free(S);
 }
+
+/* SPH density of the reference's SPH example (examples/SPH.C:11-37 DensityFn,
+ * examples/DensityVisitor.h leaf(), kernelM4 examples/SPHUtils.h:20-26): the
+ * k nearest neighbours of every particle, itself included, found here by
+ * brute force; rsq = the k-th distance^2; density = sum_j kernelM4(d2_j * 4 /
+ * rsq) m_j / (pi/8 rsq^1.5).  d2 = dx*dx + dy*dy + dz*dz with dx = x_i - x_j,
+ * as Vector3D::lengthSquared.  Neighbours (caller order) sorted by (d2, index);
+ * the density is summed in that order. */
+static double kernel_m4(double ar2) {
+  double ak = 2.0 - sqrt(ar2);
+  if (ar2 < 1.0) ak = (1.0 - 0.75 * ak * ar2);
+  else ak = 0.25 * ak * ak * ak;
+  return ak;
+}
+
+void pto_sph_density(int n, const double* x, const double* y, const double* z, const double* m, int k,
+                     int threads, double* density, double* ballsq, int* nbr, double* nd2) {
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 16) num_threads(threads > 0 ? threads : 1)
+#endif
+  for (int i = 0; i < n; i++) {
+    double bd[64];
+    int bi[64];
+    int cnt = 0;
+    const int kk = k < 64 ? k : 64;
+    for (int j = 0; j < n; j++) {
+      double dx = x[i] - x[j], dy = y[i] - y[j], dz = z[i] - z[j];
+      double d2 = dx * dx + dy * dy + dz * dz;
+      if (cnt == kk && !(d2 < bd[kk - 1] || (d2 == bd[kk - 1] && j < bi[kk - 1]))) continue;
+      int p = cnt < kk ? cnt++ : kk - 1;
+      while (p > 0 && (bd[p - 1] > d2 || (bd[p - 1] == d2 && bi[p - 1] > j))) {
+        bd[p] = bd[p - 1];
+        bi[p] = bi[p - 1];
+        p--;
+      }
+      bd[p] = d2;
+      bi[p] = j;
+    }
+    const double rsq = bd[cnt - 1], fBall = sqrt(rsq), ih2 = 4.0 / rsq;
+    double dens = 0.0;
+    for (int q = 0; q < cnt; q++) dens += kernel_m4(bd[q] * ih2) * m[bi[q]];
+    dens /= (0.125 * M_PI * (rsq * fBall));
+    density[i] = dens;
+    ballsq[i] = rsq;
+    for (int q = 0; q < k; q++) {
+      nbr[(size_t)i * k + q] = q < cnt ? bi[q] : -1;
+      nd2[(size_t)i * k + q] = q < cnt ? bd[q] : -1.0;
+    }
+  }
+}

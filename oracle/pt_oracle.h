@@ -54,6 +54,11 @@ void pto_ewald_direct(int n, const double* x, const double* y, const double* z, 
                       const double* soft, double L, int nt, const int* targets, double* ax, double* ay,
                       double* az, double* pot, int threads);
 
+/* SPH density of the reference's SPH example: k nearest neighbours (itself
+ * included, brute force) and the M4-kernel density; see pt_oracle.c. */
+void pto_sph_density(int n, const double* x, const double* y, const double* z, const double* m, int k,
+                     int threads, double* density, double* ballsq, int* nbr, double* nd2);
+
 /* FP64 direct sum (spline softening, twoh = soft_i + soft_j, G = 1) over
  * all n sources for nt target indices; isolated (no periodic images). */
 void pto_direct(int n, const double* x, const double* y, const double* z, const double* m,

@@ -25,6 +25,11 @@
  *                     per Partition (src/Partition.h:129-134)
  *   step              src/Driver.h:183-251: forces -> kick -> perturb ->
  *                     new universe -> rekey; dt from examples/Gravity.C:63-67
+ *   SPH density       examples/SPH.C:11-37 and :77-86: the reference's own
+ *                     DensityVisitor (examples/DensityVisitor.h) driven by a
+ *                     restated up-and-down walk per bucket
+ *                     (src/Traverser.h:363-482), then DensityFn with the
+ *                     reference's kernelM4 (examples/SPHUtils.h)
  *   periodic          examples/Gravity.C:19-50: EwaldInit on the root's data
  *                     (examples/Ewald.C, compiled in ref_ewald.cpp), the
  *                     (2n+1)^3 replica walks with GravityVisitor offsets, then
@@ -71,6 +76,20 @@ template <typename D>
 struct Partition;
 #define PARATREET_REGISTER_PER_LEAF_FN(name, data, fn) static auto name = fn;
 #include "Ewald.h"
+
+// Stand-in for src/ThreadStateHolder.h (a Charm++ group): doSPHCalc hands it
+// the reaction on the neighbour ("opposing effect"), summed per particle.
+class ThreadStateHolder {
+ public:
+  std::vector<Vector3D<Real>> acc;
+  std::vector<Real> work;
+  void applyOpposingEffect(const Particle& b, Vector3D<Real> a, Real w) {
+    acc[b.order] += a;
+    work[b.order] += w;
+  }
+};
+#include "DensityVisitor.h"
+#include "SPHUtils.h"
 
 namespace {
 
@@ -300,6 +319,80 @@ double now() {
 #endif
 }
 
+// One bucket's up-and-down walk (src/Traverser.h:363-482): its own leaf
+// first, then, climbing to each ancestor, the ancestor's other children in
+// child order, each subtree depth first with the visitor's open().
+template <typename Visitor>
+void upnd_bucket(Visitor& v, RNode* bucket) {
+  auto down = [&](RNode* start) {
+    std::vector<RNode*> st{start};
+    while (!st.empty()) {
+      RNode* node = st.back();
+      st.pop_back();
+      if (node->type == RNode::Type::Leaf) {
+        v.leaf(*node, *bucket);
+      } else if (node->type == RNode::Type::Internal) {
+        if (v.open(*node, *bucket)) {
+          for (int i = 0; i < node->n_children; i++) st.push_back(node->getChild(i));
+        } else {
+          v.node(*node, *bucket);
+        }
+      }
+    }
+  };
+  down(bucket);
+  RNode* top = bucket;
+  while (top->parent) {
+    RNode* par = top->parent;
+    for (int j = 0; j < par->n_children; j++)
+      if (par->getChild(j) != top) down(par->getChild(j));
+    top = par;
+  }
+}
+
+// examples/SPH.C:77-86 (startUpAndDown<DensityVisitor>) and DensityFn
+// (SPH.C:11-37): k = 32 nearest neighbours (the particle itself included),
+// then the M4-kernel density.  Outputs in caller order; nbr / nd2 hold each
+// particle's neighbours sorted by (distance^2, caller index).
+void sph_density(RefSim& s, double* density, double* ballsq, int* nbr, double* nd2, int kmax) {
+  buildTree(s);
+  const size_t nb = s.leaves.size();
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 4) num_threads(s.threads)
+#endif
+  for (long b = 0; b < (long)nb; b++) {
+    DensityVisitor v;
+    upnd_bucket(v, s.leaves[b]);
+  }
+  for (size_t b = 0; b < nb; b++) {
+    auto& leaf = *s.leaves[b];
+    for (int pi = 0; pi < leaf.n_particles; pi++) {
+      const Particle& part = leaf.particles()[pi];
+      auto& Q = leaf.data.pps[pi].neighbors;
+      auto rsq = Q[0].fKey, fBall = std::sqrt(rsq);
+      Real dens = 0.;
+      auto ih2 = 4.0 / rsq;
+      for (int i = 0; i < (int)Q.size(); i++) {
+        auto& fDist2 = Q[i].fKey;
+        auto r2 = fDist2 * ih2;
+        auto rs = paratreet::kernelM4(r2);
+        dens += rs * Q[i].pPtr->mass;
+      }
+      Real r_cubed = rsq * fBall;
+      dens /= (0.125 * M_PI * r_cubed);
+      density[part.order] = dens;
+      ballsq[part.order] = rsq;
+      std::vector<std::pair<double, int>> q;
+      for (auto& e : Q) q.push_back({e.fKey, e.pPtr->order});
+      std::sort(q.begin(), q.end());
+      for (int i = 0; i < kmax; i++) {
+        nbr[(size_t)part.order * kmax + i] = i < (int)q.size() ? q[i].second : -1;
+        nd2[(size_t)part.order * kmax + i] = i < (int)q.size() ? q[i].first : -1.0;
+      }
+    }
+  }
+}
+
 void forces(RefSim& s) {
   double t0 = now();
   buildTree(s);
@@ -454,6 +547,12 @@ int ptref_run(void* hp, int nsteps) {
     remakeUniverse(s, box);
     assignKeys(s);
   }
+  return 0;
+}
+
+/* SPH density of the reference's SPH example (k = 32 neighbours). */
+int ptref_sph_density(void* h, double* density, double* ballsq, int* nbr, double* nd2) {
+  sph_density(*(RefSim*)h, density, ballsq, nbr, nd2, 32);
   return 0;
 }
 

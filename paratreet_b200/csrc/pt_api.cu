@@ -80,6 +80,11 @@ struct pt_handle {
   unsigned* d_work3 = nullptr;           // bucket queues of the three kernels
   unsigned l_thresh = 4096;
 
+  double* sph = nullptr;  // SPH density pass: density, ball^2 (2n), neighbours (k n int32 + k n double)
+  int64_t sph_cap = 0, sph_nbr_cap = 0;
+  int32_t* sph_nbr = nullptr;
+  double* sph_nd2 = nullptr;
+
   double4* d_htab = nullptr;  // Ewald reciprocal table (h vector, hCfac)
   int htab_cap = 0;
   double* ewd = nullptr;  // Ewald direct-sum scratch
@@ -777,7 +782,7 @@ int pt_destroy(pt_handle* h) {
   dfree(o.first_child); dfree(o.count); dfree(o.mom); dfree(o.walk); dfree(o.quad); dfree(o.quadf);
   dfree(o.fifo); dfree(o.nleaf_sub); dfree(o.nempty_sub); dfree(o.leaf_base); dfree(o.empty_base);
   dfree(h->flags); dfree(h->buckets); dfree(h->bucket_work); dfree(h->list_count); dfree(h->list_off); dfree(h->list_node);
-  dfree(h->list_kind); dfree(h->dsum); dfree(h->adj); dfree(h->nadj); dfree(h->d_htab); dfree(h->ewd);
+  dfree(h->list_kind); dfree(h->dsum); dfree(h->adj); dfree(h->nadj); dfree(h->d_htab); dfree(h->ewd); dfree(h->sph); dfree(h->sph_nbr); dfree(h->sph_nd2);
   dfree(h->pool_pc); dfree(h->pool_pp); dfree(h->l_pc_start); dfree(h->l_pp_start); dfree(h->l_pc_count);
   dfree(h->l_pp_count); dfree(h->d_lcur); dfree(h->d_work3);
   for (auto& e : h->ev)
@@ -863,6 +868,67 @@ int pt_device_accel(pt_handle* h, double** ax, double** ay, double** az, double*
   if (pot) *pot = h->p.pot;
   if (pot_full) *pot_full = h->p.potf;
   if (order) *order = h->p.order;
+  return PT_OK;
+}
+
+int pt_sph_density(pt_handle* h, double* density, double* ball_sq, int32_t* nbr, double* nbr_d2) {
+  if (!h || ((nbr == nullptr) != (nbr_d2 == nullptr))) return PT_E_ARG;
+  if (!h->p.x) return fail(h, PT_E_STATE, "no particles");
+  cudaSetDevice(h->cfg.device);
+  cudaStream_t st = h->stream;
+  const int64_t n = h->n;
+  const int k = sph_k();
+  if (n == 0) return PT_OK;
+  CKR(keys_and_sort(h));
+  CKR(build_tree(h));
+  CKR(upward(h));
+  // the particle arrays were re-sorted: results of an earlier force pass no longer line up
+  h->have_forces = false;
+  h->forces_current = false;
+  h->lists_valid = false;
+  if (2 * n > h->sph_cap) {
+    CKR(dalloc(h, &h->sph, 2 * n));
+    h->sph_cap = 2 * n;
+  }
+  const bool want_nbr = nbr != nullptr;
+  if (want_nbr && n * k > h->sph_nbr_cap) {
+    CKR(dalloc(h, &h->sph_nbr, n * k));
+    CKR(dalloc(h, &h->sph_nd2, n * k));
+    h->sph_nbr_cap = n * k;
+  }
+  CK(cudaMemsetAsync(h->d_work, 0, sizeof(unsigned), st));
+  launch_sph_density(h->p, h->nd.mom, h->nd.walk, h->buckets, h->nbuckets, h->nnodes, h->sph, h->sph + n,
+                     want_nbr ? h->sph_nbr : nullptr, want_nbr ? h->sph_nd2 : nullptr, h->d_work, h->d_status,
+                     h->sms * 16, st);
+  CK(cudaGetLastError());
+  CKR(read_status(h));
+  CKR(unpermute_f64(h, h->sph, density));
+  CK(cudaStreamSynchronize(st));
+  CKR(unpermute_f64(h, h->sph + n, ball_sq));
+  CK(cudaStreamSynchronize(st));
+  if (want_nbr) {
+    // neighbours of sorted particle i -> caller order, each list sorted by (d2, caller index)
+    std::vector<int32_t> hn((size_t)n * k), order(n);
+    std::vector<double> hd((size_t)n * k);
+    CK(cudaMemcpyAsync(hn.data(), h->sph_nbr, hn.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hd.data(), h->sph_nd2, hd.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(order.data(), h->p.order, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    std::vector<std::pair<double, int32_t>> row(k);
+    for (int64_t i = 0; i < n; i++) {
+      int m = 0;
+      for (int e = 0; e < k; e++) {
+        const int32_t j = hn[(size_t)i * k + e];
+        if (j >= 0) row[m++] = {hd[(size_t)i * k + e], order[j]};
+      }
+      std::sort(row.begin(), row.begin() + m);
+      const int64_t c = order[i];
+      for (int e = 0; e < k; e++) {
+        nbr[c * k + e] = e < m ? row[e].second : -1;
+        nbr_d2[c * k + e] = e < m ? row[e].first : -1.0;
+      }
+    }
+  }
   return PT_OK;
 }
 

@@ -74,6 +74,12 @@ void launch_walk_lists(const TravParams& P, const ListParams& L, const Mom* mom,
 void launch_eval_lists(const TravParams& P, const ListParams& L, const Mom* mom, int grid, cudaStream_t st,
                        unsigned* work2);
 
+// k_sph.cu
+int sph_k();
+void launch_sph_density(Particles p, const Mom* mom, const WalkRec* walk, const int32_t* buckets, int64_t nbuckets,
+                        int64_t nnodes, double* density, double* ballsq, int32_t* nbr, double* nd2, unsigned* work,
+                        unsigned* status, int grid, cudaStream_t st);
+
 // k_adjoint.cu
 void launch_adjoint(const AdjParams& A, int grid, cudaStream_t st);
 

@@ -261,6 +261,17 @@ class GravitySimulation:
         self._check(self._lib.pt_ewald_direct_sum(self._h, t.size, L.ptr(t), *[L.ptr(o) for o in out]))
         return out
 
+    def sph_density(self, neighbors: bool = False):
+        """Density pass of the SPH example (DensityVisitor + DensityFn, k = 32):
+        density and ball^2 per particle, and with neighbors=True the 32
+        neighbours (caller indices, sorted by (d2, index)) and their d2."""
+        n = self.n
+        d, b = np.empty(n), np.empty(n)
+        nbr = np.empty((n, 32), np.int32) if neighbors else None
+        nd2 = np.empty((n, 32)) if neighbors else None
+        self._check(self._lib.pt_sph_density(self._h, L.ptr(d), L.ptr(b), L.ptr(nbr), L.ptr(nd2)))
+        return (d, b, nbr, nd2) if neighbors else (d, b)
+
     def direct_sum(self, targets):
         t = np.ascontiguousarray(targets, dtype=np.int32)
         out = [np.empty(t.size) for _ in range(4)]

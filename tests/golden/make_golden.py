@@ -21,6 +21,12 @@ ref_<case>.json
     per-bucket interaction lists, accelerations, partial potentials, and the
     state after the configured number of kick/perturb steps.  The C oracle
     and the CUDA path must reproduce these bit for bit.
+sph_<case>.json
+    The reference's SPH density pass (examples/DensityVisitor.h with a
+    restated up-and-down walk, DensityFn of examples/SPH.C, kernelM4 of
+    examples/SPHUtils.h): digests of every particle's 32 neighbours (sorted
+    by distance, then index), their d2 and the ball radii, and sampled
+    densities (which depend on the heap's summation order in the last bits).
 periodic_<case>.json
     The same sources in periodic mode (examples/Gravity.C replica walks plus
     the Ewald correction of examples/Ewald.{h,C}) on a displaced lattice:
@@ -54,6 +60,12 @@ CASES = {
     "mixture_16k": (ics.mixture, dict(n=16384, seed=7, soft=1e-4), 16, 0.7, 1e-4, 3),
     "plummer_4k_b32_t05": (ics.plummer, dict(n=4096, seed=5, soft=1e-3), 32, 0.5, 0.01, 1),
     "hernquist_8k_t10": (ics.hernquist, dict(n=8192, seed=3, soft=0.01), 32, 1.0, 0.005, 2),
+}
+
+# name -> (generator, kwargs, bucket)
+SPH_CASES = {
+    "plummer_4k": (ics.plummer, dict(n=4096, seed=9, soft=0.01), 16),
+    "mixture_8k": (ics.mixture, dict(n=8192, seed=2, soft=1e-4), 32),
 }
 
 # name -> (lattice kwargs, bucket, theta, n_replicas)
@@ -140,6 +152,22 @@ def run_periodic_case(name):
     print(name, p["x"].size)
 
 
+def run_sph_case(name):
+    gen, kw, bucket = SPH_CASES[name]
+    p = gen(**kw)
+    r = O.RefSim(p, bucket=bucket, threads=1)
+    dens, ball, nbr, nd2 = r.sph_density()
+    idx = [0, 1, 2, int(p["x"].size // 2), int(p["x"].size - 1)]
+    out = {
+        "case": name, "generator": gen.__name__, "kwargs": kw, "bucket": bucket,
+        "sha256": {"nbr": digest(nbr.astype(np.int32)), "nbr_d2": digest(nd2), "ball_sq": digest(ball)},
+        "samples": {"idx": idx, "density": [float(dens[i]) for i in idx]},
+    }
+    with open(os.path.join(OUT, f"sph_{name}.json"), "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+    print(name, p["x"].size)
+
+
 def read_tipsy_dark(path):
     with open(path, "rb") as f:
         buf = f.read()
@@ -179,6 +207,7 @@ def main():
     ap.add_argument("--reference", default="/root/reference")
     ap.add_argument("--cases", nargs="*", default=list(CASES))
     ap.add_argument("--periodic-cases", nargs="*", default=list(PERIODIC_CASES))
+    ap.add_argument("--sph-cases", nargs="*", default=list(SPH_CASES))
     a = ap.parse_args()
     if not O.ref_available():
         sys.exit("oracle/_ref/libptref.so is missing: run `make -C oracle` with the reference mounted")
@@ -187,6 +216,8 @@ def main():
         run_case(c)
     for c in a.periodic_cases:
         run_periodic_case(c)
+    for c in a.sph_cases:
+        run_sph_case(c)
 
 
 if __name__ == "__main__":
