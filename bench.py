@@ -336,6 +336,25 @@ def traversal_traffic(a):
     return None
 
 
+def sph_density_rate(a, sim, stream):
+    """The SPH example's density pass (k = 32 neighbours + M4 density) on
+    the same particles: particles/s through pt_sph_density (tree build,
+    neighbour search, density and the D2H of density and ball^2)."""
+    import torch
+    sim.sph_density()
+    ts = []
+    for _ in range(2):
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        sim.sph_density()
+        s1.record(stream)
+        torch.cuda.synchronize()
+        ts.append(s0.elapsed_time(s1) / 1e3)
+    sim.start_down()  # leave the handle with a force pass, as the other extras expect
+    return {"particles_per_s": a.n / float(np.mean(ts)), "ms_per_pass": 1e3 * float(np.mean(ts)),
+            "neighbours": 32, "note": "density pass of the SPH example: tree build + kNN + density + D2H"}
+
+
 def phase_rooflines(c, n, peaks):
     """HBM roofline of the bandwidth-bound phases of the last pass: their
     algorithmic bytes (keys 36 B/particle; sort 8 + 8 x 24 B and permute of
@@ -443,6 +462,7 @@ def extras(a, sim, p, world, rank, stream, value, shard=None):
     sim.set_precision(a.precision)
     v_other = n / float(np.mean(t64))
     res["theta_sweep"] = theta_sweep(a, sim, tgt, (dax, day, daz), stream) if a.sweep else []
+    res["sph_density"] = sph_density_rate(a, sim, stream)
     res["precision_comparison"] = {
         f"{a.precision}_force_evals_per_s": value, f"{other}_force_evals_per_s": v_other,
         "ratio_mixed_over_fp64": (value / v_other) if a.precision == "mixed" else (v_other / value),
