@@ -51,6 +51,15 @@ enum {
                    FP32 accumulation */
 };
 
+/* Traverser of the FP64 form (the interaction set is the same; the order in
+ * which a bucket's interactions are summed, and so the last bits, differ). */
+enum {
+  PT_TRANSPOSED_DOWN = 0,  /* Partition::startDown: TransposedDownTraverser, pre-order
+                              per bucket (src/Partition.h:129-134, src/Traverser.h:154-217) */
+  PT_BASIC_DOWN = 1        /* Partition::startBasicDown: BasicDownTraverser, breadth first
+                              per bucket (src/Partition.h:148-152, src/Traverser.h:296-330) */
+};
+
 /* Integrator of pt_step. */
 enum {
   PT_KKD = 0,  /* the reference's iteration (src/Driver.h:218-250,
@@ -82,7 +91,8 @@ typedef struct pt_config {
   double period;      /* cube side L (> 0) */
   double ewald_rcut;  /* fEwCut, examples/Ewald.h:26 (default 2.6) */
   double ewald_hcut;  /* dEwhCut, examples/Ewald.C:86 (default 2.8) */
-  int reserved[8];
+  int traversal;      /* PT_TRANSPOSED_DOWN (default) or PT_BASIC_DOWN */
+  int reserved[7];
 } pt_config;
 
 typedef struct pt_handle pt_handle;

@@ -71,6 +71,7 @@ def _port_lib():
         lib.pto_direct.argtypes = [C.c_int] + [_dp] * 5 + [C.c_int, _i32p] + [_dp] * 4 + [C.c_int]
         lib.pto_sph_density.argtypes = [C.c_int] + [_dp] * 4 + [C.c_int, C.c_int, _dp, _dp, _i32p, _dp]
         lib.pto_set_periodic.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_double, C.c_double]
+        lib.pto_set_traversal.argtypes = [C.c_void_p, C.c_int]
         lib.pto_ewald_direct.argtypes = [C.c_int] + [_dp] * 5 + [C.c_double, C.c_int, _i32p] + [_dp] * 4 + [C.c_int]
         _port = lib
     return _port
@@ -86,6 +87,7 @@ def _ref_lib():
         lib.ptref_set_record_lists.argtypes = [C.c_void_p, C.c_int]
         lib.ptref_forces_sample.argtypes = [C.c_void_p, C.c_double] + [C.POINTER(C.c_double)] * 3
         lib.ptref_set_periodic.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int]
+        lib.ptref_set_traversal.argtypes = [C.c_void_p, C.c_int]
         lib.ptref_sph_density.argtypes = [C.c_void_p, _dp, _dp, _i32p, _dp]
         _ref = lib
     return _ref
@@ -186,6 +188,10 @@ class PortSim(_Sim):
         h = lib.pto_create(n, *_arrs(p), bucket, theta, dt_max, threads)
         super().__init__(lib, h, n)
 
+    def set_basic_down(self, on=True):
+        """Breadth-first per-bucket order (Partition::startBasicDown)."""
+        self._lib.pto_set_traversal(self._h, 1 if on else 0)
+
     def set_periodic(self, period=1.0, n_replicas=1, rcut=2.6, hcut=2.8):
         """Periodic cube: replica walks plus the Ewald correction."""
         self._lib.pto_set_periodic(self._h, 1, period, n_replicas, rcut, hcut)
@@ -211,6 +217,10 @@ class RefSim(_Sim):
         n = p["x"].size
         h = lib.ptref_create(n, *_arrs(p), bucket, theta, dt_max, group, threads)
         super().__init__(lib, h, n)
+
+    def set_basic_down(self, on=True):
+        """Breadth-first per-bucket order (Partition::startBasicDown)."""
+        self._lib.ptref_set_traversal(self._h, 1 if on else 0)
 
     def set_periodic(self, period=1.0, n_replicas=1):
         """Periodic cube (the reference's fEwCut 2.6 and |h| <= 2.8)."""

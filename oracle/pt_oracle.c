@@ -57,6 +57,8 @@ struct pto_sim {
   double t_build, t_trav;
   /* periodic cube (examples/Gravity.C:34-50, examples/Ewald.{h,C}) */
   int periodic, n_replicas;
+  /* 0: TransposedDownTraverser (startDown), 1: BasicDownTraverser (startBasicDown) */
+  int basic_down;
   double period, ewald_rcut, ewald_hcut;
 };
 
@@ -705,6 +707,46 @@ static void walk(pto_sim* s, int tgt, double gfac, int record, unsigned long lon
   }
 }
 
+/* BasicDownTraverser::doTrav (src/Traverser.h:296-330): a deque used first in,
+ * first out -- children pushed at the front in index order, nodes taken from
+ * the back -- so one bucket's nodes are visited breadth first. */
+static void walk_bfs(pto_sim* s, int tgt, double gfac, int record, unsigned long long* cnt, const double off[3],
+                     int* queue) {
+  long head = 0, tail = 0;
+  queue[tail++] = 0;
+  while (head < tail) {
+    int nd = queue[head++];
+    int ty = s->ntype[nd];
+    if (ty == PTO_LEAF) {
+      visit_leaf(s, nd, tgt, off);
+      cnt[0] += (unsigned long long)s->nnp[nd] * (unsigned long long)s->nnp[tgt];
+      if (record) list_push(s, s->nkey[nd], 0);
+    } else if (ty == PTO_INTERNAL) {
+      cnt[2]++;
+      if (visit_open(&s->mom[nd], &s->mom[tgt], gfac, off)) {
+        int c0 = s->nchild[nd];
+        for (int c = 0; c < 8; c++) queue[tail++] = c0 + c;
+      } else {
+        visit_node(s, nd, tgt, off);
+        cnt[1] += (unsigned long long)s->nnp[tgt];
+        if (record) list_push(s, s->nkey[nd], 1);
+      }
+    }
+  }
+}
+
+static void walk_any(pto_sim* s, int tgt, double gfac, int record, unsigned long long* cnt, const double off[3]) {
+  if (!s->basic_down) {
+    walk(s, tgt, gfac, record, cnt, off);
+    return;
+  }
+  int* queue = (int*)malloc(sizeof(int) * (size_t)(s->nnodes + 1));
+  walk_bfs(s, tgt, gfac, record, cnt, off, queue);
+  free(queue);
+}
+
+void pto_set_traversal(pto_sim* s, int basic_down) { s->basic_down = basic_down; }
+
 static void traverse(pto_sim* s, int record) {
   double gfac = kOpenGeom / (s->theta * s->theta);
   memset(s->ax, 0, sizeof(double) * s->n);
@@ -721,7 +763,7 @@ static void traverse(pto_sim* s, int record) {
     for (long b = 0; b < s->nleaves; b++) {
       unsigned long long c[3] = {0, 0, 0};
       s->list_off[b] = s->list_total;
-      walk(s, s->leaves[b], gfac, 1, c, zero);
+      walk_any(s, s->leaves[b], gfac, 1, c, zero);
       pp += c[0]; pc += c[1]; op += c[2];
     }
     s->list_off[s->nleaves] = s->list_total;
@@ -737,7 +779,7 @@ static void traverse(pto_sim* s, int record) {
 #endif
           for (long b = 0; b < s->nleaves; b++) {
             unsigned long long c[3] = {0, 0, 0};
-            walk(s, s->leaves[b], gfac, 0, c, s->periodic ? off : zero);
+            walk_any(s, s->leaves[b], gfac, 0, c, s->periodic ? off : zero);
             pp += c[0]; pc += c[1]; op += c[2];
           }
         }

@@ -46,6 +46,10 @@ void pto_get_bucket_keys(const pto_sim* s, uint64_t* keys);
 long pto_list_total(const pto_sim* s);
 void pto_get_lists(const pto_sim* s, long* offsets, uint64_t* keys, int* kinds);
 
+/* 0: the transposed down traversal (Partition::startDown, pre-order per
+ * bucket); 1: the basic down traversal (Partition::startBasicDown,
+ * breadth first per bucket) -- the same interactions in another order. */
+void pto_set_traversal(pto_sim* s, int basic_down);
 /* Periodic cube of side L: (2n+1)^3 replica walks and the reference's Ewald
  * correction with real-space radius rcut*L and reciprocal cut |h| <= hcut. */
 void pto_set_periodic(pto_sim* s, int periodic, double L, int n_replicas, double rcut, double hcut);

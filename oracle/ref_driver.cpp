@@ -115,6 +115,7 @@ struct RefSim {
   int periodic = 0;
   double period = 1.0;
   int n_replicas = 0;
+  int basic_down = 0;  // Partition::startBasicDown instead of startDown
   // state
   std::vector<Particle> particles;  // sorted by key after each build
   OrientedBox<Real> universe;
@@ -265,6 +266,39 @@ struct GroupTrav {
   }
 };
 
+// BasicDownTraverser::doTrav (src/Traverser.h:296-330) for one bucket: a
+// deque, children pushed at the front, nodes taken from the back.
+void basic_down_bucket(RefSim& s, size_t b, unsigned long long& pp, unsigned long long& pc,
+                       unsigned long long& op) {
+  GravityVisitor v(Vector3D<Real>(0, 0, 0), s.theta);
+  RNode* bucket = s.leaves[b];
+  std::deque<RNode*> nodes;
+  nodes.push_front(s.root);
+  while (!nodes.empty()) {
+    RNode* node = nodes.back();
+    nodes.pop_back();
+    switch (node->type) {
+      case RNode::Type::Leaf:
+        v.leaf(*node, *bucket);
+        pp += (unsigned long long)node->n_particles * bucket->n_particles;
+        if (s.record_lists) s.lists[b].push_back({node->key, 0});
+        break;
+      case RNode::Type::Internal:
+        op++;
+        if (v.open(*node, *bucket)) {
+          for (int idx = 0; idx < node->n_children; idx++) nodes.push_front(node->getChild(idx));
+        } else {
+          v.node(*node, *bucket);
+          pc += (unsigned long long)bucket->n_particles;
+          if (s.record_lists) s.lists[b].push_back({node->key, 1});
+        }
+        break;
+      default:
+        break;
+    }
+  }
+}
+
 void traverse(RefSim& s) {
   size_t nb = s.leaves.size();
   if (s.record_lists) {
@@ -278,6 +312,16 @@ void traverse(RefSim& s) {
     nReplicas = s.n_replicas;
     ewaldProxy.local = &ewald;
     ewald.EwaldInit(s.root->data, CkCallback());
+  }
+  if (s.basic_down && !s.periodic) {
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : pp, pc, op) num_threads(s.threads)
+#endif
+    for (long b = 0; b < (long)nb; b++) basic_down_bucket(s, (size_t)b, pp, pc, op);
+    s.n_pp = pp;
+    s.n_pc = pc;
+    s.n_open = op;
+    return;
   }
   const int nr = s.periodic ? s.n_replicas : 0;
   for (int X = -nr; X <= nr; X++)
@@ -549,6 +593,9 @@ int ptref_run(void* hp, int nsteps) {
   }
   return 0;
 }
+
+/* 1: Partition::startBasicDown (breadth first per bucket), 0: startDown. */
+void ptref_set_traversal(void* h, int basic_down) { ((RefSim*)h)->basic_down = basic_down; }
 
 /* SPH density of the reference's SPH example (k = 32 neighbours). */
 int ptref_sph_density(void* h, double* density, double* ballsq, int* nbr, double* nd2) {

@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(HERE, "libpt_gravity.so")
 PT_OK = 0
 PT_FP64, PT_MIXED = 0, 1
 PT_KKD, PT_KDK = 0, 1
+PT_TRANSPOSED_DOWN, PT_BASIC_DOWN = 0, 1
 
 ERRORS = {
     -1: "PT_E_ARG", -2: "PT_E_CUDA", -3: "PT_E_NOMEM", -4: "PT_E_STATE",
@@ -44,7 +45,8 @@ class PtConfig(C.Structure):
         ("period", C.c_double),
         ("ewald_rcut", C.c_double),
         ("ewald_hcut", C.c_double),
-        ("reserved", C.c_int * 8),
+        ("traversal", C.c_int),
+        ("reserved", C.c_int * 7),
     ]
 
 

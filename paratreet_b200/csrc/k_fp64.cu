@@ -349,6 +349,7 @@ struct F64Eval {
 
 __global__ void __launch_bounds__(kTravWarps * 32) traverse_f64(TravParams P, const Mom* __restrict__ mom) {
   __shared__ WalkFrame stacks[kTravWarps][kWalkStack];
+  __shared__ int32_t queues[kTravWarps][kBfsQueue];  // basic-down order only
   __shared__ double stage[kTravWarps][5 * 32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   unsigned long long c_pp = 0, c_pc = 0, c_open = 0;
@@ -368,7 +369,9 @@ __global__ void __launch_bounds__(kTravWarps * 32) traverse_f64(TravParams P, co
     const int tbase = P.walk[tnode].pstart, ntot = P.walk[tnode].pcount;
     if (P.mode == 1) {  // count the interaction list only
       ListRecorder rec{lane, 1, 0, 0, nullptr, nullptr};
-      if (!walk_bucket(P.walk, P.nnodes, g, P.ox, P.oy, P.oz, stacks[wid], lane, rec, c_open, P.status) &&
+      if (!(P.bfs ? walk_bucket_bfs(P.walk, P.nnodes, g, P.ox, P.oy, P.oz, queues[wid], kBfsQueue, lane, rec,
+                                    c_open, P.status)
+                  : walk_bucket(P.walk, P.nnodes, g, P.ox, P.oy, P.oz, stacks[wid], lane, rec, c_open, P.status)) &&
           lane == 0)
         atomicOr(P.status, kErrStack);
       if (lane == 0) P.list_count[b - P.b_begin] = rec.n;
@@ -410,7 +413,9 @@ __global__ void __launch_bounds__(kTravWarps * 32) traverse_f64(TravParams P, co
       ev.lbase = ev.record ? P.list_off[b - P.b_begin] : 0;
       ev.lnode = P.list_node;
       ev.lkind = P.list_kind;
-      if (!walk_bucket(P.walk, P.nnodes, g, P.ox, P.oy, P.oz, stacks[wid], lane, ev, opens, P.status) &&
+      if (!(P.bfs ? walk_bucket_bfs(P.walk, P.nnodes, g, P.ox, P.oy, P.oz, queues[wid], kBfsQueue, lane, ev,
+                                    opens, P.status)
+                  : walk_bucket(P.walk, P.nnodes, g, P.ox, P.oy, P.oz, stacks[wid], lane, ev, opens, P.status)) &&
           lane == 0)
         atomicOr(P.status, kErrStack);
       if (tc == 0) c_open += opens;

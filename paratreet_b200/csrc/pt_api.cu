@@ -547,6 +547,7 @@ int traverse(pt_handle* h, int64_t b0, int64_t b1) {
   P.b_end = b1;
   P.ox = P.oy = P.oz = 0.0;
   P.bucket_work = h->bucket_work;
+  P.bfs = (h->cfg.traversal == PT_BASIC_DOWN) ? 1 : 0;
   if (h->nbuckets > 0) CK(cudaMemsetAsync(h->bucket_work, 0, h->nbuckets * sizeof(unsigned long long), st));
   P.nnodes = h->nnodes;
   P.counters = h->d_counters;
@@ -730,6 +731,7 @@ int pt_create(const pt_config* cfg, pt_handle** out) {
   *out = nullptr;
   if (!(cfg->theta > 0.0) || cfg->bucket < 1 || cfg->bucket > 32) return PT_E_ARG;
   if (cfg->precision != PT_FP64 && cfg->precision != PT_MIXED) return PT_E_ARG;
+  if (cfg->traversal != PT_TRANSPOSED_DOWN && cfg->traversal != PT_BASIC_DOWN) return PT_E_ARG;
   if (cfg->integrator != PT_KKD && cfg->integrator != PT_KDK) return PT_E_ARG;
   if (cfg->periodic && (!(cfg->period > 0.0) || cfg->n_replicas < 0 || cfg->n_replicas > 8 ||
                         !(cfg->ewald_rcut > 0.0) || cfg->ewald_rcut > 8.0 || !(cfg->ewald_hcut >= 0.0) ||

@@ -114,6 +114,7 @@ struct TravParams {
   int mode;               // 0 evaluate, 1 count lists only, 2 evaluate + record lists
   int accumulate;         // add to the stored accelerations (replica walks after the first)
   unsigned long long* bucket_work;  // per bucket (DFS index): P2P pairs + P2C evaluations; may be null
+  int bfs;                // FP64 walk in BasicDownTraverser order (breadth first) instead of pre-order
   int64_t* list_count;    // mode 1: entries per bucket
   const int64_t* list_off;// mode 2: CSR offsets
   int32_t* list_node;     // mode 2: node index per entry

@@ -26,6 +26,7 @@
 namespace pt {
 
 constexpr int kWalkStack = 32;
+constexpr int kBfsQueue = 512;  // pending sibling frames of a breadth-first walk
 constexpr unsigned kFull = 0xffffffffu;
 
 // Child classes.
@@ -173,6 +174,47 @@ __device__ __forceinline__ bool walk_bucket(const WalkRec* __restrict__ walk, in
     } else {
       bits = 0;
     }
+  }
+  return true;
+}
+
+// The same walk in BasicDownTraverser order (src/Traverser.h:296-330, the
+// deque used first in, first out): breadth first per bucket.  Siblings stay
+// consecutive in that order, so the unit of the queue is a frame -- the 8
+// children of an opened node -- processed in child order, each opened child
+// queuing its own frame at the back.  queue is a per-warp ring of qcap frames
+// (first-child indices).  Returns false if the ring overflows.
+template <class Eval>
+__device__ __forceinline__ bool walk_bucket_bfs(const WalkRec* __restrict__ walk, int64_t nnodes,
+                                                const BucketGeom& g, double ox, double oy, double oz,
+                                                int32_t* queue, int qcap, int lane, Eval& ev,
+                                                unsigned long long& n_open, unsigned* status) {
+  int c0 = 0;  // the root, as a one-child frame
+  uint32_t bits = classify_children(walk, nnodes, 0, 1, g, ox, oy, oz, lane, n_open, status);
+  int head = 0, tail = 0;
+  while (true) {
+    const uint32_t pp = bits & 0xffu, pq = (bits >> 8) & 0xffu, pm = (bits >> 16) & 0xffu, op = bits >> 24;
+    uint32_t all = pp | pq | pm | op;
+    while (all) {
+      const int k = __ffs(all) - 1;
+      all &= all - 1u;
+      if ((pp >> k) & 1u) {
+        ev.p2p(c0 + k);
+      } else if (((pq | pm) >> k) & 1u) {
+        ev.p2c(c0 + k, ((pm >> k) & 1u) != 0);
+      } else {
+        if (tail - head >= qcap) return false;
+        const int fc = walk[c0 + k].first_child;
+        __syncwarp();
+        if (lane == 0) queue[tail % qcap] = fc;
+        __syncwarp();
+        ++tail;
+      }
+    }
+    if (head == tail) break;
+    c0 = queue[head % qcap];
+    ++head;
+    bits = classify_children(walk, nnodes, c0, 8, g, ox, oy, oz, lane, n_open, status);
   }
   return true;
 }

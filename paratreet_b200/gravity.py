@@ -61,6 +61,7 @@ class Configuration:
     period: float = 1.0           # Configuration::fPeriod (cubic)
     ewald_rcut: float = 2.6       # fEwCut, examples/Ewald.h:26
     ewald_hcut: float = 2.8       # dEwhCut, examples/Ewald.C:86
+    traversal: str = "transposed"  # "transposed" (Partition::startDown) or "basic" (startBasicDown)
 
 
 @dataclass
@@ -104,6 +105,7 @@ class GravitySimulation:
         cfg.period = conf.period
         cfg.ewald_rcut = conf.ewald_rcut
         cfg.ewald_hcut = conf.ewald_hcut
+        cfg.traversal = {"transposed": L.PT_TRANSPOSED_DOWN, "basic": L.PT_BASIC_DOWN}[conf.traversal]
         h = C.c_void_p()
         rc = self._lib.pt_create(C.byref(cfg), C.byref(h))
         if rc != L.PT_OK:

@@ -21,6 +21,10 @@ ref_<case>.json
     per-bucket interaction lists, accelerations, partial potentials, and the
     state after the configured number of kick/perturb steps.  The C oracle
     and the CUDA path must reproduce these bit for bit.
+basic_<case>.json
+    The reference's gravity sources under the basic down traversal
+    (Partition::startBasicDown: breadth first per bucket): digests of the
+    accelerations, partial potentials and interaction lists.
 sph_<case>.json
     The reference's SPH density pass (examples/DensityVisitor.h with a
     restated up-and-down walk, DensityFn of examples/SPH.C, kernelM4 of
@@ -60,6 +64,12 @@ CASES = {
     "mixture_16k": (ics.mixture, dict(n=16384, seed=7, soft=1e-4), 16, 0.7, 1e-4, 3),
     "plummer_4k_b32_t05": (ics.plummer, dict(n=4096, seed=5, soft=1e-3), 32, 0.5, 0.01, 1),
     "hernquist_8k_t10": (ics.hernquist, dict(n=8192, seed=3, soft=0.01), 32, 1.0, 0.005, 2),
+}
+
+# name -> (generator, kwargs, bucket, theta)
+BASIC_CASES = {
+    "plummer_4k": (ics.plummer, dict(n=4096, seed=11, soft=0.01), 16, 0.7),
+    "hernquist_6k_t05": (ics.hernquist, dict(n=6000, seed=4, soft=0.01), 8, 0.5),
 }
 
 # name -> (generator, kwargs, bucket)
@@ -152,6 +162,25 @@ def run_periodic_case(name):
     print(name, p["x"].size)
 
 
+def run_basic_case(name):
+    gen, kw, bucket, theta = BASIC_CASES[name]
+    p = gen(**kw)
+    r = O.RefSim(p, bucket=bucket, theta=theta, threads=1)
+    r.set_basic_down()
+    r.forces(record_lists=True)
+    ax, ay, az, pot = r.acc()
+    lists = r.lists()
+    out = {
+        "case": name, "generator": gen.__name__, "kwargs": kw, "bucket": bucket, "theta": theta,
+        "sha256": {"ax": digest(ax), "ay": digest(ay), "az": digest(az), "pot": digest(pot),
+                   "list_offsets": digest(lists.offsets.astype(np.int64)), "list_keys": digest(lists.keys),
+                   "list_kinds": digest(lists.kinds.astype(np.int32))},
+    }
+    with open(os.path.join(OUT, f"basic_{name}.json"), "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+    print(name, p["x"].size)
+
+
 def run_sph_case(name):
     gen, kw, bucket = SPH_CASES[name]
     p = gen(**kw)
@@ -208,6 +237,7 @@ def main():
     ap.add_argument("--cases", nargs="*", default=list(CASES))
     ap.add_argument("--periodic-cases", nargs="*", default=list(PERIODIC_CASES))
     ap.add_argument("--sph-cases", nargs="*", default=list(SPH_CASES))
+    ap.add_argument("--basic-cases", nargs="*", default=list(BASIC_CASES))
     a = ap.parse_args()
     if not O.ref_available():
         sys.exit("oracle/_ref/libptref.so is missing: run `make -C oracle` with the reference mounted")
@@ -218,6 +248,8 @@ def main():
         run_periodic_case(c)
     for c in a.sph_cases:
         run_sph_case(c)
+    for c in a.basic_cases:
+        run_basic_case(c)
 
 
 if __name__ == "__main__":

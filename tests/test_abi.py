@@ -55,6 +55,9 @@ def test_create_rejects_bad_config():
     cfg.theta = 0.0
     assert lib.pt_create(C.byref(cfg), C.byref(h)) == -1
     cfg.theta = 0.7
+    cfg.traversal = 2  # neither PT_TRANSPOSED_DOWN nor PT_BASIC_DOWN
+    assert lib.pt_create(C.byref(cfg), C.byref(h)) == -1
+    cfg.traversal = L.PT_BASIC_DOWN
     # periodic: positive period, 0..8 replica shells, bounded cuts, no recorded lists
     cfg.periodic = 1
     assert (cfg.period, cfg.ewald_rcut, cfg.ewald_hcut) == (1.0, 2.6, 2.8)
