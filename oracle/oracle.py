@@ -88,6 +88,7 @@ def _ref_lib():
         lib.ptref_forces_sample.argtypes = [C.c_void_p, C.c_double] + [C.POINTER(C.c_double)] * 3
         lib.ptref_set_periodic.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int]
         lib.ptref_set_traversal.argtypes = [C.c_void_p, C.c_int]
+        lib.ptref_dual.argtypes = [C.c_void_p, _dp, _dp, _dp, _u64p]
         lib.ptref_sph_density.argtypes = [C.c_void_p, _dp, _dp, _i32p, _dp]
         _ref = lib
     return _ref
@@ -225,6 +226,14 @@ class RefSim(_Sim):
     def set_periodic(self, period=1.0, n_replicas=1):
         """Periodic cube (the reference's fEwCut 2.6 and |h| <= 2.8)."""
         self._lib.ptref_set_periodic(self._h, 1, period, n_replicas)
+
+    def dual(self):
+        """Subtree::startDual<GravityVisitor> (one subtree): ax, ay, az and
+        (P2P pairs, P2C evaluations)."""
+        a = [np.zeros(self.n) for _ in range(3)]
+        c = np.zeros(2, np.uint64)
+        self._lib.ptref_dual(self._h, *a, c)
+        return a, (int(c[0]), int(c[1]))
 
     def sph_density(self):
         """The reference's DensityVisitor + DensityFn (k = 32): density, ball^2,

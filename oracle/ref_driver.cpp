@@ -363,6 +363,72 @@ double now() {
 #endif
 }
 
+// DualTraverser (src/Traverser.h:485-610) with the reference's GravityVisitor
+// on a single subtree (local root = root): a stack of (source, target) pairs
+// from (root, root); cell() asks whether to open the target
+// (GravityVisitor::cell, examples/GravityVisitor.h:226-229); with
+// TargetMustBeLeaf an internal target is handled by runInvertedTraversal.
+struct DualTrav {
+  RefSim& s;
+  GravityVisitor v;
+  unsigned long long pp = 0, pc = 0;
+  explicit DualTrav(RefSim& sim) : s(sim), v(Vector3D<Real>(0, 0, 0), sim.theta) {}
+  void inverted(RNode* source, RNode* target) {  // runInvertedTraversal
+    std::vector<RNode*> st{target};
+    while (!st.empty()) {
+      RNode* node = st.back();
+      st.pop_back();
+      if (node->isLeaf()) {
+        if (node->type == RNode::Type::Leaf) {
+          v.leaf(*source, *node);  // an internal source carries no particles (n_particles = -1)
+          if (source->n_particles > 0) pp += (unsigned long long)source->n_particles * node->n_particles;
+        }
+      } else if (v.open(*source, *node)) {
+        for (int j = 0; j < node->n_children; j++) st.push_back(node->getChild(j));
+      } else {
+        v.node(*source, *node);
+        pc += (unsigned long long)node->n_particles;
+      }
+    }
+  }
+  void run() {
+    std::vector<std::pair<RNode*, RNode*>> st{{s.root, s.root}};
+    while (!st.empty()) {
+      RNode* node = st.back().first;
+      RNode* pay = st.back().second;
+      st.pop_back();
+      if (pay->type == RNode::Type::EmptyLeaf) continue;
+      if (node->type == RNode::Type::Leaf) {
+        if (pay->isLeaf()) {
+          v.leaf(*node, *pay);
+          pp += (unsigned long long)node->n_particles * pay->n_particles;
+        } else {
+          inverted(node, pay);
+        }
+      } else if (node->type == RNode::Type::Internal) {
+        if (pay->isLeaf()) {
+          if (v.open(*node, *pay)) {
+            for (int i = 0; i < node->n_children; i++) st.push_back({node->getChild(i), pay});
+          } else {
+            v.node(*node, *pay);
+            pc += (unsigned long long)pay->n_particles;
+          }
+        } else if (!v.cell(*node, *pay)) {
+          inverted(node, pay);  // TargetMustBeLeaf
+        } else {
+          for (int i = 0; i < node->n_children; i++) {
+            if (pay->depth <= node->depth) {  // ForceEvenDepth
+              for (int j = 0; j < pay->n_children; j++) st.push_back({node->getChild(i), pay->getChild(j)});
+            } else {
+              st.push_back({node->getChild(i), pay});
+            }
+          }
+        }
+      }
+    }
+  }
+};
+
 // One bucket's up-and-down walk (src/Traverser.h:363-482): its own leaf
 // first, then, climbing to each ancestor, the ancestor's other children in
 // child order, each subtree depth first with the visitor's open().
@@ -591,6 +657,27 @@ int ptref_run(void* hp, int nsteps) {
     remakeUniverse(s, box);
     assignKeys(s);
   }
+  return 0;
+}
+
+/* Subtree::startDual<GravityVisitor> on one subtree: accelerations (caller
+ * order) and the P2P pairs / P2C evaluations it made. */
+int ptref_dual(void* h, double* ax, double* ay, double* az, unsigned long long* pp_pc) {
+  RefSim& s = *(RefSim*)h;
+  buildTree(s);
+  for (auto& p : s.particles) {
+    p.acceleration = Vector3D<Real>(0.0);
+    p.potential = 0.0;
+  }
+  DualTrav t(s);
+  t.run();
+  for (auto& p : s.particles) {
+    ax[p.order] = p.acceleration.x;
+    ay[p.order] = p.acceleration.y;
+    az[p.order] = p.acceleration.z;
+  }
+  pp_pc[0] = t.pp;
+  pp_pc[1] = t.pc;
   return 0;
 }
 
