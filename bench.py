@@ -355,6 +355,27 @@ def sph_density_rate(a, sim, stream):
             "neighbours": 32, "note": "density pass of the SPH example: tree build + kNN + density + D2H"}
 
 
+def sph_pressure_rate(a, sim, stream):
+    """The SPH example's pressure pass after its density pass (ForceFn +
+    doSPHCalc with the opposing reactions): particles/s through
+    pt_sph_pressure (density pass, H2D of u, pressure kernel, D2H of density,
+    accelerations and PdV), seeded internal energies."""
+    import torch
+    u = np.random.default_rng(17).uniform(0.5, 1.5, a.n)
+    sim.sph_pressure(u)
+    ts = []
+    for _ in range(2):
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        sim.sph_pressure(u)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        ts.append(s0.elapsed_time(s1) / 1e3)
+    sim.start_down()
+    return {"particles_per_s": a.n / float(np.mean(ts)), "ms_per_pass": 1e3 * float(np.mean(ts)),
+            "neighbours": 32, "note": "density pass + pressure pass of the SPH example, host in and out"}
+
+
 def phase_rooflines(c, n, peaks):
     """HBM roofline of the bandwidth-bound phases of the last pass: their
     algorithmic bytes (keys 36 B/particle; sort 8 + 8 x 24 B and permute of
@@ -463,6 +484,7 @@ def extras(a, sim, p, world, rank, stream, value, shard=None):
     v_other = n / float(np.mean(t64))
     res["theta_sweep"] = theta_sweep(a, sim, tgt, (dax, day, daz), stream) if a.sweep else []
     res["sph_density"] = sph_density_rate(a, sim, stream)
+    res["sph_pressure"] = sph_pressure_rate(a, sim, stream)
     res["precision_comparison"] = {
         f"{a.precision}_force_evals_per_s": value, f"{other}_force_evals_per_s": v_other,
         "ratio_mixed_over_fp64": (value / v_other) if a.precision == "mixed" else (v_other / value),

@@ -160,6 +160,29 @@ class Gravity {
           "pt_get_state");
   }
 
+  // The SPH example's traversalFn (examples/SPH.C:74-101) on these
+  // particles: startUpAndDown<DensityVisitor> + DensityFn (density, ball^2),
+  // and with internal energies u also startDown<PressureVisitor> + ForceFn +
+  // the opposing effects (pressure accelerations, PdV work).
+  struct Sph {
+    std::vector<double> density, ball_sq, ax, ay, az, pdv;
+  };
+  Sph sph_density() {
+    Sph s;
+    s.density.assign(n_, 0.0);
+    s.ball_sq.assign(n_, 0.0);
+    check(pt_sph_density(h_, s.density.data(), s.ball_sq.data(), nullptr, nullptr), "pt_sph_density");
+    return s;
+  }
+  Sph sph_pressure(const std::vector<double>& u) {
+    if (u.size() != n_) throw Error(PT_E_ARG, "one internal energy per particle");
+    Sph s;
+    for (auto* v : {&s.density, &s.ax, &s.ay, &s.az, &s.pdv}) v->assign(n_, 0.0);
+    check(pt_sph_pressure(h_, u.data(), s.density.data(), s.ax.data(), s.ay.data(), s.az.data(), s.pdv.data()),
+          "pt_sph_pressure");
+    return s;
+  }
+
   pt_counters counters() const {
     pt_counters c;
     check(pt_get_counters(h_, &c), "pt_get_counters");

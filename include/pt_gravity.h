@@ -245,6 +245,20 @@ int pt_chain_grad(pt_handle* h, int nsteps, double dt, int ckpt_every, const dou
  * by (d2, index), and their d2. */
 int pt_sph_density(pt_handle* h, double* density, double* ball_sq, int32_t* nbr, double* nbr_d2);
 
+/* SPH pressure ---------------------------------------------------------------
+ * The pressure pass of the SPH example after its density pass
+ * (examples/SPH.C:87-101): startDown<PressureVisitor>, then ForceFn
+ * (examples/SPH.C:39-64) with doSPHCalc (examples/SPHUtils.h:64-133; visc = 0,
+ * aFac = vFac = 1, H = 0, gamma = 5/3) over each particle's 32 neighbours from
+ * pt_sph_density's pass (run here first on the current positions), then the
+ * opposite reactions (applyAccumulatedOpposingEffects).  u: internal energy
+ * per particle (u_predicted; velocity_predicted = the handle's velocities).
+ * Outputs: pressure accelerations and PdV work; density optional.  FP64; the
+ * reactions are summed by atomic adds, so their order (the last bits) is not
+ * fixed.  Caller order; any output may be NULL. */
+int pt_sph_pressure(pt_handle* h, const double* u, double* density, double* ax, double* ay, double* az,
+                    double* pdv);
+
 /* FP64 direct sum (the force-error yardstick) ------------------------------
  * Isolated spline-softened sum over all particles for nt caller indices,
  * the kernel of examples/GravityVisitor.h:87-120 with twoh = soft_i + soft_j. */

@@ -70,6 +70,7 @@ def _port_lib():
         lib.pto_run.argtypes = [C.c_void_p, C.c_int]
         lib.pto_direct.argtypes = [C.c_int] + [_dp] * 5 + [C.c_int, _i32p] + [_dp] * 4 + [C.c_int]
         lib.pto_sph_density.argtypes = [C.c_int] + [_dp] * 4 + [C.c_int, C.c_int, _dp, _dp, _i32p, _dp]
+        lib.pto_sph_pressure.argtypes = [C.c_int] + [_dp] * 10 + [_i32p, _dp, C.c_int] + [_dp] * 4
         lib.pto_set_periodic.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_double, C.c_double]
         lib.pto_set_traversal.argtypes = [C.c_void_p, C.c_int]
         lib.pto_ewald_direct.argtypes = [C.c_int] + [_dp] * 5 + [C.c_double, C.c_int, _i32p] + [_dp] * 4 + [C.c_int]
@@ -89,6 +90,7 @@ def _ref_lib():
         lib.ptref_set_periodic.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int]
         lib.ptref_set_traversal.argtypes = [C.c_void_p, C.c_int]
         lib.ptref_dual.argtypes = [C.c_void_p, _dp, _dp, _dp, _u64p]
+        lib.ptref_sph_pressure.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, _dp]
         lib.ptref_sph_density.argtypes = [C.c_void_p, _dp, _dp, _i32p, _dp]
         _ref = lib
     return _ref
@@ -244,6 +246,13 @@ class RefSim(_Sim):
         self._lib.ptref_sph_density(self._h, d, b, nbr, nd2)
         return d, b, nbr.reshape(n, k), nd2.reshape(n, k)
 
+    def sph_pressure(self, u):
+        """The reference's PressureVisitor + ForceFn + doSPHCalc after
+        sph_density(): pressure accelerations and PdV work (caller order)."""
+        out = [np.zeros(self.n) for _ in range(4)]
+        self._lib.ptref_sph_pressure(self._h, np.ascontiguousarray(u, dtype=np.float64), *out)
+        return out
+
     def forces(self, record_lists=False):
         self._lib.ptref_set_record_lists(self._h, 1 if record_lists else 0)
         self._lib.ptref_run(self._h, 0)
@@ -294,6 +303,19 @@ def sph_density(p: dict, k: int = 32, threads: int = 1):
     nbr = np.zeros(n * k, np.int32)
     lib.pto_sph_density(n, a[0], a[1], a[2], a[6], k, threads, d, b, nbr, nd2)
     return d, b, nbr.reshape(n, k), nd2.reshape(n, k)
+
+
+def sph_pressure(p: dict, u, density, ballsq, nbr, nd2):
+    """The SPH pressure pass (C restatement) after sph_density(): pressure
+    accelerations and PdV work with the opposite reactions added."""
+    lib = _port_lib()
+    n, k = p["x"].size, nbr.shape[1]
+    a = _arrs(p)
+    out = [np.zeros(n) for _ in range(4)]
+    lib.pto_sph_pressure(n, a[0], a[1], a[2], a[3], a[4], a[5], a[6], np.ascontiguousarray(u, dtype=np.float64),
+                         np.ascontiguousarray(density), np.ascontiguousarray(ballsq),
+                         np.ascontiguousarray(nbr, dtype=np.int32).ravel(), np.ascontiguousarray(nd2).ravel(), k, *out)
+    return out
 
 
 def sort_tree(t: Tree) -> Tree:

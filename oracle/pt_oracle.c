@@ -24,6 +24,9 @@
 #ifndef M_PI
 #define M_PI 3.14159265358979323846
 #endif
+#ifndef M_1_PI
+#define M_1_PI 0.31830988618379067154
+#endif
 
 typedef struct {
   double mass, cm[3], soft, radius;
@@ -1127,4 +1130,85 @@ void pto_sph_density(int n, const double* x, const double* y, const double* z, c
       nd2[(size_t)i * k + q] = q < cnt ? bd[q] : -1.0;
     }
   }
+}
+
+/* dkernelM4 (examples/SPHUtils.h:40-49): scaled gradient of the M4 kernel. */
+static double dkernel_m4(double ar2) {
+  double adk = sqrt(ar2);
+  if (ar2 < 1.0) adk = -3 + 2.25 * adk;
+  else adk = -0.75 * (2.0 - adk) * (2.0 - adk) / adk;
+  return adk;
+}
+
+/* The SPH example's pressure pass after pto_sph_density (examples/SPH.C:39-64
+ * ForceFn and :87-101; doSPHCalc examples/SPHUtils.h:64-133 with visc = 0,
+ * aFac = vFac = 1, H = 0, gammam1 = 2/3): every neighbour within the ball
+ * (the k nearest; nbr from pto_sph_density, in that order), the divv
+ * corrector, then per neighbour the particle's pressure acceleration and PdV
+ * work and the opposite reaction on the neighbour, added after the pass.
+ * v*: velocities (= velocity_predicted), u: internal energy (= u_predicted). */
+void pto_sph_pressure(int n, const double* x, const double* y, const double* z, const double* vx,
+                      const double* vy, const double* vz, const double* m, const double* u, const double* density,
+                      const double* ballsq, const int* nbr, const double* nd2, int k, double* ax, double* ay,
+                      double* az, double* pdv) {
+  const double gammam1 = 5.0 / 3.0 - 1.;
+  double* oa = (double*)calloc(4 * (size_t)n, sizeof(double));
+  for (int i = 0; i < n; i++) {
+    const double rsq = ballsq[i], fBall = sqrt(rsq), ih2 = 4.0 / rsq;
+    double divvi = 0, divvj = 0;
+    for (int e = 0; e < k; e++) {
+      const int q = nbr[(size_t)i * k + e];
+      if (q < 0) break;
+      const double fDist2 = nd2[(size_t)i * k + e];
+      double rs1 = dkernel_m4(fDist2 * ih2);
+      rs1 *= fDist2 * m[q];
+      divvi += rs1;
+      divvj += rs1 / density[q];
+    }
+    divvi /= density[i];
+    const double corr = (divvj != 0.0 ? divvi / divvj : 1.0);
+    double sax = 0.0, say = 0.0, saz = 0.0, spdv = 0.0;
+    for (int e = 0; e < k; e++) {
+      const int q = nbr[(size_t)i * k + e];
+      if (q < 0) break;
+      const double ph = 0.5 * fBall, ih2b = 4. / (fBall * fBall);
+      const double fNorm1 = 0.5 * M_1_PI * ih2b * ih2b / ph;
+      const double dx = x[q] - x[i], dy = y[q] - y[i], dz = z[q] - z[i];
+      const double fDist2 = dx * dx + dy * dy + dz * dz;
+      double rs1 = dkernel_m4(fDist2 * ih2b);
+      rs1 *= fNorm1;
+      rs1 *= corr;
+      const double aR = rs1 * m[i], bR = rs1 * m[q];
+      const double dvx = vx[q] - vx[i], dvy = vy[q] - vy[i], dvz = vz[q] - vz[i];
+      const double dvdotdr = 1.0 * (dvx * dx + dvy * dy + dvz * dz) + fDist2 * 0.0;
+      const double aP = u[i] * gammam1 / density[q], bP = u[q] * gammam1 / density[i];
+      const double visc = 0.0;
+      double PdV = bR * 0.5 * visc * dvdotdr;
+      PdV += bR * aP * dvdotdr;
+      spdv += PdV;
+      const double acc = (aP + bP) + visc;
+      const double s = acc * bR;
+      sax += s * dx;
+      say += s * dy;
+      saz += s * dz;
+      PdV = aR * 0.5 * visc * dvdotdr;
+      PdV += aR * aP * dvdotdr;
+      const double so = -acc * aR;
+      oa[4 * (size_t)q + 0] += so * dx;
+      oa[4 * (size_t)q + 1] += so * dy;
+      oa[4 * (size_t)q + 2] += so * dz;
+      oa[4 * (size_t)q + 3] += PdV;
+    }
+    ax[i] = sax;
+    ay[i] = say;
+    az[i] = saz;
+    pdv[i] = spdv;
+  }
+  for (int i = 0; i < n; i++) {
+    ax[i] += oa[4 * (size_t)i + 0];
+    ay[i] += oa[4 * (size_t)i + 1];
+    az[i] += oa[4 * (size_t)i + 2];
+    pdv[i] += oa[4 * (size_t)i + 3];
+  }
+  free(oa);
 }

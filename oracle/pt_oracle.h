@@ -63,6 +63,14 @@ void pto_ewald_direct(int n, const double* x, const double* y, const double* z, 
 void pto_sph_density(int n, const double* x, const double* y, const double* z, const double* m, int k,
                      int threads, double* density, double* ballsq, int* nbr, double* nd2);
 
+/* The SPH example's pressure pass after pto_sph_density: pressure
+ * accelerations and PdV work with the opposite reactions added; see
+ * pt_oracle.c. */
+void pto_sph_pressure(int n, const double* x, const double* y, const double* z, const double* vx,
+                      const double* vy, const double* vz, const double* m, const double* u, const double* density,
+                      const double* ballsq, const int* nbr, const double* nd2, int k, double* ax, double* ay,
+                      double* az, double* pdv);
+
 /* FP64 direct sum (spline softening, twoh = soft_i + soft_j, G = 1) over
  * all n sources for nt target indices; isolated (no periodic images). */
 void pto_direct(int n, const double* x, const double* y, const double* z, const double* m,

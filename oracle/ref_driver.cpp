@@ -89,6 +89,7 @@ class ThreadStateHolder {
   }
 };
 #include "DensityVisitor.h"
+#include "PressureVisitor.h"
 #include "SPHUtils.h"
 
 namespace {
@@ -492,6 +493,11 @@ void sph_density(RefSim& s, double* density, double* ballsq, int* nbr, double* n
       dens /= (0.125 * M_PI * r_cubed);
       density[part.order] = dens;
       ballsq[part.order] = rsq;
+      auto copy_part = part;  // SPH.C:30-34
+      copy_part.density = dens;
+      leaf.changeParticle(pi, copy_part);
+      leaf.data.pps[pi].sphBallSq = rsq;
+      leaf.data.max_rad = std::max(leaf.data.max_rad, fBall);
       std::vector<std::pair<double, int>> q;
       for (auto& e : Q) q.push_back({e.fKey, e.pPtr->order});
       std::sort(q.begin(), q.end());
@@ -499,7 +505,74 @@ void sph_density(RefSim& s, double* density, double* ballsq, int* nbr, double* n
         nbr[(size_t)part.order * kmax + i] = i < (int)q.size() ? q[i].second : -1;
         nd2[(size_t)part.order * kmax + i] = i < (int)q.size() ? q[i].first : -1.0;
       }
+      Q.clear();
     }
+  }
+}
+
+// The pressure half of examples/SPH.C:traversalFn (:87-101): startDown with the
+// reference's PressureVisitor (its gather of every neighbour within the ball),
+// ForceFn (SPH.C:39-64: the divv corrector, then the reference's doSPHCalc per
+// neighbour, examples/SPHUtils.h:64-133), and the opposing effects applied
+// afterwards.  Needs sph_density first.  u: internal energy (caller order),
+// used as u_predicted; velocity_predicted = velocity.  Outputs in caller order.
+void sph_pressure(RefSim& s, const double* u, double* ax, double* ay, double* az, double* pdv) {
+  const size_t n = s.particles.size(), nb = s.leaves.size();
+  for (auto& p : s.particles) {
+    p.u = p.u_predicted = u[p.order];
+    p.velocity_predicted = p.velocity;
+    p.acceleration = Vector3D<Real>(0.0);
+    p.pressure_dVolume = 0.0;
+  }
+  for (size_t b = 0; b < nb; b++) {  // transposed down traversal, pre-order per bucket
+    PressureVisitor v;
+    RNode* bucket = s.leaves[b];
+    std::vector<RNode*> st{s.root};
+    while (!st.empty()) {
+      RNode* node = st.back();
+      st.pop_back();
+      if (node->type == RNode::Type::Leaf) {
+        v.leaf(*node, *bucket);
+      } else if (node->type == RNode::Type::Internal) {
+        if (v.open(*node, *bucket)) {
+          for (int i = node->n_children - 1; i >= 0; i--) st.push_back(node->getChild(i));
+        } else {
+          v.node(*node, *bucket);
+        }
+      }
+    }
+  }
+  ThreadStateHolder tls;
+  tls.acc.assign(n, Vector3D<Real>(0.0));
+  tls.work.assign(n, 0.0);
+  for (size_t b = 0; b < nb; b++) {  // ForceFn
+    auto& leaf = *s.leaves[b];
+    for (int pi = 0; pi < leaf.n_particles; pi++) {
+      auto& part = leaf.particles()[pi];
+      auto& Q = leaf.data.pps[pi].neighbors;
+      auto rsq = leaf.data.pps[pi].sphBallSq, fBall = std::sqrt(rsq);
+      auto ih2 = 4.0 / rsq;
+      double divvi = 0, divvj = 0;
+      for (int i = 0; i < (int)Q.size(); i++) {
+        auto& fDist2 = Q[i].fKey;
+        auto r2 = fDist2 * ih2;
+        Real rs1 = paratreet::dkernelM4(r2);
+        auto& q = *(Q[i].pPtr);
+        rs1 *= fDist2 * q.mass;
+        divvi += rs1;
+        divvj += rs1 / q.density;
+      }
+      divvi /= part.density;
+      auto corr = (divvj != 0.0 ? divvi / divvj : 1.0);
+      for (int i = 0; i < (int)Q.size(); i++) paratreet::doSPHCalc(leaf, pi, fBall, &tls, *Q[i].pPtr, corr);
+      Q.clear();
+    }
+  }
+  for (auto& p : s.particles) {  // applyAccumulatedOpposingEffects
+    ax[p.order] = p.acceleration.x + tls.acc[p.order].x;
+    ay[p.order] = p.acceleration.y + tls.acc[p.order].y;
+    az[p.order] = p.acceleration.z + tls.acc[p.order].z;
+    pdv[p.order] = p.pressure_dVolume + tls.work[p.order];
   }
 }
 
@@ -683,6 +756,12 @@ int ptref_dual(void* h, double* ax, double* ay, double* az, unsigned long long* 
 
 /* 1: Partition::startBasicDown (breadth first per bucket), 0: startDown. */
 void ptref_set_traversal(void* h, int basic_down) { ((RefSim*)h)->basic_down = basic_down; }
+
+/* SPH pressure pass after ptref_sph_density (same particles). */
+int ptref_sph_pressure(void* h, const double* u, double* ax, double* ay, double* az, double* pdv) {
+  sph_pressure(*(RefSim*)h, u, ax, ay, az, pdv);
+  return 0;
+}
 
 /* SPH density of the reference's SPH example (k = 32 neighbours). */
 int ptref_sph_density(void* h, double* density, double* ballsq, int* nbr, double* nd2) {

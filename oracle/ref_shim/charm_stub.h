@@ -15,9 +15,11 @@
 #include <limits>
 #include <functional>
 #include <iostream>
+#include <cinttypes>
 
 #define CkAssert(x) assert(x)
 #define CkAbort(msg) (std::fprintf(stderr, "%s\n", msg), std::abort())
+#define CkPrintf(...) std::fprintf(stderr, __VA_ARGS__)
 
 namespace PUP {
 class er {

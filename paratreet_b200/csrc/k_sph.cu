@@ -14,6 +14,14 @@
 // (DensityVisitor::open with Space::intersect's <=), so balls that shrank
 // since the push prune more; children are pushed far to near (distance of
 // their boxes to the bucket's centre) so the nearest subtree is searched first.
+//
+// The pressure pass that follows (sph_pressure_kernel) restates ForceFn
+// (examples/SPH.C:39-64) and doSPHCalc (examples/SPHUtils.h:64-133): one warp
+// per particle, lane e = its e-th neighbour from the density pass.  The divv
+// corrector and the particle's own pressure acceleration and PdV work are warp
+// sums; the opposite reaction on each neighbour (ThreadStateHolder's opposing
+// effects, applied after the pass in the reference) is an FP64 atomic add, so
+// its summation order is not fixed.
 #include "pt_internal.cuh"
 #include "pt_walk.cuh"
 
@@ -204,7 +212,110 @@ __global__ void __launch_bounds__(kSphWarps * 32) sph_density_kernel(Particles p
   }
 }
 
+// dkernelM4 (examples/SPHUtils.h:40-49), scaled: (pi h^5 / |dx|^2) dx.gradW.
+__device__ __forceinline__ double dkernel_m4(double ar2) {
+  double adk = sqrt(ar2);
+  if (ar2 < 1.0) adk = -3 + 2.25 * adk;
+  else adk = -0.75 * (2.0 - adk) * (2.0 - adk) / adk;
+  return adk;
+}
+
+__device__ __forceinline__ double warp_sum_f64(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+static_assert(kSphK == 32, "the pressure pass maps one neighbour to one lane");
+
+// visc = 0, aFac = vFac = 1, H = 0 as in doSPHCalc; u and the outputs in
+// sorted order; the outputs start at zero.
+__global__ void __launch_bounds__(256) sph_pressure_kernel(Particles p, const double* __restrict__ density,
+                                                           const double* __restrict__ ballsq,
+                                                           const double* __restrict__ u,
+                                                           const int32_t* __restrict__ nbr,
+                                                           const double* __restrict__ nd2, int64_t n,
+                                                           double* __restrict__ ax, double* __restrict__ ay,
+                                                           double* __restrict__ az, double* __restrict__ pdv,
+                                                           unsigned* status) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const double gammam1 = 5.0 / 3.0 - 1.;
+  for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+    const int32_t q = nbr[i * kSphK + lane];
+    const double fd2 = nd2[i * kSphK + lane];
+    const bool bad = q >= n;
+    if (__any_sync(kFull, bad) && lane == 0) atomicOr(status, kErrCapacity);
+    const bool live = q >= 0 && !bad;
+    const double rsq = ballsq[i], fBall = sqrt(rsq), ih2 = 4.0 / rsq;
+    const double rhoi = density[i];
+    double rhoq = 1.0, mq = 0.0, divvi = 0.0, divvj = 0.0;
+    if (live) {
+      rhoq = density[q];
+      mq = p.m[q];
+      double rs1 = dkernel_m4(fd2 * ih2);
+      rs1 *= fd2 * mq;
+      divvi = rs1;
+      divvj = rs1 / rhoq;
+    }
+    divvi = warp_sum_f64(divvi);
+    divvj = warp_sum_f64(divvj);
+    divvi /= rhoi;
+    const double corr = (divvj != 0.0 ? divvi / divvj : 1.0);
+    double sax = 0.0, say = 0.0, saz = 0.0, spdv = 0.0;
+    if (live) {
+      const double xi = p.x[i], yi = p.y[i], zi = p.z[i];
+      const double ph = 0.5 * fBall, ih2b = 4. / (fBall * fBall);
+      const double fNorm1 = 0.5 * M_1_PI * ih2b * ih2b / ph;
+      const double dx = p.x[q] - xi, dy = p.y[q] - yi, dz = p.z[q] - zi;
+      const double fDist2 = dx * dx + dy * dy + dz * dz;
+      double rs1 = dkernel_m4(fDist2 * ih2b);
+      rs1 *= fNorm1;
+      rs1 *= corr;
+      const double aR = rs1 * p.m[i], bR = rs1 * mq;
+      const double dvx = p.vx[q] - p.vx[i], dvy = p.vy[q] - p.vy[i], dvz = p.vz[q] - p.vz[i];
+      const double dvdotdr = 1.0 * (dvx * dx + dvy * dy + dvz * dz) + fDist2 * 0.0;
+      const double aP = u[i] * gammam1 / rhoq, bP = u[q] * gammam1 / rhoi;
+      const double visc = 0.0;
+      double PdV = bR * 0.5 * visc * dvdotdr;
+      PdV += bR * aP * dvdotdr;
+      spdv = PdV;
+      const double acc = (aP + bP) + visc;
+      const double s = acc * bR;
+      sax = s * dx;
+      say = s * dy;
+      saz = s * dz;
+      if (q != i) {  // the particle's own entry has dx = 0 and adds nothing
+        PdV = aR * 0.5 * visc * dvdotdr;
+        PdV += aR * aP * dvdotdr;
+        const double so = -acc * aR;
+        atomicAdd(ax + q, so * dx);
+        atomicAdd(ay + q, so * dy);
+        atomicAdd(az + q, so * dz);
+        atomicAdd(pdv + q, PdV);
+      }
+    }
+    sax = warp_sum_f64(sax);
+    say = warp_sum_f64(say);
+    saz = warp_sum_f64(saz);
+    spdv = warp_sum_f64(spdv);
+    if (lane == 0) {
+      atomicAdd(ax + i, sax);
+      atomicAdd(ay + i, say);
+      atomicAdd(az + i, saz);
+      atomicAdd(pdv + i, spdv);
+    }
+  }
+}
+
 int sph_k() { return kSphK; }
+
+void launch_sph_pressure(Particles p, const double* density, const double* ballsq, const double* u,
+                         const int32_t* nbr, const double* nd2, int64_t n, double* ax, double* ay, double* az,
+                         double* pdv, unsigned* status, int grid, cudaStream_t st) {
+  note_launch();
+  sph_pressure_kernel<<<grid, 256, 0, st>>>(p, density, ballsq, u, nbr, nd2, n, ax, ay, az, pdv, status);
+}
 
 void launch_sph_density(Particles p, const Mom* mom, const WalkRec* walk, const int32_t* buckets, int64_t nbuckets,
                         int64_t nnodes, double* density, double* ballsq, int32_t* nbr, double* nd2, unsigned* work,

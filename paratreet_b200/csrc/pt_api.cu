@@ -450,11 +450,23 @@ int run_two_phase(pt_handle* h, TravParams& P) {
     const unsigned long long need_pp =
         std::max<unsigned long long>(h->want_pp ? h->want_pp + slack : 0, 256ull * nb + slack);
     if (need_pc > h->cap_pc || need_pp > h->cap_pp) {
+      // a quarter of headroom, so that the pass-to-pass variation of the
+      // reserved regions does not free and map the multi-GB pools again
+      // (which costs more than a whole pass); without room for it, the bare need
       dfree(h->pool_pc);
       dfree(h->pool_pp);
       h->cap_pc = h->cap_pp = 0;
-      if (cudaMalloc((void**)&h->pool_pc, need_pc * sizeof(int32_t)) != cudaSuccess ||
-          cudaMalloc((void**)&h->pool_pp, need_pp * sizeof(int32_t)) != cudaSuccess) {
+      unsigned long long alloc_pc = need_pc + need_pc / 4, alloc_pp = need_pp + need_pp / 4;
+      if (cudaMalloc((void**)&h->pool_pc, alloc_pc * sizeof(int32_t)) != cudaSuccess ||
+          cudaMalloc((void**)&h->pool_pp, alloc_pp * sizeof(int32_t)) != cudaSuccess) {
+        cudaGetLastError();
+        dfree(h->pool_pc);
+        dfree(h->pool_pp);
+        alloc_pc = need_pc;
+        alloc_pp = need_pp;
+      }
+      if ((!h->pool_pc && cudaMalloc((void**)&h->pool_pc, need_pc * sizeof(int32_t)) != cudaSuccess) ||
+          (!h->pool_pp && cudaMalloc((void**)&h->pool_pp, need_pp * sizeof(int32_t)) != cudaSuccess)) {
         // no room for the lists: this handle evaluates with the fused kernel from now on
         cudaGetLastError();
         dfree(h->pool_pc);
@@ -465,8 +477,8 @@ int run_two_phase(pt_handle* h, TravParams& P) {
         CK(cudaGetLastError());
         return PT_OK;
       }
-      h->cap_pc = need_pc;
-      h->cap_pp = need_pp;
+      h->cap_pc = alloc_pc;
+      h->cap_pp = alloc_pp;
     }
     L.pc_pool = h->pool_pc;
     L.pp_pool = h->pool_pp;
@@ -873,14 +885,14 @@ int pt_device_accel(pt_handle* h, double** ax, double** ay, double** az, double*
   return PT_OK;
 }
 
-int pt_sph_density(pt_handle* h, double* density, double* ball_sq, int32_t* nbr, double* nbr_d2) {
-  if (!h || ((nbr == nullptr) != (nbr_d2 == nullptr))) return PT_E_ARG;
-  if (!h->p.x) return fail(h, PT_E_STATE, "no particles");
-  cudaSetDevice(h->cfg.device);
+// Density pass on a rebuilt tree; leaves density and ball^2 (sorted order) in
+// h->sph and, with want_nbr, the neighbour lists in h->sph_nbr / h->sph_nd2.
+// h->sph holds 7 N doubles: density, ball^2, and the pressure pass's u, ax,
+// ay, az, PdV.
+static int sph_density_device(pt_handle* h, bool want_nbr) {
   cudaStream_t st = h->stream;
   const int64_t n = h->n;
   const int k = sph_k();
-  if (n == 0) return PT_OK;
   CKR(keys_and_sort(h));
   CKR(build_tree(h));
   CKR(upward(h));
@@ -888,11 +900,10 @@ int pt_sph_density(pt_handle* h, double* density, double* ball_sq, int32_t* nbr,
   h->have_forces = false;
   h->forces_current = false;
   h->lists_valid = false;
-  if (2 * n > h->sph_cap) {
-    CKR(dalloc(h, &h->sph, 2 * n));
-    h->sph_cap = 2 * n;
+  if (7 * n > h->sph_cap) {
+    CKR(dalloc(h, &h->sph, 7 * n));
+    h->sph_cap = 7 * n;
   }
-  const bool want_nbr = nbr != nullptr;
   if (want_nbr && n * k > h->sph_nbr_cap) {
     CKR(dalloc(h, &h->sph_nbr, n * k));
     CKR(dalloc(h, &h->sph_nd2, n * k));
@@ -903,7 +914,19 @@ int pt_sph_density(pt_handle* h, double* density, double* ball_sq, int32_t* nbr,
                      want_nbr ? h->sph_nbr : nullptr, want_nbr ? h->sph_nd2 : nullptr, h->d_work, h->d_status,
                      h->sms * 16, st);
   CK(cudaGetLastError());
-  CKR(read_status(h));
+  return read_status(h);
+}
+
+int pt_sph_density(pt_handle* h, double* density, double* ball_sq, int32_t* nbr, double* nbr_d2) {
+  if (!h || ((nbr == nullptr) != (nbr_d2 == nullptr))) return PT_E_ARG;
+  if (!h->p.x) return fail(h, PT_E_STATE, "no particles");
+  cudaSetDevice(h->cfg.device);
+  cudaStream_t st = h->stream;
+  const int64_t n = h->n;
+  const int k = sph_k();
+  if (n == 0) return PT_OK;
+  const bool want_nbr = nbr != nullptr;
+  CKR(sph_density_device(h, want_nbr));
   CKR(unpermute_f64(h, h->sph, density));
   CK(cudaStreamSynchronize(st));
   CKR(unpermute_f64(h, h->sph + n, ball_sq));
@@ -930,6 +953,33 @@ int pt_sph_density(pt_handle* h, double* density, double* ball_sq, int32_t* nbr,
         nbr_d2[c * k + e] = e < m ? row[e].first : -1.0;
       }
     }
+  }
+  return PT_OK;
+}
+
+int pt_sph_pressure(pt_handle* h, const double* u, double* density, double* ax, double* ay, double* az,
+                    double* pdv) {
+  if (!h || !u) return PT_E_ARG;
+  if (!h->p.x) return fail(h, PT_E_STATE, "no particles");
+  cudaSetDevice(h->cfg.device);
+  cudaStream_t st = h->stream;
+  const int64_t n = h->n;
+  if (n == 0) return PT_OK;
+  CKR(sph_density_device(h, true));
+  double* us = h->sph + 2 * n;
+  double* out = h->sph + 3 * n;  // ax, ay, az, PdV
+  CK(cudaMemcpyAsync(h->tmp_d, u, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  launch_gather_by_order(h->tmp_d, us, h->p.order, n, grid_for(h, n), st);
+  CK(cudaMemsetAsync(out, 0, 4 * n * sizeof(double), st));
+  launch_sph_pressure(h->p, h->sph, h->sph + n, us, h->sph_nbr, h->sph_nd2, n, out, out + n, out + 2 * n,
+                      out + 3 * n, h->d_status, h->sms * 16, st);
+  CK(cudaGetLastError());
+  CKR(read_status(h));
+  double* dst[5] = {density, ax, ay, az, pdv};
+  const double* src[5] = {h->sph, out, out + n, out + 2 * n, out + 3 * n};
+  for (int i = 0; i < 5; i++) {
+    CKR(unpermute_f64(h, src[i], dst[i]));
+    CK(cudaStreamSynchronize(st));
   }
   return PT_OK;
 }

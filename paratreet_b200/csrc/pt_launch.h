@@ -76,6 +76,9 @@ void launch_eval_lists(const TravParams& P, const ListParams& L, const Mom* mom,
 
 // k_sph.cu
 int sph_k();
+void launch_sph_pressure(Particles p, const double* density, const double* ballsq, const double* u,
+                         const int32_t* nbr, const double* nd2, int64_t n, double* ax, double* ay, double* az,
+                         double* pdv, unsigned* status, int grid, cudaStream_t st);
 void launch_sph_density(Particles p, const Mom* mom, const WalkRec* walk, const int32_t* buckets, int64_t nbuckets,
                         int64_t nnodes, double* density, double* ballsq, int32_t* nbr, double* nd2, unsigned* work,
                         unsigned* status, int grid, cudaStream_t st);

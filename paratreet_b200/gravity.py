@@ -274,6 +274,18 @@ class GravitySimulation:
         self._check(self._lib.pt_sph_density(self._h, L.ptr(d), L.ptr(b), L.ptr(nbr), L.ptr(nd2)))
         return (d, b, nbr, nd2) if neighbors else (d, b)
 
+    def sph_pressure(self, u):
+        """Pressure pass of the SPH example (ForceFn + doSPHCalc after the
+        density pass): (density, ax, ay, az, pdv) per particle for internal
+        energies u."""
+        n = self.n
+        uu = np.ascontiguousarray(u, dtype=np.float64)
+        if uu.shape != (n,):
+            raise ValueError("u must hold one value per particle")
+        out = [np.empty(n) for _ in range(5)]
+        self._check(self._lib.pt_sph_pressure(self._h, L.ptr(uu), *[L.ptr(o) for o in out]))
+        return tuple(out)
+
     def direct_sum(self, targets):
         t = np.ascontiguousarray(targets, dtype=np.int32)
         out = [np.empty(t.size) for _ in range(4)]

@@ -6,6 +6,10 @@
 //                                                    one force pass, .acc output
 //   gravity_demo steps in.tipsy out.tipsy theta bucket dt n
 //                                                    n Driver::run iterations
+//   gravity_demo sph in.tipsy out.txt bucket         SPH density + pressure pass
+//                                                    (u = 1 + i mod 7 / 10), one
+//                                                    line per particle: density
+//                                                    ax ay az pdv
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -51,6 +55,20 @@ int main(int argc, char** argv) {
       g.run(std::atoi(argv[7]));
       g.state(p);
       write_tipsy(argv[3], p, h.time);
+      return 0;
+    }
+    if (mode == "sph") {
+      conf.max_particles_per_leaf = argc > 4 ? std::atoi(argv[4]) : 16;
+      Gravity g(conf);
+      g.load(p);
+      std::vector<double> u(p.size());
+      for (size_t i = 0; i < u.size(); i++) u[i] = 1.0 + (double)(i % 7) / 10.0;
+      const Gravity::Sph s = g.sph_pressure(u);
+      FILE* f = std::fopen(argv[3], "w");
+      if (!f) throw Error(PT_E_ARG, "cannot open output");
+      for (size_t i = 0; i < u.size(); i++)
+        std::fprintf(f, "%.17g %.17g %.17g %.17g %.17g\n", s.density[i], s.ax[i], s.ay[i], s.az[i], s.pdv[i]);
+      std::fclose(f);
       return 0;
     }
     std::fprintf(stderr, "unknown mode %s\n", mode.c_str());

@@ -31,6 +31,10 @@ sph_<case>.json
     examples/SPHUtils.h): digests of every particle's 32 neighbours (sorted
     by distance, then index), their d2 and the ball radii, and sampled
     densities (which depend on the heap's summation order in the last bits).
+    Then the pressure pass (PressureVisitor walk, ForceFn of examples/SPH.C,
+    doSPHCalc of examples/SPHUtils.h, the opposing effects added after it)
+    for seeded internal energies u: sampled pressure accelerations and PdV
+    work, and their L1 norms (summation order again decides the last bits).
 periodic_<case>.json
     The same sources in periodic mode (examples/Gravity.C replica walks plus
     the Ewald correction of examples/Ewald.{h,C}) on a displaced lattice:
@@ -181,6 +185,11 @@ def run_basic_case(name):
     print(name, p["x"].size)
 
 
+def sph_energies(n):
+    """The internal energies of the pressure goldens."""
+    return np.random.default_rng(17).uniform(0.5, 1.5, n)
+
+
 def run_sph_case(name):
     gen, kw, bucket = SPH_CASES[name]
     p = gen(**kw)
@@ -191,6 +200,18 @@ def run_sph_case(name):
         "case": name, "generator": gen.__name__, "kwargs": kw, "bucket": bucket,
         "sha256": {"nbr": digest(nbr.astype(np.int32)), "nbr_d2": digest(nd2), "ball_sq": digest(ball)},
         "samples": {"idx": idx, "density": [float(dens[i]) for i in idx]},
+    }
+    n = p["x"].size
+    u = sph_energies(n)
+    ax, ay, az, pdv = r.sph_pressure(u)
+    pidx = sorted(set(idx) | set(int(i) for i in np.random.default_rng(3).choice(n, 27, replace=False)))
+    out["pressure"] = {
+        "u": "numpy default_rng(17).uniform(0.5, 1.5, n)", "idx": pidx,
+        "ax": [float(ax[i]) for i in pidx], "ay": [float(ay[i]) for i in pidx],
+        "az": [float(az[i]) for i in pidx], "pdv": [float(pdv[i]) for i in pidx],
+        "l1": {k: float(np.abs(v).sum()) for k, v in (("ax", ax), ("ay", ay), ("az", az), ("pdv", pdv))},
+        "acc_scale": float(max(np.abs(ax).max(), np.abs(ay).max(), np.abs(az).max())),
+        "pdv_scale": float(np.abs(pdv).max()),
     }
     with open(os.path.join(OUT, f"sph_{name}.json"), "w") as f:
         json.dump(out, f, indent=1, sort_keys=True)

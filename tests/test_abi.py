@@ -74,6 +74,8 @@ def test_null_handle_calls_return_errors():
     assert lib.pt_compute_forces(None) == -1
     assert lib.pt_step(None, 1) == -1
     assert lib.pt_destroy(None) == 0
+    assert lib.pt_sph_density(None, None, None, None, None) == -1
+    assert lib.pt_sph_pressure(None, None, None, None, None, None, None) == -1
 
 
 def test_visitor_mirror():

@@ -96,3 +96,26 @@ def test_cpp_driver_steps_match_python(demo, tmp_path):
         st = s.state()
     for k in ("x", "y", "z", "vx", "vy", "vz"):
         assert np.array_equal(got[k], st[k]), k
+
+
+@pytest.mark.gpu
+def test_cpp_sph_pressure_matches_python(demo, tmp_path):
+    """Gravity::sph_pressure (the SPH example's traversalFn) from C++ against
+    the same pass through the Python binding: densities to 1e-13, pressure
+    accelerations and PdV to 1e-12 of the largest value (atomic summation
+    order of the reactions)."""
+    from paratreet_b200.gravity import GravitySimulation
+    p = ics.plummer(5000, seed=6, soft=0.02)
+    f, out = str(tmp_path / "g.tipsy"), str(tmp_path / "sph.txt")
+    tipsy.write_tipsy(f, p, softening=True)
+    q, _ = tipsy.read_tipsy(f)
+    r = subprocess.run([demo, "sph", f, out, "16"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = np.loadtxt(out).T
+    u = 1.0 + (np.arange(q["x"].size) % 7) / 10.0
+    with GravitySimulation(max_particles_per_leaf=16) as s:
+        s.set_particles(q)
+        want = s.sph_pressure(u)
+    assert np.allclose(got[0], want[0], rtol=1e-13, atol=0)
+    for g, w in zip(got[1:], want[1:]):
+        assert np.abs(g - w).max() <= 1e-12 * max(np.abs(w).max(), 1e-300)
