@@ -298,7 +298,8 @@ def main():
                                f"{sm_max:.0f} MHz (no measured FP32/FP64 figure in MEASURED_PEAKS.json)"}
 
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
-           "warmup": a.warmup, "ms_per_step": t * 1e3 / a.steps, "higher_is_better": True,
+           "warmup": a.warmup, "ms_per_step": t * 1e3 / a.steps,
+           "step_ms": [round(x, 3) for x in step_ms], "higher_is_better": True,
            "scaling": "strong", "vs_baseline": None, "dtype": "f32 interactions / f64 tree"
            if a.precision == "mixed" else "f64", "data": "synthetic (seeded Plummer sphere)",
            "config": workload_config(a, world), "gpu_launches": launches,
