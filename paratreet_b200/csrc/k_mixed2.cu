@@ -114,13 +114,14 @@ __global__ void __launch_bounds__(kWlWarps * 32, 8) walk_lists(TravParams P, Lis
         node = w.stack[pop + e] + c;
       }
       int cls = kClsNone;
+      double gap2 = -1.0;
       WalkRec r;
       if (node >= 0) {
         if (node >= P.nnodes) {
           atomicOr(P.status, kErrCapacity);
         } else {
           r = P.walk[node];
-          cls = classify_node(r, g, P.ox, P.oy, P.oz);
+          cls = classify_node_gap(r, g, P.ox, P.oy, P.oz, gap2);
         }
       }
       opens += (unsigned long long)__popc(__ballot_sync(kFull, node >= 0 && node < P.nnodes &&
@@ -128,11 +129,14 @@ __global__ void __launch_bounds__(kWlWarps * 32, 8) walk_lists(TravParams P, Lis
       bool near = false;
       if (cls == kClsP2P || cls == kClsQuad) {
         // P2P: a pair may be softened; P2C: a target may be inside twoh of
-        // the centre (SPLINEQ's softened branch), with a relative margin
-        const double cx = r.cm[0] + P.ox, cy = r.cm[1] + P.oy, cz = r.cm[2] + P.oz;
+        // the centre (SPLINEQ's softened branch), with a relative margin.  A
+        // quadrupole node's box gap is the one its opening test measured.
+        if (cls == kClsP2P)
+          gap2 = box_gap2_exact(g.lo, g.hi, __dadd_rn(r.cm[0], P.ox), __dadd_rn(r.cm[1], P.oy),
+                                __dadd_rn(r.cm[2], P.oz));
         const double reach = (cls == kClsP2P) ? r.reach + r.soft_max + g.soft_max
                                               : (r.soft + g.soft_max) * (1.0 + 1e-5);
-        near = !(box_dist2(g.lo, g.hi, cx, cy, cz) > reach * reach);
+        near = !(gap2 > reach * reach);
       }
       {
         const bool pc = (cls == kClsQuad || cls == kClsMono);
@@ -209,13 +213,14 @@ constexpr int kEvWarps = 4;
 struct EvalWarp {
   BucketGeom geom;
   float4 st[6][32];            // staged pairs: P2C six rows; P2P px, pz, pr
-  int32_t pre[kWlBuf + 1];     // P2P: prefix of leaf sizes in a leaf block
-  int32_t ps0[kWlBuf];         // P2P: first particle of each leaf
+  int32_t ps0[kWlBuf];         // P2P: first particle of each leaf - its stream position
   float4 lof[kWlBuf];          // P2P: leaf offsets cm_leaf - cm_bucket (FP32)
   int32_t lsel[kWlBuf];        // P2P: leaves of the current kind in a block
 };
 
-// Per-lane target of a 32-target chunk, replicated over G lane groups.
+// Per-lane target of a 32-target chunk, replicated over G lane groups (lanes
+// past G * nt idle: a warp's loop runs as long as its target with the fewest
+// lanes, so a ragged split would not finish sooner).
 struct EvTarget {
   int t, grp, G, nt;
   float tx, ty, tz, ts;
@@ -333,6 +338,64 @@ __device__ __noinline__ float4 ev_p2c_pair_scalar(const EvalWarp& w, int k, floa
   return make_float4(ax, ay, az, pf);
 }
 
+// The staged node pairs k = grp, grp + G, ... of one chunk against this
+// lane's target (GravityVisitor::node, examples/GravityVisitor.h:184-224, in
+// packed FP32).  With kNear, pairs holding a near node take the scalar path.
+template <bool kNear>
+__device__ __forceinline__ void ev_p2c_pairs(const EvalWarp& w, const EvTarget& x, int npair, float2 ntx, float2 nty,
+                                             float2 ntz, float2& ax2, float2& ay2, float2& az2, float2& pp2,
+                                             float2& mm2) {
+  const float2 mthree = make_float2(-3.f, -3.f), mfive = make_float2(-5.f, -5.f), half = make_float2(0.5f, 0.5f);
+  const float4* sp = &w.st[0][x.grp];  // rows st[1..5] follow at +32 each
+  for (int k = x.grp; k < npair; k += x.G, sp += x.G) {
+    const float4 P5 = sp[160];
+    if (kNear && (__float_as_int(P5.x) | __float_as_int(P5.y)) < 0) {  // a near node: scalar, softening tested
+      const float4 v = ev_p2c_pair_scalar(w, k, x.tx, x.ty, x.tz, x.ts);
+      ax2.x += v.x;
+      ay2.x += v.y;
+      az2.x += v.z;
+      pp2.x += v.w;
+      continue;
+    }
+    const float4 P0 = sp[0], P1 = sp[32];
+    const float2 rx = __fadd2_rn(make_float2(P0.x, P0.y), ntx);  // r' = o - t = -r
+    const float2 ry = __fadd2_rn(make_float2(P0.z, P0.w), nty);
+    const float2 rz = __fadd2_rn(make_float2(P1.x, P1.y), ntz);
+    float2 r2 = __fmul2_rn(rx, rx);
+    r2 = __ffma2_rn(ry, ry, r2);
+    r2 = __ffma2_rn(rz, rz, r2);
+    const float4 P2 = sp[64], P3 = sp[96], P4 = sp[128];
+    const float2 a = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+    const float2 d2 = __fmul2_rn(a, a);
+    const float2 bb = __fmul2_rn(a, d2);                       // b = 1/r^3
+    const float2 nc = __fmul2_rn(__fmul2_rn(bb, d2), mthree);  // -c = -3/r^5
+    const float2 d = __fmul2_rn(__fmul2_rn(nc, d2), mfive);    // d = 15/r^7
+    const float2 xx = make_float2(P2.x, P2.y), xy = make_float2(P2.z, P2.w);
+    const float2 xz = make_float2(P3.x, P3.y), yy = make_float2(P3.z, P3.w);
+    const float2 yz = make_float2(P4.x, P4.y), zz = make_float2(P4.z, P4.w);
+    const float2 qx = __ffma2_rn(xz, rz, __ffma2_rn(xy, ry, __fmul2_rn(xx, rx)));  // q' = -q
+    const float2 qy = __ffma2_rn(yz, rz, __ffma2_rn(yy, ry, __fmul2_rn(xy, rx)));
+    const float2 qz = __ffma2_rn(zz, rz, __ffma2_rn(yz, ry, __fmul2_rn(xz, rx)));
+    const float2 qir = __fmul2_rn(half, __ffma2_rn(qz, rz, __ffma2_rn(qy, ry, __fmul2_rn(qx, rx))));
+    const float2 M = make_float2(P1.z, P1.w), tr = make_float2(P5.x, P5.y);
+    // qir3 = b M + d qir - c tr; acc += qir3 r' - c q'; pot += b tr - c qir - M a
+    const float2 qir3 = __ffma2_rn(nc, tr, __ffma2_rn(d, qir, __fmul2_rn(bb, M)));
+    ax2 = __ffma2_rn(nc, qx, __ffma2_rn(qir3, rx, ax2));
+    ay2 = __ffma2_rn(nc, qy, __ffma2_rn(qir3, ry, ay2));
+    az2 = __ffma2_rn(nc, qz, __ffma2_rn(qir3, rz, az2));
+    pp2 = __ffma2_rn(nc, qir, __ffma2_rn(bb, tr, pp2));
+    mm2 = __ffma2_rn(M, a, mm2);
+  }
+}
+
+// The rare chunks with a near node, out of line so that the common loop keeps
+// its registers.
+__device__ __noinline__ void ev_p2c_pairs_near(const EvalWarp& w, const EvTarget& x, int npair, float2 ntx,
+                                               float2 nty, float2 ntz, float2& ax2, float2& ay2, float2& az2,
+                                               float2& pp2, float2& mm2) {
+  ev_p2c_pairs<true>(w, x, npair, ntx, nty, ntz, ax2, ay2, az2, pp2, mm2);
+}
+
 template <int kMinBlocks>
 __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams P, ListParams L,
                                                                      const Mom* __restrict__ mom) {
@@ -341,7 +404,6 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams
   const int lane = threadIdx.x & 31;
   const float qnan = __int_as_float(0x7fc00000);
   const float kPad = 1.0e10f;
-  const float2 mthree = make_float2(-3.f, -3.f), mfive = make_float2(-5.f, -5.f), half = make_float2(0.5f, 0.5f);
   int64_t b;
   int tnode;
   while (next_bucket(P, lane, b, tnode)) {
@@ -359,6 +421,8 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams
       const float2 ntx = make_float2(-x.tx, -x.tx), nty = make_float2(-x.ty, -x.ty), ntz = make_float2(-x.tz, -x.tz);
       Kahan4 K;
       K.zero();
+      // plain packed sums over four chunks, then one compensated add
+      float2 ax2 = make_float2(0.f, 0.f), ay2 = ax2, az2 = ax2, pp2 = ax2, mm2 = ax2;
       for (int cs = 0; cs < count; cs += 64) {
         // stage this lane's two nodes as a pair
         float4 o[2], r0[2], r1[2];
@@ -395,52 +459,22 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams
         }
         __syncwarp();
         const int npair = (min(64, count - cs) + 1) >> 1;
-        float2 ax2 = make_float2(0.f, 0.f), ay2 = ax2, az2 = ax2, pp2 = ax2, mm2 = ax2;
+        // the softening test per pair only in chunks that hold a near node
+        // (voted by every lane, idle ones included)
+        const bool chunk_near = __any_sync(kFull, near[0] || near[1]);
         if (x.grp < x.G) {
-          for (int k = x.grp; k < npair; k += x.G) {
-            const float4 P5 = w.st[5][k];
-            if ((__float_as_int(P5.x) | __float_as_int(P5.y)) < 0) {  // a near node: scalar, softening tested
-              const float4 v = ev_p2c_pair_scalar(w, k, x.tx, x.ty, x.tz, x.ts);
-              ax2.x += v.x;
-              ay2.x += v.y;
-              az2.x += v.z;
-              pp2.x += v.w;
-              continue;
-            }
-            const float4 P0 = w.st[0][k], P1 = w.st[1][k];
-            const float2 rx = __fadd2_rn(make_float2(P0.x, P0.y), ntx);  // r' = o - t = -r
-            const float2 ry = __fadd2_rn(make_float2(P0.z, P0.w), nty);
-            const float2 rz = __fadd2_rn(make_float2(P1.x, P1.y), ntz);
-            float2 r2 = __fmul2_rn(rx, rx);
-            r2 = __ffma2_rn(ry, ry, r2);
-            r2 = __ffma2_rn(rz, rz, r2);
-            const float4 P2 = w.st[2][k], P3 = w.st[3][k], P4 = w.st[4][k];
-            const float2 a = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
-            const float2 d2 = __fmul2_rn(a, a);
-            const float2 bb = __fmul2_rn(a, d2);                       // b = 1/r^3
-            const float2 nc = __fmul2_rn(__fmul2_rn(bb, d2), mthree);  // -c = -3/r^5
-            const float2 d = __fmul2_rn(__fmul2_rn(nc, d2), mfive);    // d = 15/r^7
-            const float2 xx = make_float2(P2.x, P2.y), xy = make_float2(P2.z, P2.w);
-            const float2 xz = make_float2(P3.x, P3.y), yy = make_float2(P3.z, P3.w);
-            const float2 yz = make_float2(P4.x, P4.y), zz = make_float2(P4.z, P4.w);
-            const float2 qx = __ffma2_rn(xz, rz, __ffma2_rn(xy, ry, __fmul2_rn(xx, rx)));  // q' = -q
-            const float2 qy = __ffma2_rn(yz, rz, __ffma2_rn(yy, ry, __fmul2_rn(xy, rx)));
-            const float2 qz = __ffma2_rn(zz, rz, __ffma2_rn(yz, ry, __fmul2_rn(xz, rx)));
-            const float2 qir = __fmul2_rn(half, __ffma2_rn(qz, rz, __ffma2_rn(qy, ry, __fmul2_rn(qx, rx))));
-            const float2 M = make_float2(P1.z, P1.w), tr = make_float2(P5.x, P5.y);
-            // qir3 = b M + d qir - c tr; acc += qir3 r' - c q'; pot += b tr - c qir - M a
-            const float2 qir3 = __ffma2_rn(nc, tr, __ffma2_rn(d, qir, __fmul2_rn(bb, M)));
-            ax2 = __ffma2_rn(nc, qx, __ffma2_rn(qir3, rx, ax2));
-            ay2 = __ffma2_rn(nc, qy, __ffma2_rn(qir3, ry, ay2));
-            az2 = __ffma2_rn(nc, qz, __ffma2_rn(qir3, rz, az2));
-            pp2 = __ffma2_rn(nc, qir, __ffma2_rn(bb, tr, pp2));
-            mm2 = __ffma2_rn(M, a, mm2);
-          }
+          if (chunk_near)
+            ev_p2c_pairs_near(w, x, npair, ntx, nty, ntz, ax2, ay2, az2, pp2, mm2);
+          else
+            ev_p2c_pairs<false>(w, x, npair, ntx, nty, ntz, ax2, ay2, az2, pp2, mm2);
         }
-        K.add(0, ax2.x + ax2.y);
-        K.add(1, ay2.x + ay2.y);
-        K.add(2, az2.x + az2.y);
-        K.add(3, (pp2.x + pp2.y) - (mm2.x + mm2.y));
+        if (((cs >> 6) & 3) == 3 || cs + 64 >= count) {
+          K.add(0, ax2.x + ax2.y);
+          K.add(1, ay2.x + ay2.y);
+          K.add(2, az2.x + az2.y);
+          K.add(3, (pp2.x + pp2.y) - (mm2.x + mm2.y));
+          ax2 = ay2 = az2 = pp2 = mm2 = make_float2(0.f, 0.f);
+        }
       }
       ev_finish(w, K, x, P, t0, lane, P.accumulate == 0);
     }
@@ -501,40 +535,49 @@ __device__ __forceinline__ void ev_p2p_leaves(EvalWarp& w, int nleaves, const Tr
   }
   const int tota = __shfl_sync(kFull, inca, 31);
   const int total = tota + __shfl_sync(kFull, incb, 31);
-  if (lane < nleaves) {
-    w.pre[lane] = inca - na;
-    w.ps0[lane] = s0a;
-  }
-  if (lane + 32 < nleaves) {
-    w.pre[lane + 32] = tota + incb - nb;
-    w.ps0[lane + 32] = s0b;
-  }
-  if (lane == 0) w.pre[nleaves] = total;
+  // stream position of each leaf's first source, in registers (past the
+  // block: never reached); ps0 becomes source index - stream position
+  const int preA = (lane < nleaves) ? inca - na : INT_MAX;
+  const int preB = (lane + 32 < nleaves) ? tota + incb - nb : INT_MAX;
+  if (lane < nleaves) w.ps0[lane] = s0a - preA;
+  if (lane + 32 < nleaves) w.ps0[lane + 32] = s0b - preB;
+  // a leaf node always holds a particle: two leaves never start together
+  if (__any_sync(kFull, (lane < nleaves && na == 0) || (lane + 32 < nleaves && nb == 0)) && lane == 0)
+    atomicOr(P.status, kErrCapacity);
   __syncwarp();
   const float kPadPos = 1.0e10f;
   const float gs = (float)w.geom.soft_max;
   const float2 ntx = make_float2(-x.tx, -x.tx), nty = make_float2(-x.ty, -x.ty), ntz = make_float2(-x.tz, -x.tz);
-  int base_leaf = 0;
+  // plain packed sums over the block's chunks, one compensated add at its end
+  float2 ax2 = make_float2(0.f, 0.f), ay2 = ax2, az2 = ax2, pp2 = ax2;  // pp2 sums +m/r
   for (int cs = 0; cs < total; cs += 64) {
     {  // stage this lane's two sources
       const int q0 = cs + 2 * lane;
-      int lo = base_leaf;  // last leaf with pre <= q: a chunk spans few leaves
-      while (lo + 1 < nleaves && w.pre[lo + 1] <= q0) lo++;
-      int lo1 = lo;
-      while (lo1 + 1 < nleaves && w.pre[lo1 + 1] <= q0 + 1) lo1++;
-      base_leaf = __shfl_sync(kFull, lo1, 31);
+      // leaf of chunk positions 2 lane and 2 lane + 1: the leaf covering
+      // position cs plus the leaves that start in (cs, q] -- one bit per start
+      // position, OR-reduced over the warp, counted with popc
+      unsigned long long bits = 0ull;
+      const int pa = preA - cs, pb = preB - cs;
+      if (pa > 0 && pa < 64) bits |= 1ull << pa;
+      if (pb > 0 && pb < 64) bits |= 1ull << pb;
+      const unsigned long long starts =
+          ((unsigned long long)__reduce_or_sync(kFull, (unsigned)(bits >> 32)) << 32) |
+          __reduce_or_sync(kFull, (unsigned)bits);
+      const int b0 = __popc(__ballot_sync(kFull, preA <= cs)) + __popc(__ballot_sync(kFull, preB <= cs)) - 1;
+      const int lo = b0 + __popcll(starts & ((2ull << (2 * lane)) - 1ull));
+      const int lo1 = lo + (int)((starts >> (2 * lane + 1)) & 1ull);
       float4 ra = make_float4(kPadPos, kPadPos, kPadPos, 0.f), rb = ra;
       float4 oa = make_float4(0.f, 0.f, 0.f, 0.f), ob = oa;
       float sa = 0.f, sb = 0.f;
       if (q0 < total) {
         oa = w.lof[lo];
-        const int j = w.ps0[lo] + (q0 - w.pre[lo]);
+        const int j = w.ps0[lo] + q0;
         ra = P.srcf[j];
         if (!kFar) sa = P.softf[j];
       }
       if (q0 + 1 < total) {
         ob = w.lof[lo1];
-        const int j = w.ps0[lo1] + (q0 + 1 - w.pre[lo1]);
+        const int j = w.ps0[lo1] + q0 + 1;
         rb = P.srcf[j];
         if (!kFar) sb = P.softf[j];
       }
@@ -549,10 +592,10 @@ __device__ __forceinline__ void ev_p2p_leaves(EvalWarp& w, int nleaves, const Tr
       __syncwarp();
     }
     const int np = (min(64, total - cs) + 1) >> 1;
-    float2 ax2 = make_float2(0.f, 0.f), ay2 = ax2, az2 = ax2, pp2 = ax2;  // pp2 sums +m/r
     if (x.grp < x.G) {
-      for (int k = x.grp; k < np; k += x.G) {
-        const float4 X = w.st[0][k], Z = w.st[1][k];
+      const float4* sp = &w.st[0][x.grp];  // rows st[1], st[2] follow at +32, +64
+      for (int k = x.grp; k < np; k += x.G, sp += x.G) {
+        const float4 X = sp[0], Z = sp[32];
         const float2 dx = __fadd2_rn(make_float2(X.x, X.y), ntx);
         const float2 dy = __fadd2_rn(make_float2(X.z, X.w), nty);
         const float2 dz = __fadd2_rn(make_float2(Z.x, Z.y), ntz);
@@ -562,7 +605,7 @@ __device__ __forceinline__ void ev_p2p_leaves(EvalWarp& w, int nleaves, const Tr
         bool fast = true;
         float4 R = make_float4(0.f, 0.f, 0.f, 0.f);
         if (!kFar) {
-          R = w.st[2][k];
+          R = sp[64];
           fast = (r2.x > R.x) && (r2.y > R.y);
         }
         if (fast) {
@@ -579,11 +622,11 @@ __device__ __forceinline__ void ev_p2p_leaves(EvalWarp& w, int nleaves, const Tr
         }
       }
     }
-    K.add(0, ax2.x + ax2.y);
-    K.add(1, ay2.x + ay2.y);
-    K.add(2, az2.x + az2.y);
-    K.add(3, -(pp2.x + pp2.y));
   }
+  K.add(0, ax2.x + ax2.y);
+  K.add(1, ay2.x + ay2.y);
+  K.add(2, az2.x + az2.y);
+  K.add(3, -(pp2.x + pp2.y));
   __syncwarp();
 }
 

@@ -37,19 +37,30 @@ struct WalkFrame {
   uint32_t bits;  // P2P (0-7) | P2C quadrupole (8-15) | P2C monopole (16-23) | open (24-31)
 };
 
-// Space::intersect(box, centre, rsq) of the reference's utility submodule
-// (stand-in convention: squared gap accumulated x, y, z; intersect iff <=).
-// Used by GravityVisitor::open (:180) and ::openSoftening (:127).
+// Squared gap between a box and a point as Space::intersect of the
+// reference's utility submodule accumulates it (stand-in convention: per axis
+// d = lo - c if positive, else c - hi if positive, else nothing; summed x, y,
+// z).  Written with selects: an axis without a gap adds 0 * 0, which leaves
+// the (non-negative) sum unchanged, so the value is the branchy form's bit for
+// bit.
+__device__ __forceinline__ double box_gap2_exact(const double lo[3], const double hi[3], double cx, double cy,
+                                                 double cz) {
+  const double c[3] = {cx, cy, cz};
+  double dsq = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const double a = __dadd_rn(lo[k], -c[k]), b = __dadd_rn(c[k], -hi[k]);
+    const double d = (a > 0) ? a : ((b > 0) ? b : 0.0);
+    dsq = __dadd_rn(dsq, __dmul_rn(d, d));
+  }
+  return dsq;
+}
+
+// Space::intersect(box, centre, rsq): intersect iff the gap is <= rsq.  Used
+// by GravityVisitor::open (:180) and ::openSoftening (:127).
 __device__ __forceinline__ bool box_sphere_exact(const double lo[3], const double hi[3], double cx,
                                                  double cy, double cz, double rsq) {
-  double dsq = 0.0, d;
-  if ((d = __dadd_rn(lo[0], -cx)) > 0) dsq = __dadd_rn(dsq, __dmul_rn(d, d));
-  else if ((d = __dadd_rn(cx, -hi[0])) > 0) dsq = __dadd_rn(dsq, __dmul_rn(d, d));
-  if ((d = __dadd_rn(lo[1], -cy)) > 0) dsq = __dadd_rn(dsq, __dmul_rn(d, d));
-  else if ((d = __dadd_rn(cy, -hi[1])) > 0) dsq = __dadd_rn(dsq, __dmul_rn(d, d));
-  if ((d = __dadd_rn(lo[2], -cz)) > 0) dsq = __dadd_rn(dsq, __dmul_rn(d, d));
-  else if ((d = __dadd_rn(cz, -hi[2])) > 0) dsq = __dadd_rn(dsq, __dmul_rn(d, d));
-  return dsq <= rsq;
+  return box_gap2_exact(lo, hi, cx, cy, cz) <= rsq;
 }
 
 // Squared distance from a point to a box (0 inside); conservative helper.
@@ -63,16 +74,23 @@ __device__ __forceinline__ double box_dist2(const double lo[3], const double hi[
 }
 
 // GravityVisitor::openSoftening (:122-128): the softening spheres overlap, or
-// the target bucket's box meets the source sphere of radius 2*soft.
-__device__ __forceinline__ bool open_softening_exact(double scx, double scy, double scz, double ssoft,
-                                                     double tcx, double tcy, double tcz, double tsoft,
-                                                     const double lo[3], const double hi[3]) {
+// the target bucket's box meets the source sphere of radius 2*soft; gap2 is
+// box_gap2_exact of the bucket box and the source centre (the same gap the
+// opening test measured).
+__device__ __forceinline__ bool open_softening_gap(double scx, double scy, double scz, double ssoft, double tcx,
+                                                   double tcy, double tcz, double tsoft, double gap2) {
   double r1 = __dmul_rn(2.0, ssoft), r2 = __dmul_rn(2.0, tsoft);
   double dx = __dadd_rn(scx, -tcx), dy = __dadd_rn(scy, -tcy), dz = __dadd_rn(scz, -tcz);
   double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
   double rs = __dadd_rn(r1, r2);
   if (d2 <= __dmul_rn(rs, rs)) return true;
-  return box_sphere_exact(lo, hi, scx, scy, scz, __dmul_rn(r1, r1));
+  return gap2 <= __dmul_rn(r1, r1);
+}
+
+__device__ __forceinline__ bool open_softening_exact(double scx, double scy, double scz, double ssoft,
+                                                     double tcx, double tcy, double tcz, double tsoft,
+                                                     const double lo[3], const double hi[3]) {
+  return open_softening_gap(scx, scy, scz, ssoft, tcx, tcy, tcz, tsoft, box_gap2_exact(lo, hi, scx, scy, scz));
 }
 
 struct BucketGeom {
@@ -91,15 +109,25 @@ __device__ __forceinline__ void load_bucket_geom(const Mom* mom, int node, Bucke
   g.soft_max = q.soft_max;
 }
 
-// Class of one node against the bucket (GravityVisitor::open / node).
-__device__ __forceinline__ int classify_node(const WalkRec& w, const BucketGeom& g, double ox, double oy, double oz) {
+// Class of one node against the bucket (GravityVisitor::open / node).  The
+// box gap of the node's centre (plus offset) serves both the opening test and
+// openSoftening's second clause; it is returned in gap2 (-1 where it was not
+// needed: leaves, empty nodes, nodes opened by their count).
+__device__ __forceinline__ int classify_node_gap(const WalkRec& w, const BucketGeom& g, double ox, double oy,
+                                                 double oz, double& gap2) {
+  gap2 = -1.0;
   if (w.type == kTypeLeaf) return kClsP2P;
   if (w.type != kTypeInternal) return kClsNone;
+  if (w.count <= kMinParticleNode) return kClsOpen;
   const double cx = __dadd_rn(w.cm[0], ox), cy = __dadd_rn(w.cm[1], oy), cz = __dadd_rn(w.cm[2], oz);
-  if (w.count <= kMinParticleNode || box_sphere_exact(g.lo, g.hi, cx, cy, cz, w.orsq)) return kClsOpen;
-  if (w.count == 0) return kClsNone;
-  return open_softening_exact(cx, cy, cz, w.soft, g.cm[0], g.cm[1], g.cm[2], g.soft, g.lo, g.hi) ? kClsMono
-                                                                                                : kClsQuad;
+  gap2 = box_gap2_exact(g.lo, g.hi, cx, cy, cz);
+  if (gap2 <= w.orsq) return kClsOpen;
+  return open_softening_gap(cx, cy, cz, w.soft, g.cm[0], g.cm[1], g.cm[2], g.soft, gap2) ? kClsMono : kClsQuad;
+}
+
+__device__ __forceinline__ int classify_node(const WalkRec& w, const BucketGeom& g, double ox, double oy, double oz) {
+  double gap2;
+  return classify_node_gap(w, g, ox, oy, oz, gap2);
 }
 
 // Classify up to 8 nodes [c0, c0+nvalid) against the bucket; returns frame bits.
