@@ -340,8 +340,9 @@ __device__ __noinline__ float4 ev_p2c_pair_scalar(const EvalWarp& w, int k, floa
 
 // The staged node pairs k = grp, grp + G, ... of one chunk against this
 // lane's target (GravityVisitor::node, examples/GravityVisitor.h:184-224, in
-// packed FP32).  With kNear, pairs holding a near node take the scalar path.
-template <bool kNear>
+// packed FP32); pairs holding a near node take the scalar path.  (A loop
+// without that test for chunks with no near node, chosen per chunk, measured
+// slower: the second copy costs registers.)
 __device__ __forceinline__ void ev_p2c_pairs(const EvalWarp& w, const EvTarget& x, int npair, float2 ntx, float2 nty,
                                              float2 ntz, float2& ax2, float2& ay2, float2& az2, float2& pp2,
                                              float2& mm2) {
@@ -349,7 +350,7 @@ __device__ __forceinline__ void ev_p2c_pairs(const EvalWarp& w, const EvTarget& 
   const float4* sp = &w.st[0][x.grp];  // rows st[1..5] follow at +32 each
   for (int k = x.grp; k < npair; k += x.G, sp += x.G) {
     const float4 P5 = sp[160];
-    if (kNear && (__float_as_int(P5.x) | __float_as_int(P5.y)) < 0) {  // a near node: scalar, softening tested
+    if ((__float_as_int(P5.x) | __float_as_int(P5.y)) < 0) {  // a near node: scalar, softening tested
       const float4 v = ev_p2c_pair_scalar(w, k, x.tx, x.ty, x.tz, x.ts);
       ax2.x += v.x;
       ay2.x += v.y;
@@ -388,14 +389,6 @@ __device__ __forceinline__ void ev_p2c_pairs(const EvalWarp& w, const EvTarget& 
   }
 }
 
-// The rare chunks with a near node, out of line so that the common loop keeps
-// its registers.
-__device__ __noinline__ void ev_p2c_pairs_near(const EvalWarp& w, const EvTarget& x, int npair, float2 ntx,
-                                               float2 nty, float2 ntz, float2& ax2, float2& ay2, float2& az2,
-                                               float2& pp2, float2& mm2) {
-  ev_p2c_pairs<true>(w, x, npair, ntx, nty, ntz, ax2, ay2, az2, pp2, mm2);
-}
-
 template <int kMinBlocks>
 __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams P, ListParams L,
                                                                      const Mom* __restrict__ mom) {
@@ -423,7 +416,17 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams
       K.zero();
       // plain packed sums over four chunks, then one compensated add
       float2 ax2 = make_float2(0.f, 0.f), ay2 = ax2, az2 = ax2, pp2 = ax2, mm2 = ax2;
+      // list entries of the coming chunk, loaded a chunk ahead so that only
+      // the node records wait at staging time
+      int en0 = (2 * lane < count) ? L.pc_pool[start + 2 * lane] : 0;
+      int en1 = (2 * lane + 1 < count) ? L.pc_pool[start + 2 * lane + 1] : 0;
       for (int cs = 0; cs < count; cs += 64) {
+        const int ec[2] = {en0, en1};
+        if (cs + 64 < count) {
+          const int qn = cs + 64 + 2 * lane;
+          en0 = (qn < count) ? L.pc_pool[start + qn] : 0;
+          en1 = (qn + 1 < count) ? L.pc_pool[start + qn + 1] : 0;
+        }
         // stage this lane's two nodes as a pair
         float4 o[2], r0[2], r1[2];
         bool near[2] = {false, false};
@@ -434,7 +437,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams
           r0[h] = make_float4(0.f, 0.f, 0.f, 0.f);
           r1[h] = r0[h];
           if (q < count) {
-            const int e = L.pc_pool[start + q];
+            const int e = ec[h];
             const int node = e & 0x3fffffff;
             near[h] = (e & 0x40000000) != 0;
             const float4* rec = reinterpret_cast<const float4*>(P.quadf + node);
@@ -459,15 +462,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams
         }
         __syncwarp();
         const int npair = (min(64, count - cs) + 1) >> 1;
-        // the softening test per pair only in chunks that hold a near node
-        // (voted by every lane, idle ones included)
-        const bool chunk_near = __any_sync(kFull, near[0] || near[1]);
-        if (x.grp < x.G) {
-          if (chunk_near)
-            ev_p2c_pairs_near(w, x, npair, ntx, nty, ntz, ax2, ay2, az2, pp2, mm2);
-          else
-            ev_p2c_pairs<false>(w, x, npair, ntx, nty, ntz, ax2, ay2, az2, pp2, mm2);
-        }
+        if (x.grp < x.G) ev_p2c_pairs(w, x, npair, ntx, nty, ntz, ax2, ay2, az2, pp2, mm2);
         if (((cs >> 6) & 3) == 3 || cs + 64 >= count) {
           K.add(0, ax2.x + ax2.y);
           K.add(1, ay2.x + ay2.y);
