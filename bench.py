@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--sweep", default="0.5,0.7,1.0",
                     help="theta values of the accuracy / throughput sweep ('' to skip)")
+    ap.add_argument("--sph", action="store_true",
+                    help="time only the SPH density and pressure passes on the workload (1 GPU)")
     return ap.parse_args()
 
 
@@ -233,6 +235,12 @@ def main():
     stream = torch.cuda.current_stream()
     sim.set_stream(stream.cuda_stream)
     sim.set_particles(p)
+    if a.sph:
+        out = {"workload": workload_config(a, world)["workload"], "sph_density": sph_density_rate(a, sim, stream),
+               "sph_pressure": sph_pressure_rate(a, sim, stream)}
+        if rank == 0:
+            print(json.dumps(out))
+        return
 
     shard = None
     if world > 1:  # buckets cut by measured work; results summed over the ranks (NCCL)

@@ -7,14 +7,22 @@
 // bit; the neighbour set is the exact k nearest (the particle itself
 // included), which the reference's conservative open() also yields.
 //
-// One warp per bucket, lanes = target particles (chunks of 32).  Each lane
-// keeps a max-heap of its k best (d2, particle) in shared memory.  The walk is
-// depth first from the root; a popped node is visited if any lane's heap is
-// not full or its ball (the current k-th d2) reaches the node's box
-// (DensityVisitor::open with Space::intersect's <=), so balls that shrank
-// since the push prune more; children are pushed far to near (distance of
-// their boxes to the bucket's centre) so the nearest subtree is searched first.
-//
+// One warp per bucket; each of its targets keeps its current 32 best
+// (d2, particle) as a list sorted ascending across the 32 lanes (lane e holds
+// entry e), in a per-warp global scratch (coalesced, L1-resident).  Candidates
+// come in batches of 32 (one per lane): a ballot against the target's 32nd
+// entry discards a batch that cannot improve the list; otherwise the passing
+// candidates are inserted (a few) or bitonic-sorted and merged (many).  Ties
+// are broken by particle index, so the list is the k smallest (d2, index).
+//   1. The lists start from a window of 64 particles around the bucket in key
+//      order (spatially close), which bounds every target's ball.
+//   2. A depth-first walk from the root visits a node if some target's ball
+//      reaches its box (DensityVisitor::open with Space::intersect's <=),
+//      children pushed far to near, and buffers the leaves it reaches; the
+//      buffer is flushed (its particles batched against every target) when
+//      full and at the end, and each flush shrinks the balls that later
+//      visits test.
+//   3. DensityFn: ball^2 = the 32nd d2, density summed over the list.
 // The pressure pass that follows (sph_pressure_kernel) restates ForceFn
 // (examples/SPH.C:39-64) and doSPHCalc (examples/SPHUtils.h:64-133): one warp
 // per particle, lane e = its e-th neighbour from the density pass.  The divv
@@ -22,21 +30,28 @@
 // sums; the opposite reaction on each neighbour (ThreadStateHolder's opposing
 // effects, applied after the pass in the reference) is an FP64 atomic add, so
 // its summation order is not fixed.
+#include <math_constants.h>
+
 #include "pt_internal.cuh"
 #include "pt_walk.cuh"
 
 namespace pt {
 
 constexpr int kSphK = 32;
-constexpr int kSphWarps = 2;
-constexpr int kSphStack = 256;  // pending nodes: <= 21 levels x 7 siblings + the root
+constexpr int kKnnWarps = 4;
+constexpr int kKnnStack = 640;   // pending frames: 4 popped per step, <= 32 pushed
+constexpr int kKnnLeaves = 128;  // leaves buffered between flushes
+constexpr int kKnnChunk = 128;   // candidates staged per pass over the targets
+constexpr int kKnnNone = 0x7fffffff;
 
-struct SphWarp {
-  double hd[kSphK][32];  // heap distances^2, column per lane
-  int32_t hi[kSphK][32]; // heap particles (sorted order)
-  int32_t stack[kSphStack];
-  double sx[32], sy[32], sz[32];
-  int32_t sidx[32];
+struct KnnWarp {
+  double cx[kKnnChunk], cy[kKnnChunk], cz[kKnnChunk];  // staged candidates
+  int32_t ci[kKnnChunk];
+  double tx[32], ty[32], tz[32];  // the chunk's targets
+  double kd[32];                  // each target's list's last entry
+  int32_t ki[32];
+  int32_t stack[kKnnStack];
+  int32_t leaf[kKnnLeaves];
 };
 
 __device__ __forceinline__ double box_d2(const double lo[3], const double hi[3], double x, double y, double z) {
@@ -58,18 +73,195 @@ __device__ __forceinline__ double kernel_m4(double ar2) {
   return ak;
 }
 
-__global__ void __launch_bounds__(kSphWarps * 32) sph_density_kernel(Particles p, const Mom* __restrict__ mom,
-                                                                      const WalkRec* __restrict__ walk,
-                                                                      const int32_t* __restrict__ buckets,
-                                                                      int64_t nbuckets, int64_t nnodes,
-                                                                      double* __restrict__ density,
-                                                                      double* __restrict__ ballsq,
-                                                                      int32_t* __restrict__ nbr,
-                                                                      double* __restrict__ nd2, unsigned* work,
-                                                                      unsigned* status) {
-  __shared__ SphWarp warps[kSphWarps];
-  SphWarp& w = warps[threadIdx.x >> 5];
+// (d, i) before (e, j): smaller d2, then smaller index.
+__device__ __forceinline__ bool knn_before(double d, int i, double e, int j) { return d < e || (d == e && i < j); }
+
+// One compare-exchange stage across lanes lane and lane ^ j; the lower lane of
+// the pair keeps the smaller element when up, the larger otherwise.
+__device__ __forceinline__ void knn_stage(double& d, int& i, int j, bool up, int lane) {
+  const double pd = __shfl_xor_sync(kFull, d, j);
+  const int pi = __shfl_xor_sync(kFull, i, j);
+  const bool keep_min = (((lane & j) == 0) == up);
+  const bool pb = knn_before(pd, pi, d, i);
+  if (keep_min ? pb : (!pb && (pd != d || pi != i))) {
+    d = pd;
+    i = pi;
+  }
+}
+
+// Sort the 32 lanes' (d, i) ascending (bitonic network).
+__device__ __forceinline__ void knn_sort32(double& d, int& i, int lane) {
+#pragma unroll
+  for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) knn_stage(d, i, j, (lane & k) == 0 || k == 32, lane);
+}
+
+// List (ascending across lanes) <- the 32 smallest of list and batch
+// (ascending): the element-wise minimum with the reversed batch is bitonic and
+// holds them; one bitonic merge sorts it.
+__device__ __forceinline__ void knn_merge(double& ld, int& li, double bd, int bi, int lane) {
+  const double rd = __shfl_sync(kFull, bd, 31 - lane);
+  const int ri = __shfl_sync(kFull, bi, 31 - lane);
+  if (knn_before(rd, ri, ld, li)) {
+    ld = rd;
+    li = ri;
+  }
+#pragma unroll
+  for (int j = 16; j > 0; j >>= 1) knn_stage(ld, li, j, true, lane);
+}
+
+// Insert one candidate (cd, ci), known to beat the list's last entry.
+__device__ __forceinline__ void knn_insert(double& ld, int& li, double cd, int ci, int lane) {
+  const int pos = __popc(__ballot_sync(kFull, knn_before(ld, li, cd, ci)));  // entries that stay ahead
+  const double ud = __shfl_up_sync(kFull, ld, 1);
+  const int ui = __shfl_up_sync(kFull, li, 1);
+  if (lane == pos) {
+    ld = cd;
+    li = ci;
+  } else if (lane > pos) {
+    ld = ud;
+    li = ui;
+  }
+}
+
+// The cnt staged candidates against every target of the chunk (nt of them),
+// target by target: a target's list (global scratch, lane e = entry e) is
+// loaded once, on the first batch of 32 that can improve it.
+__device__ __forceinline__ void knn_chunk(KnnWarp& w, int nt, int cnt, double* __restrict__ Ld,
+                                          int32_t* __restrict__ Li, int lane) {
+  __syncwarp();
+  for (int t = 0; t < nt; t++) {
+    const double xt = w.tx[t], yt = w.ty[t], zt = w.tz[t];
+    double kd = w.kd[t];
+    int ki = w.ki[t];
+    bool loaded = false;
+    double ld = CUDART_INF;
+    int li = kKnnNone;
+    for (int b = 0; b < cnt; b += 32) {
+      const int c = b + lane;
+      const int j = (c < cnt) ? w.ci[c] : -1;
+      double d2 = CUDART_INF;
+      if (j >= 0) {
+        const double dx = __dadd_rn(xt, -w.cx[c]), dy = __dadd_rn(yt, -w.cy[c]), dz = __dadd_rn(zt, -w.cz[c]);
+        d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+      }
+      const bool pass = j >= 0 && knn_before(d2, j, kd, ki);
+      const unsigned m = __ballot_sync(kFull, pass);
+      if (m == 0u) continue;
+      if (!loaded) {
+        ld = Ld[t * 32 + lane];
+        li = Li[t * 32 + lane];
+        loaded = true;
+      }
+      if (__popc(m) <= 12) {
+        unsigned r = m;
+        while (r) {
+          const int src = __ffs(r) - 1;
+          r &= r - 1u;
+          const double cd = __shfl_sync(kFull, d2, src);
+          const int cj = __shfl_sync(kFull, j, src);
+          // an earlier insertion of this batch may have raised the bar past it
+          if (knn_before(cd, cj, kd, ki)) {
+            knn_insert(ld, li, cd, cj, lane);
+            kd = __shfl_sync(kFull, ld, 31);
+            ki = __shfl_sync(kFull, li, 31);
+          }
+        }
+      } else {
+        double cd = pass ? d2 : CUDART_INF;
+        int cj = pass ? j : kKnnNone;
+        knn_sort32(cd, cj, lane);
+        knn_merge(ld, li, cd, cj, lane);
+        kd = __shfl_sync(kFull, ld, 31);
+        ki = __shfl_sync(kFull, li, 31);
+      }
+    }
+    if (loaded) {
+      Ld[t * 32 + lane] = ld;
+      Li[t * 32 + lane] = li;
+      if (lane == 0) {
+        w.kd[t] = kd;
+        w.ki[t] = ki;
+      }
+    }
+  }
+  __syncwarp();
+}
+
+// Stage candidate j (or none) in slot c.
+__device__ __forceinline__ void knn_stage_candidate(KnnWarp& w, const Particles& p, int c, int j) {
+  w.ci[c] = j;
+  if (j >= 0) {
+    w.cx[c] = p.x[j];
+    w.cy[c] = p.y[j];
+    w.cz[c] = p.z[j];
+  }
+}
+
+// The buffered leaves' particles, minus the window [w0, w1), staged
+// kKnnChunk at a time.
+__device__ __forceinline__ void knn_flush(const Particles& p, const WalkRec* __restrict__ walk, KnnWarp& w, int nt,
+                                          int nleaf, int w0, int w1, double* Ld, int32_t* Li, int lane) {
+  int fill = 0;
+  for (int l = 0; l < nleaf; l++) {
+    const int nd = w.leaf[l];
+    const int s0 = walk[nd].pstart, sn = walk[nd].pcount;
+    for (int base = 0; base < sn;) {
+      const int take = min(min(sn - base, 32), kKnnChunk - fill);
+      __syncwarp();
+      if (lane < take) {
+        const int j = s0 + base + lane;
+        knn_stage_candidate(w, p, fill + lane, (j >= w0 && j < w1) ? -1 : j);
+      }
+      fill += take;
+      base += take;
+      if (fill == kKnnChunk) {
+        knn_chunk(w, nt, fill, Ld, Li, lane);
+        fill = 0;
+      }
+    }
+  }
+  if (fill > 0) knn_chunk(w, nt, fill, Ld, Li, lane);
+}
+
+// Squared gap between two boxes (0 if they overlap).
+__device__ __forceinline__ double box_box_gap2(const double alo[3], const double ahi[3], const double blo[3],
+                                               const double bhi[3]) {
+  double d = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const double g = fmax(fmax(alo[k] - bhi[k], blo[k] - ahi[k]), 0.0);
+    d += g * g;
+  }
+  return d;
+}
+
+// The largest ball^2 (last list entry) over the chunk's targets.
+__device__ __forceinline__ double knn_rmax2(const KnnWarp& w, int lane) {
+  double r = w.kd[lane];  // -1 in the slots of absent targets
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_xor_sync(kFull, r, o));
+  return r;
+}
+
+__global__ void __launch_bounds__(kKnnWarps * 32, 7) sph_density_kernel(Particles p, int64_t n,
+                                                                        const Mom* __restrict__ mom,
+                                                                        const WalkRec* __restrict__ walk,
+                                                                        const int32_t* __restrict__ buckets,
+                                                                        int64_t nbuckets, int64_t nnodes,
+                                                                        double* __restrict__ density,
+                                                                        double* __restrict__ ballsq,
+                                                                        int32_t* __restrict__ nbr,
+                                                                        double* __restrict__ nd2, double* lists_d,
+                                                                        int32_t* lists_i, unsigned* work,
+                                                                        unsigned* status) {
+  __shared__ KnnWarp warps[kKnnWarps];
+  KnnWarp& w = warps[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
+  const int64_t slot = (int64_t)blockIdx.x * kKnnWarps + (threadIdx.x >> 5);
+  double* Ld = lists_d + slot * 1024;
+  int32_t* Li = lists_i + slot * 1024;
   while (true) {
     unsigned bi = 0;
     if (lane == 0) bi = atomicAdd(work, 1u);
@@ -81,130 +273,108 @@ __global__ void __launch_bounds__(kSphWarps * 32) sph_density_kernel(Particles p
       continue;
     }
     const int tbase = walk[tnode].pstart, ntot = walk[tnode].pcount;
-    const double gx = mom[tnode].cm[0], gy = mom[tnode].cm[1], gz = mom[tnode].cm[2];
     for (int tc = 0; tc < ntot; tc += 32) {
       const int t0 = tbase + tc, nt = min(32, ntot - tc);
       const bool act = lane < nt;
-      double xi = 0.0, yi = 0.0, zi = 0.0;
+      double x = 0.0, y = 0.0, z = 0.0;
       if (act) {
-        xi = p.x[t0 + lane];
-        yi = p.y[t0 + lane];
-        zi = p.z[t0 + lane];
+        x = p.x[t0 + lane];
+        y = p.y[t0 + lane];
+        z = p.z[t0 + lane];
       }
-      int cnt = 0;  // heap entries of this lane
-      int sp = 0;
-      if (lane == 0) w.stack[0] = 0;
-      sp = 1;
-      bool ok = true;
       __syncwarp();
-      while (sp > 0) {
-        const int node = w.stack[sp - 1];
-        sp--;
-        __syncwarp();
-        if (node < 0 || node >= nnodes) {
-          if (lane == 0) atomicOr(status, kErrCapacity);
-          continue;
+      w.tx[lane] = x;
+      w.ty[lane] = y;
+      w.tz[lane] = z;
+      w.kd[lane] = act ? CUDART_INF : -1.0;  // no target: no ball
+      w.ki[lane] = kKnnNone;
+      for (int t = 0; t < nt; t++) {
+        Ld[t * 32 + lane] = CUDART_INF;
+        Li[t * 32 + lane] = kKnnNone;
+      }
+      // 1. a window of 64 particles around the chunk in key order
+      const int64_t wl = max((int64_t)0, min((int64_t)t0 + nt / 2 - 32, n - 64));
+      const int w0 = (int)wl, w1 = (int)min(n, wl + 64);
+      knn_stage_candidate(w, p, lane, w0 + lane < w1 ? w0 + lane : -1);
+      knn_stage_candidate(w, p, 32 + lane, w0 + 32 + lane < w1 ? w0 + 32 + lane : -1);
+      knn_chunk(w, nt, 64, Ld, Li, lane);
+      // 2. the walk, 32 children (4 opened nodes) per step: a node is kept
+      // if its box comes within the largest ball of the bucket's particle box
+      // (a superset of DensityVisitor::open's per-target test, with a margin
+      // for rounding); the leaves kept are buffered and flushed after 4, 8,
+      // 16, ... so that the balls shrink early
+      const double blo[3] = {mom[tnode].lo[0], mom[tnode].lo[1], mom[tnode].lo[2]};
+      const double bhi[3] = {mom[tnode].hi[0], mom[tnode].hi[1], mom[tnode].hi[2]};
+      double rmax = knn_rmax2(w, lane);
+      int sp = 0, nleaf = 0, fthr = 4, nexp = 1, pop = -1;
+      bool ok = true;
+      while (true) {
+        const int e = lane >> 3, c = lane & 7;
+        int node = -1;
+        if (pop < 0) {
+          if (lane == 0) node = 0;
+        } else if (e < nexp) {
+          node = w.stack[pop + e] + c;
         }
-        const WalkRec& r = walk[node];
-        const int type = r.type;
-        if (type != kTypeLeaf && type != kTypeInternal) continue;
-        // open: some lane's heap is not full, or its ball reaches the box
-        const Mom& q = mom[node];
-        bool want = false;
-        if (act) want = (cnt < kSphK) || (box_d2(q.lo, q.hi, xi, yi, zi) <= w.hd[0][lane]);
-        if (!__any_sync(kFull, want)) continue;
-        if (type == kTypeInternal) {
-          // children far to near by the distance of their boxes to the bucket centre
-          const int c = lane & 7;
-          const int child = r.first_child + c;
-          double dc = -1.0;
-          bool live = false;
-          if (lane < 8 && child < nnodes) {
-            const int ct = walk[child].type;
-            live = (ct == kTypeLeaf || ct == kTypeInternal);
-            if (live) dc = box_d2(mom[child].lo, mom[child].hi, gx, gy, gz);
-          }
-          const unsigned lm = __ballot_sync(kFull, live) & 0xffu;
-          const int nlive = __popc(lm);
-          if (sp + nlive > kSphStack) {
-            ok = false;
-            break;
-          }
-          int rank = 0;  // children nearer than this one (ties: lower index first)
-#pragma unroll
-          for (int o = 0; o < 8; o++) {
-            const double d = __shfl_sync(kFull, dc, o);
-            const bool lv = (lm >> o) & 1u;
-            if (live && lv && o != c && (d < dc || (d == dc && o < c))) rank++;
-          }
-          if (live) w.stack[sp + nlive - 1 - rank] = child;  // the nearest ends on top
-          sp += nlive;
-          __syncwarp();
-          continue;
-        }
-        // leaf: every lane tests every particle (DensityVisitor::leaf)
-        const int s0 = r.pstart, sn = r.pcount;
-        for (int base = 0; base < sn; base += 32) {
-          const int cntj = min(32, sn - base);
-          __syncwarp();
-          if (lane < cntj) {
-            const int j = s0 + base + lane;
-            w.sx[lane] = p.x[j];
-            w.sy[lane] = p.y[j];
-            w.sz[lane] = p.z[j];
-            w.sidx[lane] = j;
-          }
-          __syncwarp();
-          if (act) {
-            for (int jj = 0; jj < cntj; jj++) {
-              const double dx = __dadd_rn(xi, -w.sx[jj]), dy = __dadd_rn(yi, -w.sy[jj]),
-                           dz = __dadd_rn(zi, -w.sz[jj]);
-              const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-              if (cnt < kSphK) {  // push and sift up
-                int pos = cnt++;
-                while (pos > 0) {
-                  const int par = (pos - 1) >> 1;
-                  if (!(w.hd[par][lane] < d2)) break;
-                  w.hd[pos][lane] = w.hd[par][lane];
-                  w.hi[pos][lane] = w.hi[par][lane];
-                  pos = par;
-                }
-                w.hd[pos][lane] = d2;
-                w.hi[pos][lane] = w.sidx[jj];
-              } else if (d2 < w.hd[0][lane]) {  // replace the farthest and sift down
-                int pos = 0;
-                while (true) {
-                  int ch = 2 * pos + 1;
-                  if (ch >= kSphK) break;
-                  if (ch + 1 < kSphK && w.hd[ch + 1][lane] > w.hd[ch][lane]) ch++;
-                  if (!(w.hd[ch][lane] > d2)) break;
-                  w.hd[pos][lane] = w.hd[ch][lane];
-                  w.hi[pos][lane] = w.hi[ch][lane];
-                  pos = ch;
-                }
-                w.hd[pos][lane] = d2;
-                w.hi[pos][lane] = w.sidx[jj];
-              }
+        bool keep = false, internal = false;
+        int first = 0;
+        if (node >= 0) {
+          if (node >= nnodes) {
+            atomicOr(status, kErrCapacity);
+          } else {
+            const int type = walk[node].type;
+            if (type == kTypeLeaf || type == kTypeInternal) {
+              internal = (type == kTypeInternal);
+              first = walk[node].first_child;
+              keep = box_box_gap2(mom[node].lo, mom[node].hi, blo, bhi) <= rmax * (1.0 + 1e-13);
             }
           }
         }
+        const unsigned lt = (1u << lane) - 1u;
+        const unsigned ml = __ballot_sync(kFull, keep && !internal);
+        const unsigned mi = __ballot_sync(kFull, keep && internal);
+        if (sp + __popc(mi) > kKnnStack || nleaf + __popc(ml) > kKnnLeaves) {
+          ok = false;
+          break;
+        }
         __syncwarp();
+        if (keep && !internal) w.leaf[nleaf + __popc(ml & lt)] = node;
+        if (keep && internal) w.stack[sp + __popc(mi & lt)] = first;
+        nleaf += __popc(ml);
+        sp += __popc(mi);
+        __syncwarp();
+        if (nleaf >= fthr || (sp == 0 && nleaf > 0)) {
+          knn_flush(p, walk, w, nt, nleaf, w0, w1, Ld, Li, lane);
+          nleaf = 0;
+          fthr = min(2 * fthr, kKnnLeaves - 32);
+          rmax = knn_rmax2(w, lane);
+        }
+        if (sp == 0) break;
+        nexp = sp < 4 ? sp : 4;
+        sp -= nexp;
+        pop = sp;
       }
       if (!ok && lane == 0) atomicOr(status, kErrStack);
-      // DensityFn: rsq = the heap's largest d2
-      if (act && cnt > 0) {
-        const int i = t0 + lane;
-        const double rsq = w.hd[0][lane], fBall = sqrt(rsq), ih2 = 4.0 / rsq;
-        double dens = 0.0;
-        for (int e = 0; e < cnt; e++) dens += kernel_m4(w.hd[e][lane] * ih2) * p.m[w.hi[e][lane]];
-        dens /= (0.125 * M_PI * (rsq * fBall));
-        density[i] = dens;
-        ballsq[i] = rsq;
+      // 3. DensityFn over each target's list (ascending: the ball is its last
+      // found entry)
+      for (int t = 0; t < nt; t++) {
+        const double ld = Ld[t * 32 + lane];
+        const int li = Li[t * 32 + lane];
+        const bool found = li != kKnnNone;
+        const int cnt = __popc(__ballot_sync(kFull, found));
+        const double rsq = __shfl_sync(kFull, ld, max(cnt - 1, 0));
+        const double fBall = sqrt(rsq), ih2 = 4.0 / rsq;
+        double term = found ? kernel_m4(ld * ih2) * p.m[li] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) term += __shfl_xor_sync(kFull, term, o);
+        const int i = t0 + t;
+        if (lane == 0 && cnt > 0) {
+          density[i] = term / (0.125 * M_PI * (rsq * fBall));
+          ballsq[i] = rsq;
+        }
         if (nbr) {
-          for (int e = 0; e < kSphK; e++) {
-            nbr[(int64_t)i * kSphK + e] = e < cnt ? w.hi[e][lane] : -1;
-            nd2[(int64_t)i * kSphK + e] = e < cnt ? w.hd[e][lane] : -1.0;
-          }
+          nbr[(int64_t)i * kSphK + lane] = found ? li : -1;
+          nd2[(int64_t)i * kSphK + lane] = found ? ld : -1.0;
         }
       }
       __syncwarp();
@@ -317,12 +487,15 @@ void launch_sph_pressure(Particles p, const double* density, const double* balls
   sph_pressure_kernel<<<grid, 256, 0, st>>>(p, density, ballsq, u, nbr, nd2, n, ax, ay, az, pdv, status);
 }
 
-void launch_sph_density(Particles p, const Mom* mom, const WalkRec* walk, const int32_t* buckets, int64_t nbuckets,
-                        int64_t nnodes, double* density, double* ballsq, int32_t* nbr, double* nd2, unsigned* work,
-                        unsigned* status, int grid, cudaStream_t st) {
+int sph_knn_slots(int grid) { return grid * kKnnWarps; }
+
+void launch_sph_density(Particles p, int64_t n, const Mom* mom, const WalkRec* walk, const int32_t* buckets,
+                        int64_t nbuckets, int64_t nnodes, double* density, double* ballsq, int32_t* nbr, double* nd2,
+                        double* lists_d, int32_t* lists_i, unsigned* work, unsigned* status, int grid,
+                        cudaStream_t st) {
   note_launch();
-  sph_density_kernel<<<grid, kSphWarps * 32, 0, st>>>(p, mom, walk, buckets, nbuckets, nnodes, density, ballsq, nbr,
-                                                      nd2, work, status);
+  sph_density_kernel<<<grid, kKnnWarps * 32, 0, st>>>(p, n, mom, walk, buckets, nbuckets, nnodes, density, ballsq,
+                                                      nbr, nd2, lists_d, lists_i, work, status);
 }
 
 }  // namespace pt

@@ -84,6 +84,9 @@ struct pt_handle {
   int64_t sph_cap = 0, sph_nbr_cap = 0;
   int32_t* sph_nbr = nullptr;
   double* sph_nd2 = nullptr;
+  double* sph_list_d = nullptr;  // neighbour-search scratch: per-warp lists
+  int32_t* sph_list_i = nullptr;
+  int64_t sph_list_cap = 0;
 
   double4* d_htab = nullptr;  // Ewald reciprocal table (h vector, hCfac)
   int htab_cap = 0;
@@ -797,6 +800,7 @@ int pt_destroy(pt_handle* h) {
   dfree(o.fifo); dfree(o.nleaf_sub); dfree(o.nempty_sub); dfree(o.leaf_base); dfree(o.empty_base);
   dfree(h->flags); dfree(h->buckets); dfree(h->bucket_work); dfree(h->list_count); dfree(h->list_off); dfree(h->list_node);
   dfree(h->list_kind); dfree(h->dsum); dfree(h->adj); dfree(h->nadj); dfree(h->d_htab); dfree(h->ewd); dfree(h->sph); dfree(h->sph_nbr); dfree(h->sph_nd2);
+  dfree(h->sph_list_d); dfree(h->sph_list_i);
   dfree(h->pool_pc); dfree(h->pool_pp); dfree(h->l_pc_start); dfree(h->l_pp_start); dfree(h->l_pc_count);
   dfree(h->l_pp_count); dfree(h->d_lcur); dfree(h->d_work3);
   for (auto& e : h->ev)
@@ -909,10 +913,18 @@ static int sph_density_device(pt_handle* h, bool want_nbr) {
     CKR(dalloc(h, &h->sph_nd2, n * k));
     h->sph_nbr_cap = n * k;
   }
+  // per-warp candidate lists of the neighbour search: 32 targets x 32 entries
+  const int kgrid = h->sms * 7;
+  const int64_t slots = sph_knn_slots(kgrid);
+  if (slots * 1024 > h->sph_list_cap) {
+    CKR(dalloc(h, &h->sph_list_d, slots * 1024));
+    CKR(dalloc(h, &h->sph_list_i, slots * 1024));
+    h->sph_list_cap = slots * 1024;
+  }
   CK(cudaMemsetAsync(h->d_work, 0, sizeof(unsigned), st));
-  launch_sph_density(h->p, h->nd.mom, h->nd.walk, h->buckets, h->nbuckets, h->nnodes, h->sph, h->sph + n,
-                     want_nbr ? h->sph_nbr : nullptr, want_nbr ? h->sph_nd2 : nullptr, h->d_work, h->d_status,
-                     h->sms * 16, st);
+  launch_sph_density(h->p, n, h->nd.mom, h->nd.walk, h->buckets, h->nbuckets, h->nnodes, h->sph, h->sph + n,
+                     want_nbr ? h->sph_nbr : nullptr, want_nbr ? h->sph_nd2 : nullptr, h->sph_list_d,
+                     h->sph_list_i, h->d_work, h->d_status, kgrid, st);
   CK(cudaGetLastError());
   return read_status(h);
 }

@@ -79,9 +79,11 @@ int sph_k();
 void launch_sph_pressure(Particles p, const double* density, const double* ballsq, const double* u,
                          const int32_t* nbr, const double* nd2, int64_t n, double* ax, double* ay, double* az,
                          double* pdv, unsigned* status, int grid, cudaStream_t st);
-void launch_sph_density(Particles p, const Mom* mom, const WalkRec* walk, const int32_t* buckets, int64_t nbuckets,
-                        int64_t nnodes, double* density, double* ballsq, int32_t* nbr, double* nd2, unsigned* work,
-                        unsigned* status, int grid, cudaStream_t st);
+int sph_knn_slots(int grid);
+void launch_sph_density(Particles p, int64_t n, const Mom* mom, const WalkRec* walk, const int32_t* buckets,
+                        int64_t nbuckets, int64_t nnodes, double* density, double* ballsq, int32_t* nbr, double* nd2,
+                        double* lists_d, int32_t* lists_i, unsigned* work, unsigned* status, int grid,
+                        cudaStream_t st);
 
 // k_adjoint.cu
 void launch_adjoint(const AdjParams& A, int grid, cudaStream_t st);
