@@ -226,3 +226,21 @@ def test_sph_pressure_tiny(n):
     want = O.sph_pressure(p, u, dp, bp, nbp, nd2p)
     for got, w in zip((ax, ay, az, pdv), want):
         assert _close(got, w, 1e-12)
+
+
+@pytest.mark.parametrize("ngrid,bucket", [(8, 16), (16, 32)])
+def test_sph_density_exact_ties_on_a_lattice(ngrid, bucket):
+    """Exactly equal distances (a perfect lattice): ball^2 bit-exact, density
+    to summation order and every neighbour inside the ball as the C oracle's;
+    which of the particles at exactly the ball's distance fill the last slots
+    is a tie the reference leaves open."""
+    p = ics.lattice(ngrid, seed=1, rms_cells=0.0)
+    with sim(max_particles_per_leaf=bucket) as s:
+        s.set_particles(p)
+        d, b, nbr, nd2 = s.sph_density(neighbors=True)
+    dp, bp, nbp, nd2p = O.sph_density(p)
+    assert np.array_equal(b, bp)
+    assert np.allclose(d, dp, rtol=1e-13, atol=0)
+    for i in range(p["x"].size):
+        assert set(nbr[i][nd2[i] < b[i]].tolist()) == set(nbp[i][nd2p[i] < bp[i]].tolist()), i
+        assert np.all(nd2[i][nbr[i] >= 0] <= b[i])
