@@ -65,7 +65,7 @@ __device__ __forceinline__ bool drain(const int32_t* buf, int n, Region& r, int3
   return true;
 }
 
-__global__ void __launch_bounds__(kWlWarps * 32, 8) walk_lists(TravParams P, ListParams L, const Mom* __restrict__ mom) {
+__global__ void __launch_bounds__(kWlWarps * 32, 6) walk_lists(TravParams P, ListParams L, const Mom* __restrict__ mom) {
   __shared__ WalkWarp warps[kWlWarps];
   WalkWarp& w = warps[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
@@ -99,6 +99,8 @@ __global__ void __launch_bounds__(kWlWarps * 32, 8) walk_lists(TravParams P, Lis
     if (lane == 0) load_bucket_geom(mom, tnode, w.geom);
     __syncwarp();
     const BucketGeom& g = w.geom;
+    // the bucket box in registers: every classification reads it
+    const double blo[3] = {g.lo[0], g.lo[1], g.lo[2]}, bhi[3] = {g.hi[0], g.hi[1], g.hi[2]};
     const int ntot = P.walk[tnode].pcount;
     const unsigned long long pc0 = rpc.cur, pp0 = rpp.cur;
     unsigned long long opens = 0, nsrc = 0;
@@ -121,7 +123,7 @@ __global__ void __launch_bounds__(kWlWarps * 32, 8) walk_lists(TravParams P, Lis
           atomicOr(P.status, kErrCapacity);
         } else {
           r = P.walk[node];
-          cls = classify_node_gap(r, g, P.ox, P.oy, P.oz, gap2);
+          cls = classify_node_gap(r, blo, bhi, g, P.ox, P.oy, P.oz, gap2);
         }
       }
       opens += (unsigned long long)__popc(__ballot_sync(kFull, node >= 0 && node < P.nnodes &&
@@ -132,7 +134,7 @@ __global__ void __launch_bounds__(kWlWarps * 32, 8) walk_lists(TravParams P, Lis
         // the centre (SPLINEQ's softened branch), with a relative margin.  A
         // quadrupole node's box gap is the one its opening test measured.
         if (cls == kClsP2P)
-          gap2 = box_gap2_exact(g.lo, g.hi, __dadd_rn(r.cm[0], P.ox), __dadd_rn(r.cm[1], P.oy),
+          gap2 = box_gap2_exact(blo, bhi, __dadd_rn(r.cm[0], P.ox), __dadd_rn(r.cm[1], P.oy),
                                 __dadd_rn(r.cm[2], P.oz));
         const double reach = (cls == kClsP2P) ? r.reach + r.soft_max + g.soft_max
                                               : (r.soft + g.soft_max) * (1.0 + 1e-5);

@@ -113,16 +113,22 @@ __device__ __forceinline__ void load_bucket_geom(const Mom* mom, int node, Bucke
 // box gap of the node's centre (plus offset) serves both the opening test and
 // openSoftening's second clause; it is returned in gap2 (-1 where it was not
 // needed: leaves, empty nodes, nodes opened by their count).
-__device__ __forceinline__ int classify_node_gap(const WalkRec& w, const BucketGeom& g, double ox, double oy,
-                                                 double oz, double& gap2) {
+// The same with the bucket box passed apart (lo, hi: e.g. held in registers).
+__device__ __forceinline__ int classify_node_gap(const WalkRec& w, const double lo[3], const double hi[3],
+                                                 const BucketGeom& g, double ox, double oy, double oz, double& gap2) {
   gap2 = -1.0;
   if (w.type == kTypeLeaf) return kClsP2P;
   if (w.type != kTypeInternal) return kClsNone;
   if (w.count <= kMinParticleNode) return kClsOpen;
   const double cx = __dadd_rn(w.cm[0], ox), cy = __dadd_rn(w.cm[1], oy), cz = __dadd_rn(w.cm[2], oz);
-  gap2 = box_gap2_exact(g.lo, g.hi, cx, cy, cz);
+  gap2 = box_gap2_exact(lo, hi, cx, cy, cz);
   if (gap2 <= w.orsq) return kClsOpen;
   return open_softening_gap(cx, cy, cz, w.soft, g.cm[0], g.cm[1], g.cm[2], g.soft, gap2) ? kClsMono : kClsQuad;
+}
+
+__device__ __forceinline__ int classify_node_gap(const WalkRec& w, const BucketGeom& g, double ox, double oy,
+                                                 double oz, double& gap2) {
+  return classify_node_gap(w, g.lo, g.hi, g, ox, oy, oz, gap2);
 }
 
 __device__ __forceinline__ int classify_node(const WalkRec& w, const BucketGeom& g, double ox, double oy, double oz) {
