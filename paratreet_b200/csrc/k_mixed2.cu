@@ -675,7 +675,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2p(TravParams
 }
 
 // ---------------------------------------------------------------- launchers
-int walk_lists_grid(int sms) { return sms * 8; }
+int walk_lists_grid(int sms) { return sms * 6; }  // the CTAs resident at 80 registers
 
 void launch_walk_lists(const TravParams& P, const ListParams& L, const Mom* mom, int grid, cudaStream_t st) {
   note_launch();
