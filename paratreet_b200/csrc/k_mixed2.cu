@@ -65,7 +65,7 @@ __device__ __forceinline__ bool drain(const int32_t* buf, int n, Region& r, int3
   return true;
 }
 
-__global__ void __launch_bounds__(kWlWarps * 32, 6) walk_lists(TravParams P, ListParams L, const Mom* __restrict__ mom) {
+__global__ void __launch_bounds__(kWlWarps * 32, 5) walk_lists(TravParams P, ListParams L, const Mom* __restrict__ mom) {
   __shared__ WalkWarp warps[kWlWarps];
   WalkWarp& w = warps[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
@@ -98,8 +98,8 @@ __global__ void __launch_bounds__(kWlWarps * 32, 6) walk_lists(TravParams P, Lis
     __syncwarp();
     if (lane == 0) load_bucket_geom(mom, tnode, w.geom);
     __syncwarp();
-    const BucketGeom& g = w.geom;
-    // the bucket box in registers: every classification reads it
+    // the bucket geometry in registers: every classification reads it
+    const BucketGeom g = w.geom;
     const double blo[3] = {g.lo[0], g.lo[1], g.lo[2]}, bhi[3] = {g.hi[0], g.hi[1], g.hi[2]};
     const int ntot = P.walk[tnode].pcount;
     const unsigned long long pc0 = rpc.cur, pp0 = rpp.cur;
@@ -675,7 +675,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2p(TravParams
 }
 
 // ---------------------------------------------------------------- launchers
-int walk_lists_grid(int sms) { return sms * 6; }  // the CTAs resident at 80 registers
+int walk_lists_grid(int sms) { return sms * 5; }  // the CTAs resident at 96 registers
 
 void launch_walk_lists(const TravParams& P, const ListParams& L, const Mom* mom, int grid, cudaStream_t st) {
   note_launch();
