@@ -151,6 +151,29 @@ def test_mixed_matches_fp64(gen, n, bucket):
     assert np.sqrt(np.mean(pe ** 2)) < 1e-5
 
 
+@pytest.mark.parametrize("gen,n,bucket", [("plummer", 60000, 32), ("mixture", 40000, 16)])
+def test_mixed_fused_fallback_matches_two_phase(gen, n, bucket, monkeypatch):
+    """The fused walk-and-evaluate kernel (taken when the list pools cannot be
+    allocated; PT_MIXED_FUSED=1 forces it) against the default two-phase
+    traversal: the same interactions, FP32 sums in another order."""
+    p = getattr(ics, gen)(n, seed=5)
+    res = []
+    for fused in ("0", "1"):
+        monkeypatch.setenv("PT_MIXED_FUSED", fused)
+        with sim(max_particles_per_leaf=bucket, precision="mixed") as s:
+            s.set_particles(p)
+            s.start_down()
+            s.start_down()  # a second pass: the two-phase pools are sized by the first
+            res.append((s.accelerations(), s.counters()))
+    (a2, c2), (af, cf) = res
+    assert (c2["n_pp"], c2["n_pc"], c2["n_open"]) == (cf["n_pp"], cf["n_pc"], cf["n_open"])
+    e = rel_err((af["ax"], af["ay"], af["az"]), (a2["ax"], a2["ay"], a2["az"]))
+    assert np.sqrt(np.mean(e ** 2)) < 1e-6
+    assert np.max(e) < 1e-4
+    pe = np.abs(af["pot_full"] - a2["pot_full"]) / np.abs(a2["pot_full"])
+    assert np.sqrt(np.mean(pe ** 2)) < 1e-6
+
+
 def test_direct_sum_matches_oracle():
     p = ics.plummer(6000, seed=9, soft=0.01)
     tgt = np.arange(0, 6000, 7, dtype=np.int32)
