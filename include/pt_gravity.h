@@ -156,7 +156,9 @@ int pt_compute_forces_range(pt_handle* h, int64_t b0, int64_t b1);
 /* Accelerations and potentials of the last force pass, caller order.
  * pot: the reference's potential (quadrupole node() terms only,
  * examples/GravityVisitor.h:218); pot_full: every interaction's potential
- * (P2P spline, quadrupole, monopole).  Any pointer may be NULL. */
+ * (P2P spline, quadrupole, monopole).  The mixed form's fused fallback
+ * (taken only when the interaction-list pools cannot be allocated) leaves
+ * pot at zero.  Any pointer may be NULL. */
 int pt_get_accel(pt_handle* h, double* ax, double* ay, double* az, double* pot, double* pot_full);
 /* Device pointers (sorted order, FP64) of the last force pass, and the
  * sorted-to-caller permutation (int32 order[i] = caller index of sorted i).

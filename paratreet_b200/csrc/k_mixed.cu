@@ -543,7 +543,7 @@ __global__ void __launch_bounds__(kMixWarps * 32, kMinBlocks) traverse_mixed(Tra
           P.p.ax[i] = v[0];
           P.p.ay[i] = v[1];
           P.p.az[i] = v[2];
-          P.p.pot[i] = 0.0;
+          P.p.pot[i] = 0.0;  // this fallback sums P2C and P2P potentials together: pot_full only
           P.p.potf[i] = v[3];
         }
       }

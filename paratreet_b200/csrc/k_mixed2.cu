@@ -259,29 +259,34 @@ struct Kahan4 {
   }
 };
 
-// Sum the G lane groups of each target and store or add the result.
-__device__ __forceinline__ void ev_finish(EvalWarp& w, const Kahan4& K, const EvTarget& x, const TravParams& P,
-                                          int t0, int lane, bool store) {
+// Sum the G lane groups of each target and store or add the result.  P2C
+// (p2c): pot_full gets every node's potential, pot the quadrupole node()
+// terms only (the reference's potential: pmono, the monopole nodes' part, is
+// left out); P2P adds to pot_full only (GravityVisitor::leaf applies none).
+__device__ __forceinline__ void ev_finish(EvalWarp& w, const Kahan4& K, float pmono, const EvTarget& x,
+                                          const TravParams& P, int t0, int lane, bool p2c, bool store) {
   double* red = reinterpret_cast<double*>(&w.st[0][0]);
   __syncwarp();
 #pragma unroll
-  for (int k = 0; k < 4; k++) red[4 * lane + k] = (double)K.s[k] - (double)K.c[k];
+  for (int k = 0; k < 4; k++) red[5 * lane + k] = (double)K.s[k] - (double)K.c[k];
+  red[5 * lane + 4] = (double)pmono;
   __syncwarp();
   if (lane < x.nt) {
-    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     for (int gg = 0; gg < x.G; gg++)
-      for (int k = 0; k < 4; k++) v[k] += red[4 * (gg * x.nt + lane) + k];
+      for (int k = 0; k < 5; k++) v[k] += red[5 * (gg * x.nt + lane) + k];
     const int i = t0 + lane;
     if (store) {
       P.p.ax[i] = v[0];
       P.p.ay[i] = v[1];
       P.p.az[i] = v[2];
-      P.p.pot[i] = 0.0;
+      P.p.pot[i] = p2c ? v[3] - v[4] : 0.0;
       P.p.potf[i] = v[3];
     } else {
       P.p.ax[i] += v[0];
       P.p.ay[i] += v[1];
       P.p.az[i] += v[2];
+      if (p2c) P.p.pot[i] += v[3] - v[4];
       P.p.potf[i] += v[3];
     }
   }
@@ -309,11 +314,18 @@ __device__ __forceinline__ float4 node_offset(const WalkRec* __restrict__ walk, 
                      (float)((c2 + P.oz) - g.cm[2]), 0.f);
 }
 
-// Both terms of a staged node pair in scalar form (the rare softened case).
-__device__ __noinline__ float4 ev_p2c_pair_scalar(const EvalWarp& w, int k, float tx, float ty, float tz, float ts) {
+struct P2cPair {
+  float ax, ay, az, pf;  // both nodes' terms
+  float pm;              // the potential of the monopole nodes among them
+};
+
+// Both terms of a staged node pair in scalar form (the rare softened and
+// monopole cases; a monopole node carries NaN softening).
+__device__ __noinline__ P2cPair ev_p2c_pair_scalar(const EvalWarp& w, int k, float tx, float ty, float tz,
+                                                   float ts) {
   const float4 P0 = w.st[0][k], P1 = w.st[1][k], P2 = w.st[2][k], P3 = w.st[3][k], P4 = w.st[4][k],
                P5 = w.st[5][k];
-  float ax = 0.f, ay = 0.f, az = 0.f, pf = 0.f;
+  float ax = 0.f, ay = 0.f, az = 0.f, pf = 0.f, pm = 0.f;
   // rows: (ox, oy, oz, M), (xx, xy, xz, yy), (yz, zz, soft, half trace)
   const float4 t[2][3] = {{make_float4(P0.x, P0.z, P1.x, P1.z), make_float4(P2.x, P2.z, P3.x, P3.z),
                            make_float4(P4.x, P4.z, P5.z, fabsf(P5.x))},
@@ -332,12 +344,14 @@ __device__ __noinline__ float4 ev_p2c_pair_scalar(const EvalWarp& w, int k, floa
     const float qz = B.z * rx + Cc.x * ry + Cc.y * rz;
     const float qir = 0.5f * (qx * rx + qy * ry + qz * rz);
     const float qir3 = b * A.w + d * qir - c * Cc.w;
-    pf += -A.w * a - c * qir + b * Cc.w;
+    const float pt = -A.w * a - c * qir + b * Cc.w;
+    pf += pt;
+    if (isnan(Cc.z)) pm += pt;
     ax += -qir3 * rx + c * qx;
     ay += -qir3 * ry + c * qy;
     az += -qir3 * rz + c * qz;
   }
-  return make_float4(ax, ay, az, pf);
+  return P2cPair{ax, ay, az, pf, pm};
 }
 
 // The staged node pairs k = grp, grp + G, ... of one chunk against this
@@ -347,17 +361,18 @@ __device__ __noinline__ float4 ev_p2c_pair_scalar(const EvalWarp& w, int k, floa
 // slower: the second copy costs registers.)
 __device__ __forceinline__ void ev_p2c_pairs(const EvalWarp& w, const EvTarget& x, int npair, float2 ntx, float2 nty,
                                              float2 ntz, float2& ax2, float2& ay2, float2& az2, float2& pp2,
-                                             float2& mm2) {
+                                             float2& mm2, float& pmono) {
   const float2 mthree = make_float2(-3.f, -3.f), mfive = make_float2(-5.f, -5.f), half = make_float2(0.5f, 0.5f);
   const float4* sp = &w.st[0][x.grp];  // rows st[1..5] follow at +32 each
   for (int k = x.grp; k < npair; k += x.G, sp += x.G) {
     const float4 P5 = sp[160];
-    if ((__float_as_int(P5.x) | __float_as_int(P5.y)) < 0) {  // a near node: scalar, softening tested
-      const float4 v = ev_p2c_pair_scalar(w, k, x.tx, x.ty, x.tz, x.ts);
-      ax2.x += v.x;
-      ay2.x += v.y;
-      az2.x += v.z;
-      pp2.x += v.w;
+    if ((__float_as_int(P5.x) | __float_as_int(P5.y)) < 0) {  // a near or monopole node: scalar
+      const P2cPair v = ev_p2c_pair_scalar(w, k, x.tx, x.ty, x.tz, x.ts);
+      ax2.x += v.ax;
+      ay2.x += v.ay;
+      az2.x += v.az;
+      pp2.x += v.pf;
+      pmono += v.pm;
       continue;
     }
     const float4 P0 = sp[0], P1 = sp[32];
@@ -418,6 +433,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams
       K.zero();
       // plain packed sums over four chunks, then one compensated add
       float2 ax2 = make_float2(0.f, 0.f), ay2 = ax2, az2 = ax2, pp2 = ax2, mm2 = ax2;
+      float pmono = 0.f;  // the monopole nodes' potential (left out of pot)
       // list entries of the coming chunk, loaded a chunk ahead so that only
       // the node records wait at staging time
       int en0 = (2 * lane < count) ? L.pc_pool[start + 2 * lane] : 0;
@@ -431,7 +447,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams
         }
         // stage this lane's two nodes as a pair
         float4 o[2], r0[2], r1[2];
-        bool near[2] = {false, false};
+        bool near[2] = {false, false}, mono[2] = {false, false};
 #pragma unroll
         for (int h = 0; h < 2; h++) {
           const int q = cs + 2 * lane + h;
@@ -446,6 +462,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams
             o[h] = node_offset(P.walk, node, P, w.geom);
             r0[h] = rec[0];  // mass, soft, xx, xy
             r1[h] = rec[1];  // xz, yy, yz, zz
+            mono[h] = e < 0;
             if (e < 0) {     // monopole: no second moments, NaN softening (never softened)
               r0[h] = make_float4(r0[h].x, qnan, 0.f, 0.f);
               r1[h] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -460,11 +477,12 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams
         w.st[4][lane] = make_float4(r1[0].z, r1[1].z, r1[0].w, r1[1].w);
         {  // (tr_a, tr_b, soft_a, soft_b); a near node carries its half trace negated
           const float tra = 0.5f * (r0[0].z + r1[0].y + r1[0].w), trb = 0.5f * (r0[1].z + r1[1].y + r1[1].w);
-          w.st[5][lane] = make_float4(near[0] ? -tra : tra, near[1] ? -trb : trb, r0[0].y, r0[1].y);
+          w.st[5][lane] = make_float4((near[0] || mono[0]) ? -tra : tra, (near[1] || mono[1]) ? -trb : trb,
+                                      r0[0].y, r0[1].y);
         }
         __syncwarp();
         const int npair = (min(64, count - cs) + 1) >> 1;
-        if (x.grp < x.G) ev_p2c_pairs(w, x, npair, ntx, nty, ntz, ax2, ay2, az2, pp2, mm2);
+        if (x.grp < x.G) ev_p2c_pairs(w, x, npair, ntx, nty, ntz, ax2, ay2, az2, pp2, mm2, pmono);
         if (((cs >> 6) & 3) == 3 || cs + 64 >= count) {
           K.add(0, ax2.x + ax2.y);
           K.add(1, ay2.x + ay2.y);
@@ -473,7 +491,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams
           ax2 = ay2 = az2 = pp2 = mm2 = make_float2(0.f, 0.f);
         }
       }
-      ev_finish(w, K, x, P, t0, lane, P.accumulate == 0);
+      ev_finish(w, K, pmono, x, P, t0, lane, true, P.accumulate == 0);
     }
   }
 }
@@ -669,7 +687,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2p(TravParams
           }
         }
       }
-      ev_finish(w, K, x, P, t0, lane, false);
+      ev_finish(w, K, 0.f, x, P, t0, lane, false, false);
     }
   }
 }

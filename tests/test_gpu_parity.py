@@ -149,6 +149,10 @@ def test_mixed_matches_fp64(gen, n, bucket):
     assert np.max(e) < 1e-3
     pe = np.abs(am["pot_full"] - a64["pot_full"]) / np.abs(a64["pot_full"])
     assert np.sqrt(np.mean(pe ** 2)) < 1e-5
+    # the reference's potential: quadrupole node() terms only (monopole nodes
+    # and leaves apply none), measured against the full potential's size
+    qe = np.abs(am["pot"] - a64["pot"]) / np.abs(a64["pot_full"])
+    assert np.sqrt(np.mean(qe ** 2)) < 1e-5 and np.max(qe) < 1e-3
 
 
 @pytest.mark.parametrize("gen,n,bucket", [("plummer", 60000, 32), ("mixture", 40000, 16)])
