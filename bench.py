@@ -237,7 +237,7 @@ def main():
     sim.set_particles(p)
     if a.sph:
         out = {"workload": workload_config(a, world)["workload"], "sph_density": sph_density_rate(a, sim, stream),
-               "sph_pressure": sph_pressure_rate(a, sim, stream)}
+               "sph_pressure": sph_pressure_rate(a, sim, stream), "sph_step": sph_step_rate(a, sim, stream)}
         if rank == 0:
             print(json.dumps(out))
         return
@@ -383,6 +383,24 @@ def sph_pressure_rate(a, sim, stream):
     sim.start_down()
     return {"particles_per_s": a.n / float(np.mean(ts)), "ms_per_pass": 1e3 * float(np.mean(ts)),
             "neighbours": 32, "note": "density pass + pressure pass of the SPH example, host in and out"}
+
+
+def sph_step_rate(a, sim, stream):
+    """Iterations of the SPH example (pt_sph_step: density pass, pressure
+    pass, kick + perturb with the internal-energy updates, dt = 0.01) on the
+    same particles, seeded internal energies; the SPH state goes in and out
+    through host memory once per call.  Moves the particles: run it last."""
+    import torch
+    u = np.random.default_rng(17).uniform(0.5, 1.5, a.n)
+    u, up, vp = sim.sph_run(1, u)
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    sim.sph_run(2, u, up, vp)
+    s1.record(stream)
+    torch.cuda.synchronize()
+    t = s0.elapsed_time(s1) / 1e3 / 2
+    return {"particles_per_s": a.n / t, "ms_per_step": 1e3 * t, "neighbours": 32,
+            "note": "SPH example iteration: tree build + kNN + density + pressure + kick/perturb"}
 
 
 def phase_rooflines(c, n, peaks):

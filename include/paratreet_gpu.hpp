@@ -183,6 +183,20 @@ class Gravity {
     return s;
   }
 
+  // The SPH example's Driver::run: iterations of the density pass, the
+  // pressure pass and Particle::kick / perturb with the internal-energy
+  // updates (dt = max_timestep).  The SPH fields of every particle in caller
+  // order; start u_pred = u and v_pred = the velocities (src/Reader.C:90-91).
+  struct SphState {
+    std::vector<double> u, u_pred, vpx, vpy, vpz;
+  };
+  void sph_run(int iterations, SphState& s) {
+    for (auto* v : {&s.u, &s.u_pred, &s.vpx, &s.vpy, &s.vpz})
+      if (v->size() != n_) throw Error(PT_E_ARG, "one SPH state value per particle");
+    check(pt_sph_step(h_, iterations, s.u.data(), s.u_pred.data(), s.vpx.data(), s.vpy.data(), s.vpz.data()),
+          "pt_sph_step");
+  }
+
   pt_counters counters() const {
     pt_counters c;
     check(pt_get_counters(h_, &c), "pt_get_counters");

@@ -261,6 +261,21 @@ int pt_sph_density(pt_handle* h, double* density, double* ball_sq, int32_t* nbr,
 int pt_sph_pressure(pt_handle* h, const double* u, double* density, double* ax, double* ay, double* az,
                     double* pdv);
 
+/* SPH step ------------------------------------------------------------------
+ * nsteps iterations of the SPH example's Driver::run loop (src/Driver.h:
+ * 183-251 with examples/SPH.C:74-111): tree build, the density pass, the
+ * pressure pass (as pt_sph_pressure, reading u_pred as u_predicted and
+ * vpx/vpy/vpz as velocity_predicted), then Particle::kick and
+ * Particle::perturb with their SPH updates (src/Particle.C:7-21):
+ * v += a dt/2 twice, v_pred = v + a dt, x += v dt, u -= PdV 0.5e-7 dt,
+ * u_pred = u - PdV 0.5e-7 dt.  dt = config.dt_max (the SPH example's
+ * getTimestep returns max_timestep).  u, u_pred and v_pred are in/out host
+ * arrays in caller order (start them as u and the velocities, as
+ * src/Reader.C:90-91 does); positions and velocities stay in the handle
+ * (pt_get_state).  FP64; the pressure pass's reactions are atomic adds, so
+ * trajectories match the reference to rounding, not bit for bit. */
+int pt_sph_step(pt_handle* h, int nsteps, double* u, double* u_pred, double* vpx, double* vpy, double* vpz);
+
 /* FP64 direct sum (the force-error yardstick) ------------------------------
  * Isolated spline-softened sum over all particles for nt caller indices,
  * the kernel of examples/GravityVisitor.h:87-120 with twoh = soft_i + soft_j. */

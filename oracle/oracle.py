@@ -92,6 +92,7 @@ def _ref_lib():
         lib.ptref_dual.argtypes = [C.c_void_p, _dp, _dp, _dp, _u64p]
         lib.ptref_sph_pressure.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, _dp]
         lib.ptref_sph_density.argtypes = [C.c_void_p, _dp, _dp, _i32p, _dp]
+        lib.ptref_sph_step.argtypes = [C.c_void_p, C.c_int] + [_dp] * 5
         _ref = lib
     return _ref
 
@@ -253,6 +254,15 @@ class RefSim(_Sim):
         self._lib.ptref_sph_pressure(self._h, np.ascontiguousarray(u, dtype=np.float64), *out)
         return out
 
+    def sph_step(self, nsteps, u, u_pred, v_pred):
+        """nsteps iterations of the reference's SPH example (density pass,
+        pressure pass, Particle::kick / perturb with dt = dt_max): returns the
+        SPH state (u, u_pred, (vpx, vpy, vpz)) in caller order; positions and
+        velocities through state()."""
+        st = [np.array(a, dtype=np.float64, copy=True) for a in [u, u_pred] + list(v_pred)]
+        self._lib.ptref_sph_step(self._h, int(nsteps), *st)
+        return st[0], st[1], tuple(st[2:])
+
     def forces(self, record_lists=False):
         self._lib.ptref_set_record_lists(self._h, 1 if record_lists else 0)
         self._lib.ptref_run(self._h, 0)
@@ -316,6 +326,34 @@ def sph_pressure(p: dict, u, density, ballsq, nbr, nd2):
                          np.ascontiguousarray(density), np.ascontiguousarray(ballsq),
                          np.ascontiguousarray(nbr, dtype=np.int32).ravel(), np.ascontiguousarray(nd2).ravel(), k, *out)
     return out
+
+
+def sph_step(p: dict, nsteps: int, dt: float, u, u_pred, v_pred, threads: int = 1):
+    """nsteps iterations of the SPH example on the C restatement: the density
+    and pressure passes above (the pressure pass reading u_pred and v_pred as
+    u_predicted and velocity_predicted), then Particle::kick and
+    Particle::perturb (src/Particle.C:7-21) elementwise in FP64 with the
+    reference's association.  Returns (particles, u, u_pred, (vpx, vpy, vpz))
+    in caller order."""
+    q = {k: np.array(v, copy=True) for k, v in p.items()}
+    u = np.array(u, dtype=np.float64, copy=True)
+    up = np.array(u_pred, dtype=np.float64, copy=True)
+    vp = [np.array(v, dtype=np.float64, copy=True) for v in v_pred]
+    for _ in range(nsteps):
+        dens, ball, nbr, nd2 = sph_density(q, threads=threads)
+        pv = dict(q, vx=vp[0], vy=vp[1], vz=vp[2])
+        acc = sph_pressure(pv, up, dens, ball, nbr, nd2)
+        for d, (xk, vk) in enumerate((("x", "vx"), ("y", "vy"), ("z", "vz"))):
+            a = acc[d]
+            v = q[vk] + a * dt / 2      # kick
+            v = v + (a * dt / 2)         # perturb
+            vp[d] = v + (a * dt)
+            q[xk] = q[xk] + (v * dt)
+            q[vk] = v
+        u_delta = 0.5e-7 * dt
+        u = u - acc[3] * u_delta
+        up = u - acc[3] * u_delta
+    return q, u, up, tuple(vp)
 
 
 def sort_tree(t: Tree) -> Tree:

@@ -516,11 +516,28 @@ void sph_density(RefSim& s, double* density, double* ballsq, int* nbr, double* n
 // neighbour, examples/SPHUtils.h:64-133), and the opposing effects applied
 // afterwards.  Needs sph_density first.  u: internal energy (caller order),
 // used as u_predicted; velocity_predicted = velocity.  Outputs in caller order.
+void sph_pressure_pass(RefSim& s);
+
 void sph_pressure(RefSim& s, const double* u, double* ax, double* ay, double* az, double* pdv) {
-  const size_t n = s.particles.size(), nb = s.leaves.size();
   for (auto& p : s.particles) {
     p.u = p.u_predicted = u[p.order];
     p.velocity_predicted = p.velocity;
+  }
+  sph_pressure_pass(s);
+  for (auto& p : s.particles) {
+    ax[p.order] = p.acceleration.x;
+    ay[p.order] = p.acceleration.y;
+    az[p.order] = p.acceleration.z;
+    pdv[p.order] = p.pressure_dVolume;
+  }
+}
+
+// The pressure pass on the particles' own u_predicted and velocity_predicted:
+// accelerations and PdV work start at zero and end with the opposing effects
+// added (ThreadStateHolder::applyAccumulatedOpposingEffects).
+void sph_pressure_pass(RefSim& s) {
+  const size_t n = s.particles.size(), nb = s.leaves.size();
+  for (auto& p : s.particles) {
     p.acceleration = Vector3D<Real>(0.0);
     p.pressure_dVolume = 0.0;
   }
@@ -569,10 +586,48 @@ void sph_pressure(RefSim& s, const double* u, double* ax, double* ay, double* az
     }
   }
   for (auto& p : s.particles) {  // applyAccumulatedOpposingEffects
-    ax[p.order] = p.acceleration.x + tls.acc[p.order].x;
-    ay[p.order] = p.acceleration.y + tls.acc[p.order].y;
-    az[p.order] = p.acceleration.z + tls.acc[p.order].z;
-    pdv[p.order] = p.pressure_dVolume + tls.work[p.order];
+    p.acceleration.x = p.acceleration.x + tls.acc[p.order].x;
+    p.acceleration.y = p.acceleration.y + tls.acc[p.order].y;
+    p.acceleration.z = p.acceleration.z + tls.acc[p.order].z;
+    p.pressure_dVolume = p.pressure_dVolume + tls.work[p.order];
+  }
+}
+
+// nsteps iterations of the SPH example's Driver::run (src/Driver.h:183-251
+// with examples/SPH.C:74-111): tree build and density pass, the pressure pass
+// on the particles' u_predicted / velocity_predicted, then the reference's
+// Particle::kick and Particle::perturb (src/Particle.C:7-21) with dt =
+// max_timestep, the universe remade from the drifted positions and the keys
+// reassigned.  SPH state in and out in caller order.
+void sph_step(RefSim& s, int nsteps, double* u, double* u_pred, double* vpx, double* vpy, double* vpz) {
+  const size_t n = s.particles.size();
+  for (auto& p : s.particles) {
+    p.u = u[p.order];
+    p.u_predicted = u_pred[p.order];
+    p.velocity_predicted = Vector3D<Real>(vpx[p.order], vpy[p.order], vpz[p.order]);
+  }
+  std::vector<double> d(n), b(n), nd2(n * 32);
+  std::vector<int> nbr(n * 32);
+  for (int it = 0; it < nsteps; it++) {
+    sph_density(s, d.data(), b.data(), nbr.data(), nd2.data(), 32);
+    sph_pressure_pass(s);
+    const Real dt = s.dt_max;
+    s.last_dt = dt;
+    for (auto& p : s.particles) p.kick(dt);
+    OrientedBox<Real> box;
+    for (auto& p : s.particles) {
+      p.perturb(dt);
+      box.grow(p.position);
+    }
+    remakeUniverse(s, box);
+    assignKeys(s);
+  }
+  for (auto& p : s.particles) {
+    u[p.order] = p.u;
+    u_pred[p.order] = p.u_predicted;
+    vpx[p.order] = p.velocity_predicted.x;
+    vpy[p.order] = p.velocity_predicted.y;
+    vpz[p.order] = p.velocity_predicted.z;
   }
 }
 
@@ -756,6 +811,12 @@ int ptref_dual(void* h, double* ax, double* ay, double* az, unsigned long long* 
 
 /* 1: Partition::startBasicDown (breadth first per bucket), 0: startDown. */
 void ptref_set_traversal(void* h, int basic_down) { ((RefSim*)h)->basic_down = basic_down; }
+
+/* nsteps iterations of the SPH example; SPH state in/out in caller order. */
+int ptref_sph_step(void* h, int nsteps, double* u, double* u_pred, double* vpx, double* vpy, double* vpz) {
+  sph_step(*(RefSim*)h, nsteps, u, u_pred, vpx, vpy, vpz);
+  return 0;
+}
 
 /* SPH pressure pass after ptref_sph_density (same particles). */
 int ptref_sph_pressure(void* h, const double* u, double* ax, double* ay, double* az, double* pdv) {

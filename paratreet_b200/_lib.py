@@ -104,6 +104,7 @@ SIGNATURES = {
     "pt_advance": (C.c_int, [_vp, _vp]),
     "pt_sph_density": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "pt_sph_pressure": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "pt_sph_step": (C.c_int, [_vp, C.c_int] + [_vp] * 5),
     "pt_get_bucket_work": (C.c_int, [_vp, _vp]),
     "pt_forces_frozen": (C.c_int, [_vp] + [_vp] * 4),
     "pt_adjoint": (C.c_int, [_vp] + [_vp] * 7),

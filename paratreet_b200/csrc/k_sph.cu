@@ -488,7 +488,56 @@ __global__ void __launch_bounds__(256) sph_pressure_kernel(Particles p, const do
   }
 }
 
+// The SPH example's integration after its pressure pass: Particle::kick then
+// Particle::perturb (src/Particle.C:7-21) with the SPH fields.  Particle i is
+// in sorted order (accelerations, PdV work, positions, velocities); u, u_pred
+// and the predicted velocities are kept in caller order and reached through
+// p.order.  Same association as the reference: (a dt) / 2, a dt, v dt,
+// PdV (0.5e-7 dt); this file is compiled without FMA contraction.
+__global__ void __launch_bounds__(256) sph_kick_perturb_kernel(Particles p, const double* __restrict__ ax,
+                                                               const double* __restrict__ ay,
+                                                               const double* __restrict__ az,
+                                                               const double* __restrict__ pdv, double* __restrict__ u,
+                                                               double* __restrict__ u_pred, double* __restrict__ vpx,
+                                                               double* __restrict__ vpy, double* __restrict__ vpz,
+                                                               int64_t n, double dt) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = p.order[i];
+    const double a[3] = {ax[i], ay[i], az[i]};
+    double v[3] = {p.vx[i], p.vy[i], p.vz[i]};
+    double vp[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      v[d] += a[d] * dt / 2;    // kick
+      v[d] += (a[d] * dt / 2);  // perturb
+      vp[d] = v[d] + (a[d] * dt);
+    }
+    p.x[i] += (v[0] * dt);
+    p.y[i] += (v[1] * dt);
+    p.z[i] += (v[2] * dt);
+    p.vx[i] = v[0];
+    p.vy[i] = v[1];
+    p.vz[i] = v[2];
+    vpx[c] = vp[0];
+    vpy[c] = vp[1];
+    vpz[c] = vp[2];
+    const double uDelta = 0.5e-7 * dt;
+    const double w = pdv[i];
+    const double uc = u[c] - w * uDelta;
+    u[c] = uc;
+    u_pred[c] = uc - w * uDelta;
+  }
+}
+
 int sph_k() { return kSphK; }
+
+void launch_sph_kick_perturb(Particles p, const double* ax, const double* ay, const double* az, const double* pdv,
+                             double* u, double* u_pred, double* vpx, double* vpy, double* vpz, int64_t n, double dt,
+                             int grid, cudaStream_t st) {
+  if (n <= 0) return;
+  note_launch();
+  sph_kick_perturb_kernel<<<grid, 256, 0, st>>>(p, ax, ay, az, pdv, u, u_pred, vpx, vpy, vpz, n, dt);
+}
 
 void launch_sph_pressure(Particles p, const double* density, const double* ballsq, const double* u,
                          const int32_t* nbr, const double* nd2, int64_t n, double* ax, double* ay, double* az,

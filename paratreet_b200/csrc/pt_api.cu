@@ -87,6 +87,8 @@ struct pt_handle {
   double* sph_list_d = nullptr;  // neighbour-search scratch: per-warp lists
   int32_t* sph_list_i = nullptr;
   int64_t sph_list_cap = 0;
+  double* sph_state = nullptr;  // SPH step: u, u_pred, v_pred (caller order, 5 N), sorted v_pred (3 N)
+  int64_t sph_state_cap = 0;
 
   double4* d_htab = nullptr;  // Ewald reciprocal table (h vector, hCfac)
   int htab_cap = 0;
@@ -800,7 +802,7 @@ int pt_destroy(pt_handle* h) {
   dfree(o.fifo); dfree(o.nleaf_sub); dfree(o.nempty_sub); dfree(o.leaf_base); dfree(o.empty_base);
   dfree(h->flags); dfree(h->buckets); dfree(h->bucket_work); dfree(h->list_count); dfree(h->list_off); dfree(h->list_node);
   dfree(h->list_kind); dfree(h->dsum); dfree(h->adj); dfree(h->nadj); dfree(h->d_htab); dfree(h->ewd); dfree(h->sph); dfree(h->sph_nbr); dfree(h->sph_nd2);
-  dfree(h->sph_list_d); dfree(h->sph_list_i);
+  dfree(h->sph_list_d); dfree(h->sph_list_i); dfree(h->sph_state);
   dfree(h->pool_pc); dfree(h->pool_pp); dfree(h->l_pc_start); dfree(h->l_pp_start); dfree(h->l_pc_count);
   dfree(h->l_pp_count); dfree(h->d_lcur); dfree(h->d_work3);
   for (auto& e : h->ev)
@@ -993,6 +995,54 @@ int pt_sph_pressure(pt_handle* h, const double* u, double* density, double* ax, 
     CKR(unpermute_f64(h, src[i], dst[i]));
     CK(cudaStreamSynchronize(st));
   }
+  return PT_OK;
+}
+
+// nsteps iterations of the SPH example: density pass, pressure pass with the
+// predicted energies and velocities, then kick + perturb with the SPH updates.
+// dt = max_timestep (examples/SPH.C getTimestep).  The caller-order state
+// (u, u_pred, v_pred) stays on the device across the steps; the sorted copies
+// the pressure pass reads are gathered by p.order after each re-sort.
+int pt_sph_step(pt_handle* h, int nsteps, double* u, double* u_pred, double* vpx, double* vpy, double* vpz) {
+  if (!h || nsteps < 0 || !u || !u_pred || !vpx || !vpy || !vpz) return PT_E_ARG;
+  if (!h->p.x) return fail(h, PT_E_STATE, "no particles");
+  if (!(h->cfg.dt_max > 0.0)) return fail(h, PT_E_ARG, "dt_max must be positive");
+  cudaSetDevice(h->cfg.device);
+  cudaStream_t st = h->stream;
+  const int64_t n = h->n;
+  if (n == 0 || nsteps == 0) return PT_OK;
+  if (8 * n > h->sph_state_cap) {
+    CKR(dalloc(h, &h->sph_state, 8 * n));
+    h->sph_state_cap = 8 * n;
+  }
+  double* cs = h->sph_state;  // caller order: u, u_pred, vpx, vpy, vpz
+  double* vps = cs + 5 * n;   // sorted v_pred
+  double* in[5] = {u, u_pred, vpx, vpy, vpz};
+  for (int k = 0; k < 5; k++) CK(cudaMemcpyAsync(cs + k * n, in[k], n * sizeof(double), cudaMemcpyHostToDevice, st));
+  const int g = grid_for(h, n);
+  const double dt = h->cfg.dt_max;
+  for (int s = 0; s < nsteps; s++) {
+    CKR(sph_density_device(h, true));  // re-sorts the particles, builds the tree, density + neighbours
+    double* us = h->sph + 2 * n;
+    double* out = h->sph + 3 * n;  // ax, ay, az, PdV
+    launch_gather_by_order(cs + n, us, h->p.order, n, g, st);
+    for (int d = 0; d < 3; d++) launch_gather_by_order(cs + (2 + d) * n, vps + d * n, h->p.order, n, g, st);
+    CK(cudaMemsetAsync(out, 0, 4 * n * sizeof(double), st));
+    Particles q = h->p;  // the pressure pass reads velocity_predicted
+    q.vx = vps;
+    q.vy = vps + n;
+    q.vz = vps + 2 * n;
+    launch_sph_pressure(q, h->sph, h->sph + n, us, h->sph_nbr, h->sph_nd2, n, out, out + n, out + 2 * n,
+                        out + 3 * n, h->d_status, h->sms * 16, st);
+    launch_sph_kick_perturb(h->p, out, out + n, out + 2 * n, out + 3 * n, cs, cs + n, cs + 2 * n, cs + 3 * n,
+                            cs + 4 * n, n, dt, g, st);
+    CK(cudaGetLastError());
+    CKR(read_status(h));
+    h->last_dt = dt;
+  }
+  double* outs[5] = {u, u_pred, vpx, vpy, vpz};
+  for (int k = 0; k < 5; k++) CK(cudaMemcpyAsync(outs[k], cs + k * n, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
   return PT_OK;
 }
 

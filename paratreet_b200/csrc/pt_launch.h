@@ -79,6 +79,9 @@ int sph_k();
 void launch_sph_pressure(Particles p, const double* density, const double* ballsq, const double* u,
                          const int32_t* nbr, const double* nd2, int64_t n, double* ax, double* ay, double* az,
                          double* pdv, unsigned* status, int grid, cudaStream_t st);
+void launch_sph_kick_perturb(Particles p, const double* ax, const double* ay, const double* az, const double* pdv,
+                             double* u, double* u_pred, double* vpx, double* vpy, double* vpz, int64_t n, double dt,
+                             int grid, cudaStream_t st);
 int sph_knn_slots(int grid);
 void launch_sph_density(Particles p, int64_t n, const Mom* mom, const WalkRec* walk, const int32_t* buckets,
                         int64_t nbuckets, int64_t nnodes, double* density, double* ballsq, int32_t* nbr, double* nd2,

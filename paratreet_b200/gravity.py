@@ -286,6 +286,26 @@ class GravitySimulation:
         self._check(self._lib.pt_sph_pressure(self._h, L.ptr(uu), *[L.ptr(o) for o in out]))
         return tuple(out)
 
+    def sph_run(self, iterations: int, u, u_pred=None, v_pred=None):
+        """Iterations of the SPH example (density pass, pressure pass, kick and
+        perturb with the internal-energy updates; dt = max_timestep).  u,
+        u_pred (default u) and v_pred (3 arrays, default the current
+        velocities) are the particles' SPH state in caller order; returns the
+        updated (u, u_pred, (vpx, vpy, vpz)).  Positions and velocities stay in
+        the simulation (state())."""
+        n = self.n
+        uu = np.array(u, dtype=np.float64, copy=True)
+        up = uu.copy() if u_pred is None else np.array(u_pred, dtype=np.float64, copy=True)
+        if v_pred is None:
+            st = self.state()
+            vp = [st["vx"].copy(), st["vy"].copy(), st["vz"].copy()]
+        else:
+            vp = [np.array(v, dtype=np.float64, copy=True) for v in v_pred]
+        if any(a.shape != (n,) for a in [uu, up] + vp):
+            raise ValueError("u, u_pred and each v_pred component must hold one value per particle")
+        self._check(self._lib.pt_sph_step(self._h, int(iterations), L.ptr(uu), L.ptr(up), *[L.ptr(v) for v in vp]))
+        return uu, up, tuple(vp)
+
     def direct_sum(self, targets):
         t = np.ascontiguousarray(targets, dtype=np.int32)
         out = [np.empty(t.size) for _ in range(4)]

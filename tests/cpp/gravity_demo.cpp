@@ -10,6 +10,10 @@
 //                                                    (u = 1 + i mod 7 / 10), one
 //                                                    line per particle: density
 //                                                    ax ay az pdv
+//   gravity_demo sphsteps in.tipsy out.txt bucket dt n
+//                                                    n SPH iterations (same u),
+//                                                    one line per particle: x y z
+//                                                    vx vy vz u u_pred
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -68,6 +72,28 @@ int main(int argc, char** argv) {
       if (!f) throw Error(PT_E_ARG, "cannot open output");
       for (size_t i = 0; i < u.size(); i++)
         std::fprintf(f, "%.17g %.17g %.17g %.17g %.17g\n", s.density[i], s.ax[i], s.ay[i], s.az[i], s.pdv[i]);
+      std::fclose(f);
+      return 0;
+    }
+    if (mode == "sphsteps" && argc > 6) {
+      conf.max_particles_per_leaf = std::atoi(argv[4]);
+      conf.max_timestep = std::atof(argv[5]);
+      Gravity g(conf);
+      g.load(p);
+      Gravity::SphState s;
+      s.u.resize(p.size());
+      for (size_t i = 0; i < p.size(); i++) s.u[i] = 1.0 + (double)(i % 7) / 10.0;
+      s.u_pred = s.u;  // src/Reader.C:90-91
+      s.vpx = p.vx;
+      s.vpy = p.vy;
+      s.vpz = p.vz;
+      g.sph_run(std::atoi(argv[6]), s);
+      g.state(p);
+      FILE* f = std::fopen(argv[3], "w");
+      if (!f) throw Error(PT_E_ARG, "cannot open output");
+      for (size_t i = 0; i < p.size(); i++)
+        std::fprintf(f, "%.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g\n", p.x[i], p.y[i], p.z[i], p.vx[i],
+                     p.vy[i], p.vz[i], s.u[i], s.u_pred[i]);
       std::fclose(f);
       return 0;
     }

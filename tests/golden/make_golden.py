@@ -35,6 +35,13 @@ sph_<case>.json
     doSPHCalc of examples/SPHUtils.h, the opposing effects added after it)
     for seeded internal energies u: sampled pressure accelerations and PdV
     work, and their L1 norms (summation order again decides the last bits).
+sphstep_<case>.json
+    Iterations of the reference's SPH example (the density and pressure
+    passes above, then the reference's own Particle::kick and
+    Particle::perturb of src/Particle.C with dt = max_timestep) from seeded
+    velocities and internal energies: sampled positions, velocities,
+    predicted velocities, u and u_predicted after the last step, with their
+    scales (the pressure pass's summation order decides the last bits).
 periodic_<case>.json
     The same sources in periodic mode (examples/Gravity.C replica walks plus
     the Ewald correction of examples/Ewald.{h,C}) on a displaced lattice:
@@ -80,6 +87,11 @@ BASIC_CASES = {
 SPH_CASES = {
     "plummer_4k": (ics.plummer, dict(n=4096, seed=9, soft=0.01), 16),
     "mixture_8k": (ics.mixture, dict(n=8192, seed=2, soft=1e-4), 32),
+}
+
+# name -> (generator, kwargs, bucket, dt, steps)
+SPH_STEP_CASES = {
+    "plummer_3k": (ics.plummer, dict(n=3000, seed=4, soft=0.01), 16, 0.01, 3),
 }
 
 # name -> (lattice kwargs, bucket, theta, n_replicas)
@@ -218,6 +230,40 @@ def run_sph_case(name):
     print(name, p["x"].size)
 
 
+def sph_step_inputs(p):
+    """Seeded velocities (the generator's plus N(0, 0.3)) and internal
+    energies of the SPH step goldens."""
+    n = p["x"].size
+    rng = np.random.default_rng(8)
+    q = dict(p)
+    for k in ("vx", "vy", "vz"):
+        q[k] = p[k] + rng.normal(0.0, 0.3, n)
+    return q, rng.uniform(0.2, 2.0, n)
+
+
+def run_sph_step_case(name):
+    gen, kw, bucket, dt, steps = SPH_STEP_CASES[name]
+    p, u = sph_step_inputs(gen(**kw))
+    n = p["x"].size
+    r = O.RefSim(p, bucket=bucket, dt_max=dt, threads=1)
+    ru, rup, rvp = r.sph_step(steps, u, u.copy(), (p["vx"], p["vy"], p["vz"]))
+    x, y, z, vx, vy, vz = r.state()
+    idx = sorted(int(i) for i in np.random.default_rng(5).choice(n, 32, replace=False))
+    arrs = {"x": x, "y": y, "z": z, "vx": vx, "vy": vy, "vz": vz, "u": ru, "u_pred": rup,
+            "vpx": rvp[0], "vpy": rvp[1], "vpz": rvp[2]}
+    out = {
+        "case": name, "generator": gen.__name__, "kwargs": kw, "bucket": bucket, "dt": dt, "steps": steps,
+        "inputs": "velocities + numpy default_rng(8).normal(0, 0.3, n) per axis, then u = "
+                  "default_rng(8).uniform(0.2, 2.0, n) from the same generator; u_pred = u, v_pred = v",
+        "idx": idx,
+        "samples": {k: [float(v[i]) for i in idx] for k, v in arrs.items()},
+        "scale": {k: float(np.abs(v).max()) for k, v in arrs.items()},
+    }
+    with open(os.path.join(OUT, f"sphstep_{name}.json"), "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+    print(name, n)
+
+
 def read_tipsy_dark(path):
     with open(path, "rb") as f:
         buf = f.read()
@@ -259,9 +305,15 @@ def main():
     ap.add_argument("--periodic-cases", nargs="*", default=list(PERIODIC_CASES))
     ap.add_argument("--sph-cases", nargs="*", default=list(SPH_CASES))
     ap.add_argument("--basic-cases", nargs="*", default=list(BASIC_CASES))
+    ap.add_argument("--sph-step-cases", nargs="*", default=list(SPH_STEP_CASES))
+    ap.add_argument("--only-sph-step", action="store_true", help="write only the sphstep_ fixtures")
     a = ap.parse_args()
     if not O.ref_available():
         sys.exit("oracle/_ref/libptref.so is missing: run `make -C oracle` with the reference mounted")
+    for c in a.sph_step_cases:
+        run_sph_step_case(c)
+    if a.only_sph_step:
+        return
     make_kat(a.reference)
     for c in a.cases:
         run_case(c)

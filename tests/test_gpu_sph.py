@@ -244,3 +244,67 @@ def test_sph_density_exact_ties_on_a_lattice(ngrid, bucket):
     for i in range(p["x"].size):
         assert set(nbr[i][nd2[i] < b[i]].tolist()) == set(nbp[i][nd2p[i] < bp[i]].tolist()), i
         assert np.all(nd2[i][nbr[i] >= 0] <= b[i])
+
+
+def _step_state(s, u, up, vp):
+    st = s.state()
+    return dict(st, u=u, u_pred=up, vpx=vp[0], vpy=vp[1], vpz=vp[2])
+
+
+@pytest.mark.parametrize("gen,n,bucket,steps", [("plummer", 4000, 16, 3), ("mixture", 6000, 32, 2)])
+def test_sph_step_matches_oracle(gen, n, bucket, steps):
+    """Iterations of the SPH example (pt_sph_step: density, pressure with the
+    predicted energies and velocities, kick + perturb with the u updates)
+    against the C oracle's: same neighbour sets each step, sums in another
+    order (warp sums, atomic reactions), so within 1e-12 of each field's
+    largest value."""
+    p, u = _with_velocities(getattr(ics, gen)(n, seed=21))
+    rng = np.random.default_rng(9)
+    up = u * rng.uniform(0.9, 1.1, n)
+    vp = tuple(p[k] + rng.normal(0.0, 0.01, n) for k in ("vx", "vy", "vz"))
+    with sim(max_particles_per_leaf=bucket, max_timestep=0.01) as s:
+        s.set_particles(p)
+        gu, gup, gvp = s.sph_run(steps, u, up, vp)
+        got = _step_state(s, gu, gup, gvp)
+    q, pu, pup, pvp = O.sph_step(p, steps, 0.01, u, up, vp, threads=8)
+    want = dict(q, u=pu, u_pred=pup, vpx=pvp[0], vpy=pvp[1], vpz=pvp[2])
+    for k in ("x", "y", "z", "vx", "vy", "vz", "u", "u_pred", "vpx", "vpy", "vpz"):
+        assert _close(got[k], want[k], 1e-12), k
+    assert not np.allclose(got["x"], p["x"])
+
+
+@pytest.mark.parametrize("name", sorted(f[8:-5] for f in os.listdir(GOLD) if f.startswith("sphstep_")))
+def test_sph_step_matches_reference_golden(name):
+    with open(os.path.join(GOLD, f"sphstep_{name}.json")) as f:
+        g = json.load(f)
+    p, u = _with_velocities(getattr(ics, g["generator"])(**g["kwargs"]))
+    with sim(max_particles_per_leaf=g["bucket"], max_timestep=g["dt"]) as s:
+        s.set_particles(p)
+        gu, gup, gvp = s.sph_run(g["steps"], u)
+        got = _step_state(s, gu, gup, gvp)
+    for k, want in g["samples"].items():
+        scale = max(g["scale"][k], 1e-300)
+        assert np.all(np.abs(got[k][g["idx"]] - np.asarray(want)) <= 1e-12 * scale), k
+
+
+def test_sph_step_large_one_step_properties():
+    """N = 2^18 Plummer, one step from u_pred = u and v_pred = v: the velocity
+    change is a dt from the pressure pass on the same state, u and u_pred
+    follow the reference's PdV update, and momentum is conserved."""
+    p, u = _with_velocities(ics.plummer(1 << 18, seed=3, soft=1e-3))
+    dt = 1e-3
+    with sim(max_particles_per_leaf=32, max_timestep=dt) as s:
+        s.set_particles(p)
+        _, ax, ay, az, pdv = s.sph_pressure(u)
+        gu, gup, gvp = s.sph_run(1, u)
+        st = s.state()
+    for a, k, vpk in ((ax, "vx", 0), (ay, "vy", 1), (az, "vz", 2)):
+        dv = st[k] - p[k]
+        assert _close(dv, a * dt, 1e-9), k
+        assert _close(gvp[vpk] - st[k], a * dt, 1e-9), k
+        # sum m a = 0 to summation order; dv also carries the rounding of v + a dt
+        bound = float(np.sum(p["m"] * (np.abs(a * dt) + np.abs(p[k]))))
+        assert abs(float(np.sum(p["m"] * dv))) <= 1e-12 * bound
+    ud = 0.5e-7 * dt
+    assert _close(gu, u - pdv * ud, 1e-15) and _close(gup, u - 2 * pdv * ud, 1e-15)
+    assert np.all(np.isfinite(st["x"])) and not np.allclose(st["x"], p["x"])
