@@ -483,7 +483,9 @@ def extras(a, sim, p, world, rank, stream, value, shard=None):
     res["e2e"] = {"value": n * steps / t, "unit": UNIT, "h2d_bytes_per_step": 8 * 8 * n,
                   "d2h_bytes_per_step": 4 * 8 * n, "steps": steps,
                   "path": "pt_set_particles (pinned H2D) + pt_compute_forces + pt_get_accel (D2H)"}
-    if rank != 0:
+    if world > 1:
+        # the accuracy, FP64, sweep, SPH and CPU-baseline extras belong to the
+        # 1-GPU run; every rank stops here so that none holds its GPU waiting
         return res
     # force errors vs the FP64 direct sum on seeded targets, mixed and FP64
     rng = np.random.default_rng(43)
