@@ -257,7 +257,9 @@ int pt_sph_density(pt_handle* h, double* density, double* ball_sq, int32_t* nbr,
  * per particle (u_predicted; velocity_predicted = the handle's velocities).
  * Outputs: pressure accelerations and PdV work; density optional.  FP64; the
  * reactions are summed by atomic adds, so their order (the last bits) is not
- * fixed.  Caller order; any output may be NULL. */
+ * fixed.  A term that fails doSPHCalc's isfinite(acc) assertion (examples/
+ * SPHUtils.h:122; a ball of zero radius, as with N = 1 or coincident
+ * particles) returns PT_E_DEVICE.  Caller order; any output may be NULL. */
 int pt_sph_pressure(pt_handle* h, const double* u, double* density, double* ax, double* ay, double* az,
                     double* pdv);
 
@@ -273,7 +275,9 @@ int pt_sph_pressure(pt_handle* h, const double* u, double* density, double* ax, 
  * arrays in caller order (start them as u and the velocities, as
  * src/Reader.C:90-91 does); positions and velocities stay in the handle
  * (pt_get_state).  FP64; the pressure pass's reactions are atomic adds, so
- * trajectories match the reference to rounding, not bit for bit. */
+ * trajectories match the reference to rounding, not bit for bit.  A step whose
+ * pressure pass fails (as pt_sph_pressure) returns its error before the kick,
+ * with the particles of the steps before it. */
 int pt_sph_step(pt_handle* h, int nsteps, double* u, double* u_pred, double* vpx, double* vpy, double* vpz);
 
 /* FP64 direct sum (the force-error yardstick) ------------------------------

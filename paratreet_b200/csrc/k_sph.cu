@@ -443,6 +443,7 @@ __global__ void __launch_bounds__(256) sph_pressure_kernel(Particles p, const do
     divvi /= rhoi;
     const double corr = (divvj != 0.0 ? divvi / divvj : 1.0);
     double sax = 0.0, say = 0.0, saz = 0.0, spdv = 0.0;
+    bool acc_bad = false;  // doSPHCalc asserts isfinite(acc) (examples/SPHUtils.h:122)
     if (live) {
       const double xi = p.x[i], yi = p.y[i], zi = p.z[i];
       const double ph = 0.5 * fBall, ih2b = 4. / (fBall * fBall);
@@ -461,6 +462,7 @@ __global__ void __launch_bounds__(256) sph_pressure_kernel(Particles p, const do
       PdV += bR * aP * dvdotdr;
       spdv = PdV;
       const double acc = (aP + bP) + visc;
+      acc_bad = !isfinite(acc);
       const double s = acc * bR;
       sax = s * dx;
       say = s * dy;
@@ -475,6 +477,7 @@ __global__ void __launch_bounds__(256) sph_pressure_kernel(Particles p, const do
         atomicAdd(pdv + q, PdV);
       }
     }
+    if (__any_sync(kFull, acc_bad) && lane == 0) atomicOr(status, kErrSphNonFinite);
     sax = warp_sum_f64(sax);
     say = warp_sum_f64(say);
     saz = warp_sum_f64(saz);

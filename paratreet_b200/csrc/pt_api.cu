@@ -253,6 +253,7 @@ int read_status(pt_handle* h) {
     if (st & kErrAdjointSoftened) m += " adjoint met a softened quadrupole term (not differentiated);";
     if (st & kErrSort) m += " radix sort look-back timed out;";
     if (st & kErrPool) m += " interaction-list pools exhausted;";
+    if (st & kErrSphNonFinite) m += " SPH pressure term not finite (a ball of zero radius: N = 1 or coincident particles);";
     return fail(h, (st & kErrNonFinite) ? PT_E_NONFINITE : PT_E_DEVICE, m);
   }
   return PT_OK;
@@ -1034,6 +1035,8 @@ int pt_sph_step(pt_handle* h, int nsteps, double* u, double* u_pred, double* vpx
     q.vz = vps + 2 * n;
     launch_sph_pressure(q, h->sph, h->sph + n, us, h->sph_nbr, h->sph_nd2, n, out, out + n, out + 2 * n,
                         out + 3 * n, h->d_status, h->sms * 16, st);
+    CK(cudaGetLastError());
+    CKR(read_status(h));  // a failed pressure pass leaves the particles as they were
     launch_sph_kick_perturb(h->p, out, out + n, out + 2 * n, out + 3 * n, cs, cs + n, cs + 2 * n, cs + 3 * n,
                             cs + 4 * n, n, dt, g, st);
     CK(cudaGetLastError());

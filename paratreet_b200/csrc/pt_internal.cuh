@@ -29,6 +29,7 @@ enum : unsigned {
   kErrAdjointSoftened = 1u << 5,
   kErrSort = 1u << 6,                 // radix sort look-back gave up waiting
   kErrPool = 1u << 7,                 // two-phase traversal: a list outgrew its region or pool (retried)
+  kErrSphNonFinite = 1u << 8,         // SPH pressure: a term failed doSPHCalc's isfinite(acc)
 };
 
 // Particle state, structure of arrays, FP64, in key-sorted order after a build.

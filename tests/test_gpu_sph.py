@@ -308,3 +308,39 @@ def test_sph_step_large_one_step_properties():
     ud = 0.5e-7 * dt
     assert _close(gu, u - pdv * ud, 1e-15) and _close(gup, u - 2 * pdv * ud, 1e-15)
     assert np.all(np.isfinite(st["x"])) and not np.allclose(st["x"], p["x"])
+
+
+@pytest.mark.parametrize("n", [2, 7, 33])
+def test_sph_step_tiny(n):
+    """Fewer particles than neighbours: the lists hold every particle (padded
+    with -1), and the steps still match the C oracle's."""
+    p = ics.plummer(max(n, 2), seed=3, soft=0.05)
+    p = {k: v[:n].copy() for k, v in p.items()}
+    p, u = _with_velocities(p, seed=1)
+    with sim(max_particles_per_leaf=16, max_timestep=0.01) as s:
+        s.set_particles(p)
+        gu, gup, gvp = s.sph_run(2, u)
+        got = _step_state(s, gu, gup, gvp)
+    q, pu, pup, pvp = O.sph_step(p, 2, 0.01, u, u, (p["vx"], p["vy"], p["vz"]))
+    want = dict(q, u=pu, u_pred=pup, vpx=pvp[0], vpy=pvp[1], vpz=pvp[2])
+    for k in want:
+        if k in got:
+            assert _close(got[k], want[k], 1e-12), k
+
+
+def test_sph_single_particle_is_reported():
+    """One particle: its only neighbour is itself, the ball has zero radius and
+    the reference's doSPHCalc fails its isfinite(acc) assertion; here the
+    pressure pass and the step return an error and the handle stays usable."""
+    from paratreet_b200._lib import PtError
+    p = ics.plummer(8, seed=3, soft=0.05)
+    one = {k: v[:1].copy() for k, v in p.items()}
+    with sim(max_particles_per_leaf=16, max_timestep=0.01) as s:
+        s.set_particles(one)
+        with pytest.raises(PtError, match="SPH pressure term not finite"):
+            s.sph_pressure(np.ones(1))
+        with pytest.raises(PtError, match="SPH pressure term not finite"):
+            s.sph_run(1, np.ones(1))
+        s.set_particles(p)
+        d, ax, ay, az, pdv = s.sph_pressure(np.ones(8))
+        assert all(np.all(np.isfinite(a)) for a in (d, ax, ay, az, pdv))
