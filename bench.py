@@ -385,6 +385,26 @@ def sph_pressure_rate(a, sim, stream):
             "neighbours": 32, "note": "density pass + pressure pass of the SPH example, host in and out"}
 
 
+def driver_step_rate(a, sim, stream):
+    """Seconds per Driver::run iteration (pt_step: force pass, time step from
+    the maximum speed, the reference's kick and perturb) on the bench
+    particles.  Moves the particles: run it after the extras that read them."""
+    import torch
+    sim.run(1)
+    ts, tf = [], []
+    for _ in range(2):
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        sim.run(1)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        ts.append(s0.elapsed_time(s1))
+        tf.append(float(sim.counters()["ms_total"]))
+    step, force = float(np.mean(ts)), float(np.mean(tf))
+    return {"s_per_step": step / 1e3, "force_pass_ms": force, "rest_ms": step - force,
+            "note": "rest = time step (max-speed reduction) + kick/perturb kernel + host synchronisation"}
+
+
 def sph_step_rate(a, sim, stream):
     """Iterations of the SPH example (pt_sph_step: density pass, pressure
     pass, kick + perturb with the internal-energy updates, dt = 0.01) on the
@@ -514,6 +534,7 @@ def extras(a, sim, p, world, rank, stream, value, shard=None):
     res["theta_sweep"] = theta_sweep(a, sim, tgt, (dax, day, daz), stream) if a.sweep else []
     res["sph_density"] = sph_density_rate(a, sim, stream)
     res["sph_pressure"] = sph_pressure_rate(a, sim, stream)
+    res["driver_step"] = driver_step_rate(a, sim, stream)
     res["precision_comparison"] = {
         f"{a.precision}_force_evals_per_s": value, f"{other}_force_evals_per_s": v_other,
         "ratio_mixed_over_fp64": (value / v_other) if a.precision == "mixed" else (v_other / value),
