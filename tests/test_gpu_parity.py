@@ -155,6 +155,26 @@ def test_mixed_matches_fp64(gen, n, bucket):
     assert np.sqrt(np.mean(qe ** 2)) < 1e-5 and np.max(qe) < 1e-3
 
 
+def test_mixed_matches_fp64_full_size():
+    """The 2^24 Plummer workload (eps 1e-3, bucket 32, theta 0.7): both forms
+    make the same interactions (P2P pairs, P2C evaluations and opening tests
+    counted on the device) and the mixed accelerations stay within 1e-5 RMS
+    of the FP64 ones over all particles."""
+    p = ics.plummer(1 << 24, seed=42, soft=1e-3)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        with sim(max_particles_per_leaf=32, theta=0.7, precision=prec) as s:
+            s.set_particles(p)
+            s.start_down()
+            out[prec] = (s.accelerations(), s.counters())
+    (a64, c64), (am, cm) = out["fp64"], out["mixed"]
+    for k in ("n_pp", "n_pc", "n_open", "n_nodes", "n_buckets"):
+        assert c64[k] == cm[k], k
+    assert all(np.all(np.isfinite(am[k])) for k in ("ax", "ay", "az", "pot", "pot_full"))
+    e = rel_err((am["ax"], am["ay"], am["az"]), (a64["ax"], a64["ay"], a64["az"]))
+    assert np.sqrt(np.mean(e ** 2)) < 1e-5
+
+
 @pytest.mark.parametrize("gen,n,bucket", [("plummer", 60000, 32), ("mixture", 40000, 16)])
 def test_mixed_fused_fallback_matches_two_phase(gen, n, bucket, monkeypatch):
     """The fused walk-and-evaluate kernel (taken when the list pools cannot be
