@@ -222,7 +222,8 @@ struct EvalWarp {
 
 // Per-lane target of a 32-target chunk, replicated over G lane groups (lanes
 // past G * nt idle: a warp's loop runs as long as its target with the fewest
-// lanes, so a ragged split would not finish sooner).
+// lanes, so a ragged split would not finish sooner).  eval_p2p switches to
+// two targets per lane (EvTarget2) where that needs fewer iterations.
 struct EvTarget {
   int t, grp, G, nt;
   float tx, ty, tz, ts;
@@ -258,6 +259,86 @@ struct Kahan4 {
     s[k] = t;
   }
 };
+
+// Two targets per lane (P2P): lane l of group l / h holds targets 2 (l % h)
+// and 2 (l % h) + 1 (h = ceil(nt / 2); t2 == nt when there is none), so each
+// staged source meets two targets per packed instruction.  Chosen for the
+// chunk sizes where it leaves fewer lanes idle than one target per lane.
+struct EvTarget2 {
+  int t1, t2, grp, G, nt;
+  float2 tx, ty, tz, ts;
+};
+
+__device__ __forceinline__ bool ev_two_targets(int nt) {
+  const int g1 = 32 / nt, it1 = (32 + g1 - 1) / g1;
+  const int h = (nt + 1) >> 1, g2 = 32 / h, it2 = 2 * ((32 + g2 - 1) / g2);
+  return it2 < it1;
+}
+
+__device__ __forceinline__ EvTarget2 ev_target2(const Particles& p, const BucketGeom& g, int t0, int nt, int lane) {
+  EvTarget2 x;
+  const int h = (nt + 1) >> 1;
+  x.nt = nt;
+  x.G = 32 / h;
+  x.grp = lane / h;
+  x.t1 = 2 * (lane % h);
+  x.t2 = min(x.t1 + 1, nt);
+  x.tx = x.ty = x.tz = x.ts = make_float2(0.f, 0.f);
+  if (x.grp < x.G) {
+    const int i1 = t0 + x.t1, i2 = t0 + min(x.t2, nt - 1);  // no second target: the first again
+    x.tx = make_float2((float)(p.x[i1] - g.cm[0]), (float)(p.x[i2] - g.cm[0]));
+    x.ty = make_float2((float)(p.y[i1] - g.cm[1]), (float)(p.y[i2] - g.cm[1]));
+    x.tz = make_float2((float)(p.z[i1] - g.cm[2]), (float)(p.z[i2] - g.cm[2]));
+    x.ts = make_float2((float)p.soft[i1], (float)p.soft[i2]);
+  }
+  return x;
+}
+
+__device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
+  const float y = v - c;
+  const float t = s + y;
+  c = (t - s) - y;
+  s = t;
+}
+
+// The second target's compensated sums of a two-target lane live in rows 3
+// and 4 of the staging area (P2P stages rows 0-2 only).
+__device__ __forceinline__ void ev_two_zero(EvalWarp& w, int lane) {
+  __syncwarp();  // earlier readers of the area (the last chunk's reduction) are done
+  w.st[3][lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+  w.st[4][lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// ev_finish for two-target lanes (P2P: adds to ax, ay, az and pot_full).
+__device__ __forceinline__ void ev_finish2(EvalWarp& w, const Kahan4& K, const EvTarget2& x, const TravParams& P,
+                                           int t0, int lane) {
+  const float4 s2 = w.st[3][lane], c2 = w.st[4][lane];
+  double* red = reinterpret_cast<double*>(&w.st[0][0]);
+  __syncwarp();
+  if (x.grp < x.G) {
+    const int b1 = 4 * (x.grp * x.nt + x.t1);
+#pragma unroll
+    for (int k = 0; k < 4; k++) red[b1 + k] = (double)K.s[k] - (double)K.c[k];
+    if (x.t2 < x.nt) {
+      const int b2 = 4 * (x.grp * x.nt + x.t2);
+      red[b2 + 0] = (double)s2.x - (double)c2.x;
+      red[b2 + 1] = (double)s2.y - (double)c2.y;
+      red[b2 + 2] = (double)s2.z - (double)c2.z;
+      red[b2 + 3] = (double)s2.w - (double)c2.w;
+    }
+  }
+  __syncwarp();
+  if (lane < x.nt) {
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int gg = 0; gg < x.G; gg++)
+      for (int k = 0; k < 4; k++) v[k] += red[4 * (gg * x.nt + lane) + k];
+    const int i = t0 + lane;
+    P.p.ax[i] += v[0];
+    P.p.ay[i] += v[1];
+    P.p.az[i] += v[2];
+    P.p.potf[i] += v[3];
+  }
+}
 
 // Sum the G lane groups of each target and store or add the result.  P2C
 // (p2c): pot_full gets every node's potential, pot the quadrupole node()
@@ -524,8 +605,8 @@ __device__ __forceinline__ void ev_near_source(float m, float dx, float dy, floa
 // examples/GravityVisitor.h:144-160, in FP32): their sources are staged 64
 // per chunk as 32 interleaved pairs px = (x_a, x_b, y_a, y_b), pz = (z_a,
 // z_b, m_a, m_b), relative to the bucket, and evaluated with packed FP32.
-template <bool kFar>
-__device__ __forceinline__ void ev_p2p_leaves(EvalWarp& w, int nleaves, const TravParams& P, const EvTarget& x,
+template <bool kFar, bool kTwo, class Tgt>
+__device__ __forceinline__ void ev_p2p_leaves(EvalWarp& w, int nleaves, const TravParams& P, const Tgt& x,
                                               int lane, Kahan4& K) {
   int s0a = 0, s0b = 0, na = 0, nb = 0;
   if (lane < nleaves) {
@@ -562,7 +643,16 @@ __device__ __forceinline__ void ev_p2p_leaves(EvalWarp& w, int nleaves, const Tr
   __syncwarp();
   const float kPadPos = 1.0e10f;
   const float gs = (float)w.geom.soft_max;
-  const float2 ntx = make_float2(-x.tx, -x.tx), nty = make_float2(-x.ty, -x.ty), ntz = make_float2(-x.tz, -x.tz);
+  float2 ntx, nty, ntz;
+  if constexpr (kTwo) {
+    ntx = make_float2(-x.tx.x, -x.tx.y);
+    nty = make_float2(-x.ty.x, -x.ty.y);
+    ntz = make_float2(-x.tz.x, -x.tz.y);
+  } else {
+    ntx = make_float2(-x.tx, -x.tx);
+    nty = make_float2(-x.ty, -x.ty);
+    ntz = make_float2(-x.tz, -x.tz);
+  }
   // plain packed sums over the block's chunks, one compensated add at its end
   float2 ax2 = make_float2(0.f, 0.f), ay2 = ax2, az2 = ax2, pp2 = ax2;  // pp2 sums +m/r
   for (int cs = 0; cs < total; cs += 64) {
@@ -607,6 +697,40 @@ __device__ __forceinline__ void ev_p2p_leaves(EvalWarp& w, int nleaves, const Tr
       __syncwarp();
     }
     const int np = (min(64, total - cs) + 1) >> 1;
+    if constexpr (kTwo) {
+      if (x.grp < x.G) {
+        const float4* sp = &w.st[0][x.grp];
+        for (int k = x.grp; k < np; k += x.G, sp += x.G) {
+          const float4 X = sp[0], Z = sp[32];
+          float4 R = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (!kFar) R = sp[64];
+#pragma unroll
+          for (int h = 0; h < 2; h++) {  // source a, then source b, against both targets
+            const float sx = h ? X.y : X.x, sy = h ? X.w : X.z, sz = h ? Z.y : Z.x, sm = h ? Z.w : Z.z;
+            const float2 dx = __fadd2_rn(make_float2(sx, sx), ntx);
+            const float2 dy = __fadd2_rn(make_float2(sy, sy), nty);
+            const float2 dz = __fadd2_rn(make_float2(sz, sz), ntz);
+            float2 r2 = __fmul2_rn(dx, dx);
+            r2 = __ffma2_rn(dy, dy, r2);
+            r2 = __ffma2_rn(dz, dz, r2);
+            const float reach2 = h ? R.y : R.x;
+            if (kFar || ((r2.x > reach2) && (r2.y > reach2))) {
+              const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+              const float2 mr = __fmul2_rn(make_float2(sm, sm), ri);
+              const float2 mr3 = __fmul2_rn(mr, __fmul2_rn(ri, ri));
+              ax2 = __ffma2_rn(dx, mr3, ax2);
+              ay2 = __ffma2_rn(dy, mr3, ay2);
+              az2 = __ffma2_rn(dz, mr3, az2);
+              pp2 = __fadd2_rn(pp2, mr);
+            } else {
+              const float ss = h ? R.w : R.z;
+              ev_near_source(sm, dx.x, dy.x, dz.x, r2.x, reach2, ss, x.ts.x, ax2.x, ay2.x, az2.x, pp2.x);
+              ev_near_source(sm, dx.y, dy.y, dz.y, r2.y, reach2, ss, x.ts.y, ax2.y, ay2.y, az2.y, pp2.y);
+            }
+          }
+        }
+      }
+    } else {
     if (x.grp < x.G) {
       const float4* sp = &w.st[0][x.grp];  // rows st[1], st[2] follow at +32, +64
       for (int k = x.grp; k < np; k += x.G, sp += x.G) {
@@ -637,12 +761,53 @@ __device__ __forceinline__ void ev_p2p_leaves(EvalWarp& w, int nleaves, const Tr
         }
       }
     }
+    }
   }
-  K.add(0, ax2.x + ax2.y);
-  K.add(1, ay2.x + ay2.y);
-  K.add(2, az2.x + az2.y);
-  K.add(3, -(pp2.x + pp2.y));
+  if constexpr (kTwo) {
+    K.add(0, ax2.x);
+    K.add(1, ay2.x);
+    K.add(2, az2.x);
+    K.add(3, -pp2.x);
+    float4 s2 = w.st[3][lane], c2 = w.st[4][lane];
+    kahan_add(s2.x, c2.x, ax2.y);
+    kahan_add(s2.y, c2.y, ay2.y);
+    kahan_add(s2.z, c2.z, az2.y);
+    kahan_add(s2.w, c2.w, -pp2.y);
+    w.st[3][lane] = s2;
+    w.st[4][lane] = c2;
+  } else {
+    K.add(0, ax2.x + ax2.y);
+    K.add(1, ay2.x + ay2.y);
+    K.add(2, az2.x + az2.y);
+    K.add(3, -(pp2.x + pp2.y));
+  }
   __syncwarp();
+}
+
+// The bucket's P2P list in blocks of 64 entries: far leaves, then near ones.
+template <bool kTwo, class Tgt>
+__device__ __forceinline__ void ev_p2p_blocks(EvalWarp& w, const TravParams& P, const ListParams& L, const Tgt& x,
+                                              int64_t start, int count, int lane, Kahan4& K) {
+  for (int blk = 0; blk < count; blk += 64) {
+    const bool va = blk + lane < count, vb = blk + lane + 32 < count;
+    const int ea = va ? L.pp_pool[start + blk + lane] : 0;
+    const int eb = vb ? L.pp_pool[start + blk + lane + 32] : 0;
+#pragma unroll
+    for (int kind = 0; kind < 2; kind++) {  // far leaves, then near leaves
+      const bool sa = va && ((ea < 0) == (kind == 1)), sb = vb && ((eb < 0) == (kind == 1));
+      const unsigned ma = __ballot_sync(kFull, sa), mb = __ballot_sync(kFull, sb);
+      const unsigned lt = (1u << lane) - 1u;
+      __syncwarp();
+      if (sa) w.lsel[__popc(ma & lt)] = ea & 0x7fffffff;
+      if (sb) w.lsel[__popc(ma) + __popc(mb & lt)] = eb & 0x7fffffff;
+      __syncwarp();
+      const int n = __popc(ma) + __popc(mb);
+      if (n) {
+        if (kind == 0) ev_p2p_leaves<true, kTwo>(w, n, P, x, lane, K);
+        else ev_p2p_leaves<false, kTwo>(w, n, P, x, lane, K);
+      }
+    }
+  }
 }
 
 template <int kMinBlocks>
@@ -664,33 +829,24 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2p(TravParams
     const int tbase = P.walk[tnode].pstart, ntot = P.walk[tnode].pcount;
     for (int tc = 0; tc < ntot; tc += 32) {
       const int t0 = tbase + tc, nt = min(32, ntot - tc);
+      if (ev_two_targets(nt)) {
+        const EvTarget2 x = ev_target2(P.p, w.geom, t0, nt, lane);
+        ev_two_zero(w, lane);
+        Kahan4 K;
+        K.zero();
+        ev_p2p_blocks<true>(w, P, L, x, start, count, lane, K);
+        ev_finish2(w, K, x, P, t0, lane);
+        continue;
+      }
       const EvTarget x = ev_target(P.p, w.geom, t0, nt, lane);
       Kahan4 K;
       K.zero();
-      for (int blk = 0; blk < count; blk += 64) {
-        const bool va = blk + lane < count, vb = blk + lane + 32 < count;
-        const int ea = va ? L.pp_pool[start + blk + lane] : 0;
-        const int eb = vb ? L.pp_pool[start + blk + lane + 32] : 0;
-#pragma unroll
-        for (int kind = 0; kind < 2; kind++) {  // far leaves, then near leaves
-          const bool sa = va && ((ea < 0) == (kind == 1)), sb = vb && ((eb < 0) == (kind == 1));
-          const unsigned ma = __ballot_sync(kFull, sa), mb = __ballot_sync(kFull, sb);
-          const unsigned lt = (1u << lane) - 1u;
-          __syncwarp();
-          if (sa) w.lsel[__popc(ma & lt)] = ea & 0x7fffffff;
-          if (sb) w.lsel[__popc(ma) + __popc(mb & lt)] = eb & 0x7fffffff;
-          __syncwarp();
-          const int n = __popc(ma) + __popc(mb);
-          if (n) {
-            if (kind == 0) ev_p2p_leaves<true>(w, n, P, x, lane, K);
-            else ev_p2p_leaves<false>(w, n, P, x, lane, K);
-          }
-        }
-      }
+      ev_p2p_blocks<false>(w, P, L, x, start, count, lane, K);
       ev_finish(w, K, 0.f, x, P, t0, lane, false, false);
     }
   }
 }
+
 
 // ---------------------------------------------------------------- launchers
 int walk_lists_grid(int sms) { return sms * 5; }  // the CTAs resident at 96 registers
