@@ -390,9 +390,9 @@ def driver_step_rate(a, sim, stream):
     the maximum speed, the reference's kick and perturb) on the bench
     particles.  Moves the particles: run it after the extras that read them."""
     import torch
-    sim.run(1)
+    sim.run(2)
     ts, tf = [], []
-    for _ in range(2):
+    for _ in range(5):
         s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s0.record(stream)
         sim.run(1)
@@ -400,9 +400,12 @@ def driver_step_rate(a, sim, stream):
         torch.cuda.synchronize()
         ts.append(s0.elapsed_time(s1))
         tf.append(float(sim.counters()["ms_total"]))
-    step, force = float(np.mean(ts)), float(np.mean(tf))
+    k = int(np.argsort(ts)[len(ts) // 2])  # the median step and its own force pass
+    step, force = float(ts[k]), float(tf[k])
     return {"s_per_step": step / 1e3, "force_pass_ms": force, "rest_ms": step - force,
-            "note": "rest = time step (max-speed reduction) + kick/perturb kernel + host synchronisation"}
+            "steps_ms": [round(t, 3) for t in ts], "warmup_steps": 2,
+            "note": "median of 5 steps; rest = time step (max-speed reduction) + kick/perturb kernel + "
+                    "host synchronisation"}
 
 
 def sph_step_rate(a, sim, stream):
