@@ -856,7 +856,8 @@ void launch_walk_lists(const TravParams& P, const ListParams& L, const Mom* mom,
   walk_lists<<<grid, kWlWarps * 32, 0, st>>>(P, L, mom);
 }
 // eval_p2c keeps 80 registers (6 CTAs per SM; at 64 it spills), eval_p2p
-// fits 64 (8 CTAs per SM)
+// 64 (8 CTAs per SM; its two-target path spills 52 bytes there, and still
+// measured faster than at 72 registers and 7 CTAs per SM)
 void launch_eval_lists(const TravParams& P, const ListParams& L, const Mom* mom, int grid, cudaStream_t st,
                        unsigned* work2) {
   TravParams Q = P;
