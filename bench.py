@@ -549,6 +549,10 @@ def extras(a, sim, p, world, rank, stream, value, shard=None):
         threads = os.cpu_count() or 1
         v, desc = reference_sample(p, a, threads, seconds=a.cpu_seconds)
         res["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "reference", "sample": desc}
+        # one core, for the scaling of the reference's own code over the host threads
+        v1, desc1 = reference_sample(p, a, 1, seconds=max(1.0, a.cpu_seconds / 4))
+        res["cpu_baseline"]["single_core"] = {"value": v1, "sample": desc1,
+                                              "threads_speedup": v / v1 if v1 else None}
     except Exception as e:  # reported, not fatal
         res["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                                "sample": f"failed: {e}"}
