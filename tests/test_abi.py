@@ -76,6 +76,7 @@ def test_null_handle_calls_return_errors():
     assert lib.pt_destroy(None) == 0
     assert lib.pt_sph_density(None, None, None, None, None) == -1
     assert lib.pt_sph_pressure(None, None, None, None, None, None, None) == -1
+    assert lib.pt_sph_step(None, 1, None, None, None, None, None) == -1
 
 
 def test_visitor_mirror():
