@@ -64,8 +64,9 @@ def balanced_cuts(weights, world: int) -> list[int]:
 def rescale_cuts(cuts: list[int], nb_old: int, nb_new: int) -> list[int]:
     """Carry cut positions over to a rebuilt tree with nb_new buckets (the
     same fractions of the key-ordered list); the last range stays open."""
-    if nb_old <= 0:
-        return list(cuts)
+    world = len(cuts) - 1
+    if nb_old <= 0:  # nothing measured (an empty tree): equal bucket counts
+        return [r * nb_new // world for r in range(world)] + [BIG]
     out = [0] + [min(nb_new, int(round(c * nb_new / nb_old))) for c in cuts[1:-1]] + [BIG]
     for i in range(1, len(out)):
         out[i] = max(out[i], out[i - 1])

@@ -162,3 +162,29 @@ def test_gloo_ranks_match_one_rank(tmp_path, world):
             assert np.array_equal(got[k], want[k]), (r, k)
         cuts = got["cuts"] if cuts is None else cuts
         assert np.array_equal(got["cuts"], cuts)  # every rank agrees on the next cut
+
+
+def test_cuts_properties():
+    """Any weights and rank count: the cuts are monotone, start at 0 and end at
+    the bucket count, every range is within one bucket of the ideal load, and
+    the cuts carried over to a tree of another size still cover every bucket
+    once (the last range stays open)."""
+    from hypothesis import given, settings, strategies as st
+
+    @settings(max_examples=200, deadline=None)
+    @given(st.lists(st.integers(0, 10 ** 6), min_size=0, max_size=300), st.integers(1, 12),
+           st.integers(0, 600))
+    def check(w, world, nb_new):
+        w = np.asarray(w, dtype=np.int64)
+        c = balanced_cuts(w, world)
+        assert len(c) == world + 1 and c[0] == 0 and c[-1] == w.size
+        assert all(a <= b for a, b in zip(c, c[1:]))
+        if w.size and w.sum() > 0:
+            loads = [int(w[a:b].sum()) for a, b in zip(c, c[1:])]
+            assert max(loads) <= w.sum() / world + w.max()
+        r = rescale_cuts(c, w.size, nb_new)
+        assert r[0] == 0 and r[-1] == BIG and all(a <= b for a, b in zip(r, r[1:]))
+        covered = sum(min(b, nb_new) - min(a, nb_new) for a, b in zip(r, r[1:]))
+        assert covered == nb_new
+
+    check()
