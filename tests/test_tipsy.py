@@ -99,3 +99,31 @@ def test_reference_fixture_reads_like_the_known_answer_arrays():
     assert np.array_equal(p["soft"], kat["eps"].astype(np.float64))
     acc = tipsy.read_acc(os.path.join(REF_GRAVITY, "direct.acc"))
     assert np.array_equal(acc[:, kat["targets"]].T, kat["acc"])
+
+
+def test_round_trip_random(tmp_path):
+    """Any particle count (none included) and type mix, both precisions: what
+    the writer stores, the reader returns (cast to the file's precision), gas,
+    dark and star in that order."""
+    from hypothesis import given, settings, strategies as st
+
+    @settings(max_examples=60, deadline=None)
+    @given(st.integers(0, 200), st.booleans(), st.integers(0, 2 ** 31 - 1))
+    def check(n, double, seed):
+        rng = np.random.default_rng(seed)
+        p = {k: rng.normal(0.0, 1.0, n) for k in ("x", "y", "z", "vx", "vy", "vz")}
+        p["m"] = rng.uniform(0.1, 1.0, n)
+        p["soft"] = rng.uniform(0.001, 0.1, n)
+        p["type"] = rng.integers(0, 3, n).astype(np.int8)
+        f = str(tmp_path / f"r{seed}.tipsy")
+        tipsy.write_tipsy(f, p, time=1.5, double=double, softening=True)
+        q, h = tipsy.read_tipsy(f)
+        assert h.nbodies == n and h.time == 1.5
+        o = np.concatenate([np.flatnonzero(p["type"] == t) for t in (0, 1, 2)]).astype(np.int64)
+        cast = (lambda a: a) if double else (lambda a: a.astype(np.float32).astype(np.float64))
+        for k in ("x", "y", "z", "vx", "vy", "vz"):
+            assert np.array_equal(q[k], cast(p[k][o])), k
+        assert np.array_equal(q["type"], p["type"][o])
+        os.remove(f)
+
+    check()
