@@ -4,7 +4,9 @@ Run in a container where the reference tree is mounted and the
 reference-sources oracle (oracle/_ref/libptref.so, ``make -C oracle``) is
 built:
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py [--reference PATH]
+
+PATH defaults to $PT_REFERENCE, else <repo>/../reference.
 
 Outputs
 -------
@@ -300,7 +302,9 @@ def make_kat(reference):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    repo = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    ap.add_argument("--reference", default=os.environ.get("PT_REFERENCE", os.path.join(os.path.dirname(repo),
+                                                                                       "reference")))
     ap.add_argument("--cases", nargs="*", default=list(CASES))
     ap.add_argument("--periodic-cases", nargs="*", default=list(PERIODIC_CASES))
     ap.add_argument("--sph-cases", nargs="*", default=list(SPH_CASES))

@@ -10,7 +10,11 @@ import pytest
 from paratreet_b200 import ics, tipsy
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-REF_GRAVITY = os.path.join(os.environ.get("PT_REFERENCE", "/root/reference"), "tests", "gravity")
+# the reference checkout: $PT_REFERENCE, else a sibling of this repository
+REF_ROOT = os.environ.get("PT_REFERENCE",
+                          os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))),
+                                       "reference"))
+REF_GRAVITY = os.path.join(REF_ROOT, "tests", "gravity")
 
 
 def mixed_types(n=300, seed=1):
@@ -89,7 +93,7 @@ def test_acc_round_trip(tmp_path):
     assert open(f).readline() == "123\n"
 
 
-@pytest.mark.skipif(not os.path.exists(REF_GRAVITY), reason="reference tree not mounted")
+@pytest.mark.skipif(not os.path.exists(REF_GRAVITY), reason="reference checkout not found (set PT_REFERENCE)")
 def test_reference_fixture_reads_like_the_known_answer_arrays():
     kat = np.load(os.path.join(GOLD, "lambs_kat.npz"))
     p, h = tipsy.read_tipsy(os.path.join(REF_GRAVITY, "lambs.00200_subsamp_30K"))
