@@ -15,9 +15,11 @@
 // Host code sees only a stand-in for the symbol, so the device address is
 // looked up with cudaGetSymbolAddress, once per device, with that device
 // current, on the first call made on that device.  Make that first call
-// before any stream capture.  All calls share the array and it keeps the last
-// call's contents: the status word is cleared at the start of every call and
-// every partial that is read was written by the same call.  Calls whose work
+// before any stream capture.  Every call copies the status word to host
+// memory and synchronises its stream before it returns.  All calls share the
+// array and it keeps the last call's contents: the status word is cleared at
+// the start of every call and every partial that is read was written by the
+// same call.  Calls whose work
 // overlaps on the GPU (different streams, or different host threads on one
 // device) race on the array and must be serialised by the caller.
 #include <cstdio>
@@ -90,12 +92,15 @@ __global__ void __launch_bounds__(kNoAllocTile) noalloc_direct(const double* __r
   }
 }
 
-// Sum the slices of each target in slice order (0.0 + s0 + s1 + ...).
+// Sum the slices of each target in slice order (0.0 + s0 + s1 + ...).  When
+// the direct-sum kernel flagged a target index outside [0, n), nothing is
+// written: the caller's output arrays keep their contents.
 __global__ void __launch_bounds__(256) noalloc_reduce(const double* __restrict__ part, int nsplit, int64_t nt,
                                                       double* __restrict__ ax, double* __restrict__ ay,
-                                                      double* __restrict__ az, double* __restrict__ pot) {
+                                                      double* __restrict__ az, double* __restrict__ pot,
+                                                      const unsigned* __restrict__ status) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t >= nt) return;
+  if (t >= nt || *status != 0u) return;
   double s[4] = {0.0, 0.0, 0.0, 0.0};
   for (int sl = 0; sl < nsplit; sl++)
     for (int k = 0; k < 4; k++) s[k] += part[((int64_t)sl * nt + t) * 4 + k];
@@ -182,7 +187,7 @@ extern "C" int pt_direct_sum_noalloc(int64_t n, const double* x, const double* y
   note_launch();
   noalloc_direct<<<grid, kNoAllocTile, 0, st>>>(x, y, z, m, soft, n, targets, nt, (int)nsplit, part, status);
   note_launch();
-  noalloc_reduce<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(part, (int)nsplit, nt, ax, ay, az, pot);
+  noalloc_reduce<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(part, (int)nsplit, nt, ax, ay, az, pot, status);
   unsigned h_status = 0;
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(&h_status, status, sizeof(unsigned), cudaMemcpyDeviceToHost, st);

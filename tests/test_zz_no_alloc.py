@@ -55,3 +55,21 @@ def test_direct_sum_noalloc_matches_allocating_entry_point():
                                    C.c_void_p(dtgt.data_ptr()), *[C.c_void_p(o.data_ptr()) for o in outs],
                                    stream, err, len(err))
     assert rc == -1 and b"scratch limit" in err.value
+
+    # a target index outside [0, n) is found by the kernel, which skips it (it
+    # never reads through a bad index): the call reports it and leaves the
+    # outputs untouched, and the next good call starts from a cleared status word
+    n = src[0].numel()
+    for bad in (n, -1):
+        btgt = torch.from_numpy(np.array([0, bad, 7], dtype=np.int32)).to(dev)
+        for o in outs:
+            o.fill_(float("nan"))
+        rc = lib.pt_direct_sum_noalloc(n, *[C.c_void_p(t.data_ptr()) for t in src], 3, C.c_void_p(btgt.data_ptr()),
+                                       *[C.c_void_p(o.data_ptr()) for o in outs], stream, err, len(err))
+        assert rc == -1 and b"outside [0, n)" in err.value
+        assert all(bool(torch.isnan(o[:3]).all()) for o in outs)
+    rc = lib.pt_direct_sum_noalloc(n, *[C.c_void_p(t.data_ptr()) for t in src], tgt.size, C.c_void_p(dtgt.data_ptr()),
+                                   *[C.c_void_p(o.data_ptr()) for o in outs], stream, err, len(err))
+    assert rc == 0, err.value.decode()
+    for a, b in zip([o.cpu().numpy() for o in outs], ref):
+        assert np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)) < 1e-12
