@@ -185,37 +185,53 @@ def run_reference(a):
         print(json.dumps({"impl": "reference", "metric": METRIC,
                           "unavailable": "reference-sources oracle (oracle/_ref) was not built"}))
         return 0
+    cfg["precision"] = "fp64"  # the reference's gravity sources built with -DUSE_DOUBLE_FP
     p = make_ics(a)
     threads = os.cpu_count() or 1
     vals = []
-    sample_desc = None
+    info = None
     for s in range(a.warmup + a.steps):
-        v, sample_desc = reference_sample(p, a, threads, seconds=a.cpu_seconds / 2)
+        v, info = reference_sample(p, a, threads, seconds=a.cpu_seconds / 2)
         if s >= a.warmup:
             vals.append(v)
     value = float(np.mean(vals))
     out = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
            "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "data": "synthetic",
            "dtype": "f64", "config": cfg, "vs_baseline": None,
-           "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
-                            "sample": sample_desc},
+           "cpu_baseline": dict({"value": value, "unit": UNIT, "cores": threads, "kind": "reference"}, **info),
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
     return 0
 
 
-def reference_sample(p, a, threads, seconds=10.0):
+REF_FLAGS = "-O3 -ffp-contract=off -fno-fast-math -DUSE_DOUBLE_FP (FP64)"
+
+
+def reference_sample(p, a, threads, seconds=10.0, bucket=None, theta=None, label=None):
     """Reference CPU path (the reference's own gravity sources): full tree
-    build at N, traversal of a strided sample of bucket groups, scaled to N."""
+    build at N, then the traversal of bucket groups of 16 buckets (one
+    Partition each; the reference's defaults give 8 partitions per PE) in a
+    seeded random order until `seconds` are spent, scaled to all buckets.
+    Returns (force evaluations/s, description dict)."""
     from oracle import oracle as O
-    r = O.RefSim(p, bucket=a.bucket, theta=a.theta, dt_max=0.01, group=16, threads=threads)
+    bucket = a.bucket if bucket is None else bucket
+    theta = a.theta if theta is None else theta
+    n = p["x"].size
+    r = O.RefSim(p, bucket=bucket, theta=theta, dt_max=0.01, group=16, threads=threads)
     t_build, t_trav, frac = r.forces_sample(stride=0, budget_s=seconds)
     r.close()
     t_est = t_build + t_trav / max(frac, 1e-12)
-    desc = (f"reference gravity sources (oracle/_ref, -O2 FP64) on {threads} threads: full tree build at "
-            f"N={a.n} ({t_build:.2f} s) + traversal of {100 * frac:.3f}% of the particles' buckets "
+    desc = (f"reference gravity sources (oracle/_ref, {REF_FLAGS}) on {threads} thread(s): full tree build at "
+            f"N={n} ({t_build:.2f} s) + traversal of {100 * frac:.3f}% of the particles' buckets "
             f"({t_trav:.2f} s), traversal scaled to all buckets")
-    return a.n / t_est, desc
+    info = {"sample": desc, "workload": label or workload_config(a, 1)["workload"],
+            "sampled_fraction": frac, "build_s": t_build, "traversal_s_sampled": t_trav,
+            "traversal_s_scaled": t_trav / max(frac, 1e-12), "threads": threads,
+            "charm_equivalent": f"+p {threads} (one PE per host thread; the reference's defaults then cut "
+                                f"{8 * threads} partitions, examples/Main.C:27-28)",
+            "flags": REF_FLAGS, "tree_build": "restated serial build around the reference's own "
+                                             "CentroidData / MultipoleMoments (oracle/ref_driver.cpp)"}
+    return n / t_est, info
 
 
 # ----------------------------------------------------------------- our arm
@@ -385,14 +401,16 @@ def sph_pressure_rate(a, sim, stream):
             "neighbours": 32, "note": "density pass + pressure pass of the SPH example, host in and out"}
 
 
-def driver_step_rate(a, sim, stream):
+def driver_step_rate(a, sim, stream, steps=20):
     """Seconds per Driver::run iteration (pt_step: force pass, time step from
     the maximum speed, the reference's kick and perturb) on the bench
-    particles.  Moves the particles: run it after the extras that read them."""
+    particles, over `steps` consecutive iterations after two warm-up ones
+    (median, mean and max).  Moves the particles: run it after the extras
+    that read them."""
     import torch
     sim.run(2)
     ts, tf = [], []
-    for _ in range(5):
+    for _ in range(steps):
         s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s0.record(stream)
         sim.run(1)
@@ -402,10 +420,12 @@ def driver_step_rate(a, sim, stream):
         tf.append(float(sim.counters()["ms_total"]))
     k = int(np.argsort(ts)[len(ts) // 2])  # the median step and its own force pass
     step, force = float(ts[k]), float(tf[k])
-    return {"s_per_step": step / 1e3, "force_pass_ms": force, "rest_ms": step - force,
+    return {"s_per_step": step / 1e3, "s_per_step_mean": float(np.mean(ts)) / 1e3,
+            "s_per_step_max": float(np.max(ts)) / 1e3, "max_over_median": float(np.max(ts)) / step,
+            "force_pass_ms": force, "rest_ms": step - force,
             "steps_ms": [round(t, 3) for t in ts], "warmup_steps": 2,
-            "note": "median of 5 steps; rest = time step (max-speed reduction) + kick/perturb kernel + "
-                    "host synchronisation"}
+            "note": f"median, mean and max of {steps} consecutive steps; rest = time step (max-speed "
+                    "reduction) + kick/perturb kernel + host synchronisation of the median step"}
 
 
 def sph_step_rate(a, sim, stream):
@@ -446,35 +466,138 @@ def phase_rooflines(c, n, peaks):
 
 
 def theta_sweep(a, sim, tgt, direct, stream):
-    """Force evaluations/s and errors vs the FP64 direct sum of both forms
+    """Force evaluations/s and errors vs the FP64 direct sum of the three
+    forms (mixed; FP64 over the same two-phase lists; the ordered FP64 walk)
     over the theta values of --sweep (same particles and targets)."""
-    import torch
-    n = a.n
     rows = []
     for th in [float(v) for v in a.sweep.split(",") if v]:
         sim.set_theta(th)
         row = {"theta": th}
-        for prec, reps in (("mixed", 2), ("fp64", 1)):
-            sim.set_precision(prec)
-            sim.start_down()
-            ts = []
-            for _ in range(reps):
-                s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                s0.record(stream)
-                sim.start_down()
-                s1.record(stream)
-                torch.cuda.synchronize()
-                ts.append(s0.elapsed_time(s1) / 1e3)
-            acc = sim.accelerations()
-            c = sim.counters()
-            row[prec] = {"force_evals_per_s": n / float(np.mean(ts)), "ms_per_pass": 1e3 * float(np.mean(ts)),
-                         "err_vs_direct": rel_errors((acc["ax"][tgt], acc["ay"][tgt], acc["az"][tgt]), direct),
-                         "interactions_per_particle": (c["n_pp"] + c["n_pc"]) / n}
+        for prec, reps in (("mixed", 2), ("fp64_lists", 1), ("fp64", 1)):
+            row[prec] = timed_form(a, sim, tgt, direct, stream, prec, reps)
         row["ratio_mixed_over_fp64"] = row["mixed"]["force_evals_per_s"] / row["fp64"]["force_evals_per_s"]
+        row["ratio_mixed_over_fp64_lists"] = (row["mixed"]["force_evals_per_s"] /
+                                              row["fp64_lists"]["force_evals_per_s"])
         rows.append(row)
     sim.set_theta(a.theta)
     sim.set_precision(a.precision)
     return rows
+
+
+def timed_form(a, sim, tgt, direct, stream, prec, reps):
+    """Force evaluations/s (mean of reps passes after one untimed pass) and
+    the force error against the direct sum, of one form at the current theta."""
+    import torch
+    sim.set_precision(prec)
+    sim.start_down()
+    ts = []
+    for _ in range(reps):
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        sim.start_down()
+        s1.record(stream)
+        torch.cuda.synchronize()
+        ts.append(s0.elapsed_time(s1) / 1e3)
+    acc = sim.accelerations()
+    c = sim.counters()
+    return {"force_evals_per_s": a.n / float(np.mean(ts)), "ms_per_pass": 1e3 * float(np.mean(ts)),
+            "ms_traverse": c["ms_traverse"],
+            "err_vs_direct": rel_errors((acc["ax"][tgt], acc["ay"][tgt], acc["az"][tgt]), direct),
+            "interactions_per_particle": (c["n_pp"] + c["n_pc"]) / a.n}
+
+
+def accuracy_clause(a, sim, tgt, direct, stream, bound=1e-4, lo=0.35, hi=0.50):
+    """The headline metric under its own accuracy clause: the largest theta on
+    a 0.01 grid in [lo, hi] at which the tree's RMS relative force error
+    against the FP64 direct sum (the seeded targets) is <= bound, found by
+    bisection on the mixed form (whose error equals the FP64 form's to about
+    1e-7 relative), then both forms timed and their errors measured there,
+    and the errors one grid step above it."""
+    grid = [round(lo + 0.01 * k, 2) for k in range(int(round((hi - lo) / 0.01)) + 1)]
+    probes = {}
+
+    def rms(th):
+        if th not in probes:
+            sim.set_theta(th)
+            sim.set_precision("mixed")
+            sim.start_down()
+            acc = sim.accelerations()
+            probes[th] = rel_errors((acc["ax"][tgt], acc["ay"][tgt], acc["az"][tgt]), direct)["rms"]
+        return probes[th]
+
+    out = {"bound_rms": bound, "grid": [grid[0], grid[-1], 0.01]}
+    if rms(grid[0]) > bound:
+        out["theta"] = None
+        out["note"] = f"rms {probes[grid[0]]:.3e} > bound already at theta {grid[0]}"
+    else:
+        i, j = 0, len(grid) - 1  # rms(grid[i]) <= bound; grid[j] unknown or above
+        if rms(grid[j]) <= bound:
+            i = j
+        while j - i > 1:
+            k = (i + j) // 2
+            if rms(grid[k]) <= bound:
+                i = k
+            else:
+                j = k
+        th = grid[i]
+        sim.set_theta(th)
+        row = {"theta": th}
+        row["mixed"] = timed_form(a, sim, tgt, direct, stream, "mixed", 2)
+        row["fp64_lists"] = timed_form(a, sim, tgt, direct, stream, "fp64_lists", 1)
+        row["fp64"] = timed_form(a, sim, tgt, direct, stream, "fp64", 1)
+        row["ratio_mixed_over_fp64"] = row["mixed"]["force_evals_per_s"] / row["fp64"]["force_evals_per_s"]
+        row["ratio_mixed_over_fp64_lists"] = (row["mixed"]["force_evals_per_s"] /
+                                              row["fp64_lists"]["force_evals_per_s"])
+        row["all_within_bound"] = bool(all(row[f]["err_vs_direct"]["rms"] <= bound
+                                           for f in ("mixed", "fp64_lists", "fp64")))
+        out.update(row)
+        if i + 1 < len(grid):
+            out["next_theta_mixed_rms"] = {"theta": grid[i + 1], "rms": rms(grid[i + 1])}
+    out["probes_mixed_rms"] = {str(k): v for k, v in sorted(probes.items())}
+    sim.set_theta(a.theta)
+    sim.set_precision(a.precision)
+    return out
+
+
+def adjoint_cost(a, stream):
+    """Cost of one adjoint force pass against one forward pass on the
+    differentiation workload (Hernquist N = 262,144, seed 3, eps 0.01,
+    theta 0.6, bucket 16): the forward pass that records the interaction
+    lists the adjoint differentiates (mixed form), the plain two-phase mixed
+    pass, and pt_adjoint (cotangent in and gradients out through host
+    memory), each the mean of 3 after one untimed call."""
+    import torch
+    from paratreet_b200 import ics
+    from paratreet_b200.gravity import GravitySimulation
+    n = 262144
+    q = ics.hernquist(n, seed=3, soft=0.01)
+    cot = np.random.default_rng(64).normal(size=(3, n))
+
+    def timed(f, reps=3):
+        f()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(reps):
+            f()
+        s1.record(stream)
+        torch.cuda.synchronize()
+        return s0.elapsed_time(s1) / reps
+
+    out = {"workload": "hernquist N=262144 eps=0.01 bucket=16 theta=0.6"}
+    with GravitySimulation(max_particles_per_leaf=16, theta=0.6, precision="mixed") as plain:
+        plain.set_stream(stream.cuda_stream)
+        plain.set_particles(q)
+        out["forward_ms_two_phase"] = timed(plain.start_down)
+    with GravitySimulation(max_particles_per_leaf=16, theta=0.6, precision="mixed", record_lists=True) as s:
+        s.set_stream(stream.cuda_stream)
+        s.set_particles(q)
+        out["forward_ms_recording_lists"] = timed(s.start_down)
+        s.start_down()
+        out["adjoint_ms"] = timed(lambda: s.adjoint(*cot))
+    out["adjoint_over_recording_forward"] = out["adjoint_ms"] / out["forward_ms_recording_lists"]
+    out["adjoint_over_two_phase_forward"] = out["adjoint_ms"] / out["forward_ms_two_phase"]
+    out["target"] = "adjoint <= 2.5 x one forward pass"
+    return out
 
 
 def extras(a, sim, p, world, rank, stream, value, shard=None):
@@ -534,29 +657,84 @@ def extras(a, sim, p, world, rank, stream, value, shard=None):
     diff = rel_errors((am["ax"], am["ay"], am["az"]), (a64["ax"], a64["ay"], a64["az"]))
     sim.set_precision(a.precision)
     v_other = n / float(np.mean(t64))
-    res["theta_sweep"] = theta_sweep(a, sim, tgt, (dax, day, daz), stream) if a.sweep else []
-    res["sph_density"] = sph_density_rate(a, sim, stream)
-    res["sph_pressure"] = sph_pressure_rate(a, sim, stream)
-    res["driver_step"] = driver_step_rate(a, sim, stream)
     res["precision_comparison"] = {
         f"{a.precision}_force_evals_per_s": value, f"{other}_force_evals_per_s": v_other,
         "ratio_mixed_over_fp64": (value / v_other) if a.precision == "mixed" else (v_other / value),
         f"{a.precision}_err_vs_direct": err_m, f"{other}_err_vs_direct": err_o,
         "mixed_vs_fp64_all_particles": diff, "targets": int(tgt.size), "target_seed": 43,
         f"{other}_ms_traverse": c64["ms_traverse"]}
+    import torch.cuda as tc
+    nsm = tc.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    sm_max = measured_peaks().get("sm_max_mhz") or 1965.0
+    peak64 = nsm * 64 * 2 * sm_max * 1e6 / 1e12
+
+    def fp64_roofline(c, kernel):
+        ach = (20.0 * c["n_pp"] + 66.0 * c["n_pc"]) / (c["ms_traverse"] / 1e3) / 1e12
+        return {"bound": "fp64", "achieved": ach, "peak": peak64, "unit": "TFLOP/s", "frac": ach / peak64,
+                "kernel": kernel, "flop_model": "20 per P2P pair + 66 per P2C evaluation",
+                "peak_source": f"nominal: {nsm} SMs x 64 FP64 lanes x 2 x {sm_max:.0f} MHz"}
+
+    if other == "fp64":
+        res["precision_comparison"]["fp64_roofline"] = fp64_roofline(c64, "traverse_f64")
+    if a.precision == "mixed":
+        # the FP64 comparator built like the mixed form (same lists and layout)
+        fl = timed_form(a, sim, tgt, (dax, day, daz), stream, "fp64_lists", 2)
+        cl = sim.counters()
+        sim.set_precision(a.precision)
+        pc = res["precision_comparison"]
+        pc["fp64_lists_force_evals_per_s"] = fl["force_evals_per_s"]
+        pc["fp64_lists_err_vs_direct"] = fl["err_vs_direct"]
+        pc["fp64_lists_ms_traverse"] = cl["ms_traverse"]
+        pc["ratio_mixed_over_fp64_lists"] = value / fl["force_evals_per_s"]
+        pc["fp64_lists_roofline"] = fp64_roofline(cl, "walk_lists + eval_p2c_f64 + eval_p2p_f64")
+        pc["forms"] = {"mixed": "FP32 interactions over the two-phase lists",
+                       "fp64_lists": "FP64 interactions over the same two-phase lists and work layout",
+                       "fp64": "the ordered FP64 walk, bit-exact with the reference"}
+    res["theta_sweep"] = theta_sweep(a, sim, tgt, (dax, day, daz), stream) if a.sweep else []
+    res["accuracy_clause"] = accuracy_clause(a, sim, tgt, (dax, day, daz), stream)
+    res["sph_density"] = sph_density_rate(a, sim, stream)
+    res["sph_pressure"] = sph_pressure_rate(a, sim, stream)
+    res["driver_step"] = driver_step_rate(a, sim, stream)
+    res["adjoint_cost"] = adjoint_cost(a, stream)
     # CPU baseline: the reference's gravity sources on the host cores
     try:
         threads = os.cpu_count() or 1
-        v, desc = reference_sample(p, a, threads, seconds=a.cpu_seconds)
-        res["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "reference", "sample": desc}
+        v, info = reference_sample(p, a, threads, seconds=a.cpu_seconds)
+        res["cpu_baseline"] = dict({"value": v, "unit": UNIT, "cores": threads, "kind": "reference"}, **info)
         # one core, for the scaling of the reference's own code over the host threads
-        v1, desc1 = reference_sample(p, a, 1, seconds=max(1.0, a.cpu_seconds / 4))
-        res["cpu_baseline"]["single_core"] = {"value": v1, "sample": desc1,
-                                              "threads_speedup": v / v1 if v1 else None}
+        v1, info1 = reference_sample(p, a, 1, seconds=max(1.0, a.cpu_seconds / 4))
+        res["cpu_baseline"]["single_core"] = dict({"value": v1, "threads_speedup": v / v1 if v1 else None}, **info1)
+        res["cpu_baseline"]["configs"] = cpu_baseline_configs(a, threads, v, info)
     except Exception as e:  # reported, not fatal
         res["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                                "sample": f"failed: {e}"}
     return res
+
+
+def cpu_baseline_configs(a, threads, v_c2, info_c2):
+    """The reference's CPU path at the smaller workloads as well: the 10,000
+    particle Plummer sphere (eps 0.01, bucket 16) and the 2^20 mixture (eps
+    1e-4, bucket 16), theta 0.7, one full force pass each on all host threads
+    and on one, beside the bench workload's own figure."""
+    from paratreet_b200 import ics
+    rows = {}
+    for name, gen, kw in (("plummer_10k", ics.plummer, dict(n=10000, seed=42, soft=0.01)),
+                          ("mixture_1m", ics.mixture, dict(n=1 << 20, seed=7, soft=1e-4))):
+        q = gen(**kw)
+        label = f"{name}: N={kw['n']} eps={kw['soft']} bucket=16 theta=0.7"
+        row = {}
+        for th, budget in ((threads, 60.0), (1, 20.0)):
+            v, info = reference_sample(q, a, th, seconds=budget, bucket=16, theta=0.7, label=label)
+            row[f"threads_{th}"] = {"value": v, "sampled_fraction": info["sampled_fraction"],
+                                   "build_s": info["build_s"], "traversal_s_scaled": info["traversal_s_scaled"],
+                                   "charm_equivalent": f"+p {th}"}
+        rows[name] = dict(row, workload=label, unit=UNIT)
+    rows["plummer_16m"] = {"workload": info_c2["workload"], "unit": UNIT,
+                           f"threads_{threads}": {"value": v_c2, "sampled_fraction": info_c2["sampled_fraction"],
+                                                  "build_s": info_c2["build_s"],
+                                                  "traversal_s_scaled": info_c2["traversal_s_scaled"],
+                                                  "charm_equivalent": f"+p {threads}"}}
+    return rows
 
 
 if __name__ == "__main__":

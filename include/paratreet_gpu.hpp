@@ -80,7 +80,7 @@ struct Configuration {
   int max_particles_per_leaf = 16;  // -l
   double theta = 0.7;
   double max_timestep = 1e-5;       // -j
-  int precision = PT_FP64;          // PT_FP64 (reference-exact) or PT_MIXED
+  int precision = PT_FP64;          // PT_FP64 (reference-exact), PT_MIXED or PT_FP64_LISTS
   int integrator = PT_KKD;          // PT_KKD (Driver::run) or PT_KDK
   int device = 0;
   bool periodic = false;            // bPeriodic

@@ -46,9 +46,13 @@ enum {
 enum {
   PT_FP64 = 0,  /* reference-exact FP64 (bit-identical to the reference built
                    with -DUSE_DOUBLE_FP) */
-  PT_MIXED = 1  /* FP64 positions, tree and opening tests; FP32 P2P / P2C
+  PT_MIXED = 1,  /* FP64 positions, tree and opening tests; FP32 P2P / P2C
                    interactions on bucket-relative offsets with compensated
                    FP32 accumulation */
+  PT_FP64_LISTS = 2  /* the mixed form's two-phase traversal (same lists, same
+                        work layout) with FP64 interactions: the FP64
+                        comparator of PT_MIXED; equal to PT_FP64 up to the
+                        order of each particle's sums (not bit-exact) */
 };
 
 /* Traverser of the FP64 form (the interaction set is the same; the order in
@@ -129,6 +133,16 @@ const char* pt_last_error(const pt_handle* h);
 int pt_set_stream(pt_handle* h, void* stream);
 int pt_set_theta(pt_handle* h, double theta);
 int pt_set_precision(pt_handle* h, int precision);
+/* Failure-path control of the key sort, for tests.  Each digit pass of the
+ * onesweep radix sort (the replacement of std::sort at src/Subtree.h:281)
+ * resolves its tile's offsets by looking back at the tiles before it; a look-
+ * back polls a tile that has not yet published its counts at most `polls`
+ * times (default 2^21, which is never reached in practice) and then gives up.
+ * The force pass then stops before it permutes the particles and returns
+ * PT_E_DEVICE ("radix sort look-back timed out"); the handle keeps its last
+ * consistent state and the next call sorts afresh.  0 gives up at the first
+ * poll of an unpublished tile.  polls < 0 is PT_E_ARG. */
+int pt_set_sort_spin_limit(pt_handle* h, int64_t polls);
 
 /* Particles -------------------------------------------------------------- */
 /* Replaces Reader::load + the universe reduction (src/Reader.C:11-107,
@@ -197,10 +211,23 @@ int pt_get_tree(pt_handle* h, uint64_t* keys, int32_t* ints4, double* dbls18);
 /* Keys of the buckets (leaves) in DFS order (Subtree::leaves). */
 int pt_get_bucket_keys(pt_handle* h, uint64_t* keys);
 /* Interaction lists of the last pass (needs record_lists): CSR over buckets
- * in DFS order; entries are node keys in traversal order, kinds 0 = leaf()
- * P2P, 1 = node() P2C. */
+ * in DFS order; entries are node keys, kinds 0 = leaf() P2P, 1 = node() P2C.
+ * PT_FP64 records them in the reference's traversal order; the two-phase
+ * forms (PT_MIXED, PT_FP64_LISTS) record the lists their walk wrote (per
+ * bucket its leaves, then its nodes) -- the same sets. */
 int pt_get_lists_size(pt_handle* h, int64_t* total);
 int pt_get_lists(pt_handle* h, int64_t* offsets, uint64_t* keys, int32_t* kinds);
+/* Per bucket (DFS order), an order-independent 64-bit digest of its
+ * interaction list in the last pass and the list's length: the sum mod 2^64
+ * of a mix of (node, class) over the entries, class 0 = leaf() P2P,
+ * 1 = node() quadrupole P2C, 2 = node() monopole P2C (addGravity).  which = 0:
+ * the recorded lists (record_lists, the FP64 walk in the reference's order);
+ * which = 1: the lists that the mixed form's two-phase walk wrote and
+ * evaluated in its last pass (non-periodic, every bucket).  Equal digests of
+ * the two show that both forms make the same interactions (the traversal of
+ * src/Traverser.h:154-217 with GravityVisitor::open / node / leaf) without
+ * copying the lists to the host.  PT_E_STATE if the lists are not there. */
+int pt_get_list_digests(pt_handle* h, int which, uint64_t* digest, int64_t* count);
 int pt_get_counters(pt_handle* h, pt_counters* c);
 /* P2P pairs + P2C evaluations of each bucket (DFS order, pt_get_tree_size
  * buckets) in the last force pass, replicas included; 0 for buckets outside
@@ -304,9 +331,11 @@ int pt_ewald_direct_sum(pt_handle* h, int64_t nt, const int32_t* targets, double
  * loads it until exit, which limits nt to 262,136 (larger nt is rejected with
  * PT_E_ARG).  Works on the current device; the first call on a device looks up
  * the array's address (make that call before any stream capture).  Issued on
- * `stream` (cudaStream_t, NULL = default) and synchronised before return.
- * Calls that overlap on the GPU share the array and race.  On error a message
- * is written to errbuf (errlen bytes, may be NULL). */
+ * `stream` (cudaStream_t, NULL = default); every call copies a status word to
+ * host memory and synchronises `stream` before it returns.  A target index
+ * outside [0, n) is found on the device and returned as PT_E_ARG with nothing
+ * written to the outputs.  Calls that overlap on the GPU share the array and
+ * race.  On error a message is written to errbuf (errlen bytes, may be NULL). */
 int pt_direct_sum_noalloc(int64_t n, const double* x, const double* y, const double* z,
                           const double* m, const double* soft, int64_t nt, const int32_t* targets,
                           double* ax, double* ay, double* az, double* pot, void* stream,

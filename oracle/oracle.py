@@ -73,6 +73,8 @@ def _port_lib():
         lib.pto_sph_pressure.argtypes = [C.c_int] + [_dp] * 10 + [_i32p, _dp, C.c_int] + [_dp] * 4
         lib.pto_set_periodic.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_double, C.c_double]
         lib.pto_set_traversal.argtypes = [C.c_void_p, C.c_int]
+        lib.pto_get_mono.argtypes = [C.c_void_p]
+        lib.pto_get_mono.restype = C.c_ulonglong
         lib.pto_ewald_direct.argtypes = [C.c_int] + [_dp] * 5 + [C.c_double, C.c_int, _i32p] + [_dp] * 4 + [C.c_int]
         _port = lib
     return _port
@@ -202,6 +204,10 @@ class PortSim(_Sim):
 
     def forces(self, record_lists=False):
         self._lib.pto_forces(self._h, 1 if record_lists else 0)
+
+    def mono_count(self):
+        """node() calls of the last pass that took the monopole fallback."""
+        return int(self._lib.pto_get_mono(self._h))
 
     def run(self, nsteps):
         self._lib.pto_run(self._h, nsteps)

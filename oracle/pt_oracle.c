@@ -57,6 +57,7 @@ struct pto_sim {
   int* list_kind;
   long list_total, list_cap;
   unsigned long long n_pp, n_pc, n_open;
+  unsigned long long n_mono; /* node() calls that took the monopole fallback */
   double t_build, t_trav;
   /* periodic cube (examples/Gravity.C:34-50, examples/Ewald.{h,C}) */
   int periodic, n_replicas;
@@ -521,11 +522,12 @@ static void visit_leaf(pto_sim* s, int src, int tgt, const double off[3]) {
 }
 
 /* GravityVisitor::node, :184-224 (non-HEXADECAPOLE :207-221), with the
- * unsoftened monopole fallback addGravity, :130-139. */
-static void visit_node(pto_sim* s, int src, int tgt, const double off[3]) {
+ * unsoftened monopole fallback addGravity, :130-139.  Returns 1 when the
+ * monopole fallback was taken. */
+static int visit_node(pto_sim* s, int src, int tgt, const double off[3]) {
   const pto_mom* q = &s->mom[src];
   const pto_mom* t = &s->mom[tgt];
-  if (q->count == 0) return;
+  if (q->count == 0) return 0;
   int t0 = s->npstart[tgt], tn = s->nnp[tgt];
   if (open_softening(q, t, off)) {
     for (int i = t0; i < t0 + tn; i++) {
@@ -541,7 +543,7 @@ static void visit_node(pto_sim* s, int src, int tgt, const double off[3]) {
         s->potf[i] += -q->mass / sqrt(rsq);
       }
     }
-    return;
+    return 1;
   }
   for (int i = t0; i < t0 + tn; i++) {
     double rx = (s->x[i] - q->cm[0]) - off[0];
@@ -702,7 +704,7 @@ static void walk(pto_sim* s, int tgt, double gfac, int record, unsigned long lon
         int c0 = s->nchild[nd];
         for (int c = 7; c >= 0; c--) stack[sp++] = c0 + c;
       } else {
-        visit_node(s, nd, tgt, off);
+        cnt[3] += (unsigned long long)visit_node(s, nd, tgt, off);
         cnt[1] += (unsigned long long)s->nnp[tgt];
         if (record) list_push(s, s->nkey[nd], 1);
       }
@@ -730,7 +732,7 @@ static void walk_bfs(pto_sim* s, int tgt, double gfac, int record, unsigned long
         int c0 = s->nchild[nd];
         for (int c = 0; c < 8; c++) queue[tail++] = c0 + c;
       } else {
-        visit_node(s, nd, tgt, off);
+        cnt[3] += (unsigned long long)visit_node(s, nd, tgt, off);
         cnt[1] += (unsigned long long)s->nnp[tgt];
         if (record) list_push(s, s->nkey[nd], 1);
       }
@@ -757,17 +759,17 @@ static void traverse(pto_sim* s, int record) {
   memset(s->az, 0, sizeof(double) * s->n);
   memset(s->pot, 0, sizeof(double) * s->n);
   memset(s->potf, 0, sizeof(double) * s->n);
-  unsigned long long pp = 0, pc = 0, op = 0;
+  unsigned long long pp = 0, pc = 0, op = 0, mo = 0;
   const double zero[3] = {0.0, 0.0, 0.0};
   if (record) {
     free(s->list_off);
     s->list_off = (long*)malloc(sizeof(long) * (s->nleaves + 1));
     s->list_total = 0;
     for (long b = 0; b < s->nleaves; b++) {
-      unsigned long long c[3] = {0, 0, 0};
+      unsigned long long c[4] = {0, 0, 0, 0};
       s->list_off[b] = s->list_total;
       walk_any(s, s->leaves[b], gfac, 1, c, zero);
-      pp += c[0]; pc += c[1]; op += c[2];
+      pp += c[0]; pc += c[1]; op += c[2]; mo += c[3];
     }
     s->list_off[s->nleaves] = s->list_total;
   } else {
@@ -778,12 +780,12 @@ static void traverse(pto_sim* s, int record) {
         for (int Z = -nr; Z <= nr; Z++) {
           const double off[3] = {X * s->period, Y * s->period, Z * s->period};
 #ifdef _OPENMP
-#pragma omp parallel for schedule(dynamic, 16) reduction(+ : pp, pc, op) num_threads(s->threads)
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : pp, pc, op, mo) num_threads(s->threads)
 #endif
           for (long b = 0; b < s->nleaves; b++) {
-            unsigned long long c[3] = {0, 0, 0};
+            unsigned long long c[4] = {0, 0, 0, 0};
             walk_any(s, s->leaves[b], gfac, 0, c, s->periodic ? off : zero);
-            pp += c[0]; pc += c[1]; op += c[2];
+            pp += c[0]; pc += c[1]; op += c[2]; mo += c[3];
           }
         }
     if (s->periodic) ewald_correction(s);
@@ -791,6 +793,7 @@ static void traverse(pto_sim* s, int record) {
   s->n_pp = pp;
   s->n_pc = pc;
   s->n_open = op;
+  s->n_mono = mo;
 }
 
 /* ---------------------------------------------------------------- API */
@@ -933,6 +936,8 @@ void pto_get_counters(const pto_sim* s, unsigned long long* out4, double* times2
 }
 
 long pto_num_nodes(const pto_sim* s) { return s->nnodes; }
+
+unsigned long long pto_get_mono(const pto_sim* s) { return s->n_mono; }
 
 void pto_get_nodes(const pto_sim* s, uint64_t* keys, int* ints4, double* d18) {
   for (long i = 0; i < s->nnodes; i++) {

@@ -37,6 +37,7 @@ void pto_get_state(const pto_sim* s, double* x, double* y, double* z, double* vx
 void pto_get_universe(const pto_sim* s, double* lo3, double* hi3);
 /* counters: n_pp, n_pc, n_open, n_buckets; times: build, traverse seconds */
 void pto_get_counters(const pto_sim* s, unsigned long long* out4, double* times2, double* last_dt);
+unsigned long long pto_get_mono(const pto_sim* s);
 long pto_num_nodes(const pto_sim* s);
 /* Same layout as the reference-side dump: ints [type, depth, count, n_children],
  * 18 doubles [mass, cm3, soft, radius, xx, xy, xz, yy, yz, zz, lo3, hi3]. */

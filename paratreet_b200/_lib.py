@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libpt_gravity.so")
 
 PT_OK = 0
-PT_FP64, PT_MIXED = 0, 1
+PT_FP64, PT_MIXED, PT_FP64_LISTS = 0, 1, 2
 PT_KKD, PT_KDK = 0, 1
 PT_TRANSPOSED_DOWN, PT_BASIC_DOWN = 0, 1
 
@@ -81,6 +81,7 @@ SIGNATURES = {
     "pt_set_stream": (C.c_int, [_vp, _vp]),
     "pt_set_theta": (C.c_int, [_vp, C.c_double]),
     "pt_set_precision": (C.c_int, [_vp, C.c_int]),
+    "pt_set_sort_spin_limit": (C.c_int, [_vp, _i64]),
     "pt_set_particles": (C.c_int, [_vp, _i64] + [_vp] * 8),
     "pt_set_particles_device": (C.c_int, [_vp, _i64] + [_vp] * 8),
     "pt_num_particles": (_i64, [_vp]),
@@ -98,6 +99,7 @@ SIGNATURES = {
     "pt_get_bucket_keys": (C.c_int, [_vp, _vp]),
     "pt_get_lists_size": (C.c_int, [_vp, C.POINTER(_i64)]),
     "pt_get_lists": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "pt_get_list_digests": (C.c_int, [_vp, C.c_int, _vp, _vp]),
     "pt_get_counters": (C.c_int, [_vp, C.POINTER(PtCounters)]),
     "pt_direct_sum": (C.c_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp]),
     "pt_ewald_direct_sum": (C.c_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp]),

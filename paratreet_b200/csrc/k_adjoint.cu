@@ -5,16 +5,17 @@
 // for the interactions recorded by the last force pass (each bucket's leaf()
 // P2P sources and node() P2C nodes, examples/GravityVisitor.h:130-224).
 //
-//  adjoint_lists   one warp per bucket, lanes = targets, FP64:
+//  adjoint_lists   one warp per bucket, FP64 (work layout at AdjWarp below):
 //    P2P  a_i += m_j b(r) d,  d = x_j - x_i (SPLINE, :87-120).  The tidal
 //         tensor T = b I + (b'(r)/r) d d^T gives xbar_i -= m_j T abar_i,
-//         xbar_j += m_j T abar_i, mbar_j += b d.abar_i (source terms summed over
-//         the warp's targets, then one atomic add per source).
+//         xbar_j += m_j T abar_i, mbar_j += b d.abar_i (source terms summed
+//         in shared memory over the bucket's targets, then one atomic add per
+//         source).
 //    P2C  a_i += f(r) with r = x_i - cm, f = -(bM + d q - c tr) r + c Q r
 //         (quadrupole, unsoftened branch) or f = -M r / r^3 (monopole).  The
 //         symmetric Jacobian J = df/dr gives xbar_i += J abar_i, and the
 //         node receives cmbar -= J abar_i, Mbar += df/dM . abar_i and the six
-//         Qbar components, summed over the warp and added atomically.
+//         Qbar components, summed in shared memory and added atomically.
 //  adjoint_upward  the upward pass (examples/MultipoleMoments.h:204-353) in
 //         closed form: M = sum m_k, cm = sum m_k x_k / M,
 //         Q_ab = sum m_k (x_k - cm)_a (x_k - cm)_b, so every internal ancestor
@@ -37,10 +38,10 @@ __device__ __forceinline__ double wsum(double v) {
   return v;
 }
 
-// SPLINE force term b(r) and its derivative db/dr.
-__device__ __forceinline__ void spline_b_db(double r2, double twoh, double& b, double& db) {
-  const double r = sqrt(r2);
-  if (r < twoh) {
+// SPLINE force term b(r) and its derivative db/dr, from r^2 and 1/r.
+__device__ __forceinline__ void spline_b_db(double r2, double ir, double twoh, double& b, double& db) {
+  if (r2 < twoh * twoh) {
+    const double r = r2 * ir;
     const double dih = 2.0 / twoh;
     const double u = r * dih;
     const double d3 = dih * dih * dih, d4 = d3 * dih;
@@ -48,22 +49,151 @@ __device__ __forceinline__ void spline_b_db(double r2, double twoh, double& b, d
       b = d3 * (4.0 / 3.0 - 6.0 / 5.0 * u * u + 0.5 * u * u * u);
       db = d4 * (-12.0 / 5.0 * u + 1.5 * u * u);
     } else {
-      const double ir = 1.0 / r;
       const double ir3 = ir * ir * ir;
       b = -1.0 / 15.0 * ir3 + d3 * (8.0 / 3.0 - 3.0 * u + 6.0 / 5.0 * u * u - 1.0 / 6.0 * u * u * u);
       db = 0.2 * ir3 * ir + d4 * (-3.0 + 12.0 / 5.0 * u - 0.5 * u * u);
     }
   } else {
-    const double ir = 1.0 / r;
     b = ir * ir * ir;
     db = -3.0 * b * ir;
   }
 }
 
+// Work layout of adjoint_lists: one warp per bucket, the bucket's n_t targets
+// replicated over G = floor(32 / n_t) lane groups (as the evaluation kernels
+// do).  A chunk of up to 32 list nodes, or of 32 source particles of the
+// listed leaves, is staged in shared memory with one adjoint accumulator row
+// per staged slot; group g takes the slots g, g + G, ...  Inside a group, at
+// step s lane t handles its group's slot number (s + t) mod L (L = max(n_t,
+// the group's slots)), so no two lanes touch one slot in a step and each
+// (target, slot) pair is visited once; a __syncwarp separates the steps.  The
+// target-side terms stay in registers; the source-side ones are added to the
+// slot's row and flushed with one atomic add per slot and value after the
+// chunk.  Atomic adds make the last bits of the results order-dependent.
+struct AdjWarp {
+  double st[12][32];   // staged slot data: P2C cm x/y/z, M, xx, xy, xz, yy, yz, zz, kind, soft; P2P x/y/z, m, soft
+  double acc[10][32];  // per slot adjoint rows: node (cm x/y/z, M, 6 moments) or source (x/y/z, m)
+  int32_t sidx[32];    // the slot's node or particle index
+  int32_t lnode[32];   // P2P: the window's leaves
+  int32_t lincl[32];   // P2P: inclusive prefix of their particle counts
+};
+
+struct AdjTarget {
+  int t, grp, G, nt;
+  bool act;
+  double x, y, z, s, ax, ay, az;
+};
+
+// One P2C pair (target, staged node k): target-side Jacobian term j (added to
+// the target's registers) and the ten node-side terms (added to row k).
+__device__ __forceinline__ void adj_p2c_pair(AdjWarp& w, int k, const AdjTarget& x, double& gx, double& gy,
+                                             double& gz, unsigned* status) {
+  const double rx = x.x - w.st[0][k], ry = x.y - w.st[1][k], rz = x.z - w.st[2][k];
+  const double M = w.st[3][k];
+  const double r2 = rx * rx + ry * ry + rz * rz;
+  const double ir = rsqrt(r2);
+  const double ir2 = ir * ir;
+  const double ra = rx * x.ax + ry * x.ay + rz * x.az;
+  double c[10];
+  double jx, jy, jz;
+  if (w.st[10][k] == 2.0) {  // monopole: f = -M r / r^3
+    const double b3 = ir2 * ir;
+    const double t = 3.0 * b3 * ir2 * ra;
+    jx = -M * (b3 * x.ax - t * rx);
+    jy = -M * (b3 * x.ay - t * ry);
+    jz = -M * (b3 * x.az - t * rz);
+#pragma unroll
+    for (int q = 4; q < 10; q++) c[q] = 0.0;
+    c[3] = -b3 * ra;
+  } else {
+    const double twoh = w.st[11][k] + x.s;
+    if (r2 < twoh * twoh) {  // the softened quadrupole branch: reported, not differentiated
+      atomicOr(status, kErrAdjointSoftened);
+      return;
+    }
+    const double xx = w.st[4][k], xy = w.st[5][k], xz = w.st[6][k];
+    const double yy = w.st[7][k], yz = w.st[8][k], zz = w.st[9][k];
+    const double bb = ir2 * ir, cc = 3.0 * bb * ir2, dd = 5.0 * cc * ir2, ee = 7.0 * dd * ir2;
+    const double qx = xx * rx + xy * ry + xz * rz;
+    const double qy = xy * rx + yy * ry + yz * rz;
+    const double qz = xz * rx + yz * ry + zz * rz;
+    const double qq = 0.5 * (qx * rx + qy * ry + qz * rz);
+    const double tr = 0.5 * (xx + yy + zz);
+    const double s = bb * M + dd * qq - cc * tr;
+    const double qra = qx * x.ax + qy * x.ay + qz * x.az;
+    const double qax = xx * x.ax + xy * x.ay + xz * x.az;
+    const double qay = xy * x.ax + yy * x.ay + yz * x.az;
+    const double qaz = xz * x.ax + yz * x.ay + zz * x.az;
+    const double k1 = (cc * M + ee * qq - dd * tr) * ra - dd * qra;
+    jx = -s * x.ax + k1 * rx + cc * qax - dd * ra * qx;
+    jy = -s * x.ay + k1 * ry + cc * qay - dd * ra * qy;
+    jz = -s * x.az + k1 * rz + cc * qaz - dd * ra * qz;
+    c[3] = -bb * ra;
+    const double h = -dd * ra;
+    c[4] = h * 0.5 * rx * rx + cc * ra * 0.5 + cc * x.ax * rx;
+    c[5] = h * 0.5 * ry * ry + cc * ra * 0.5 + cc * x.ay * ry;
+    c[6] = h * 0.5 * rz * rz + cc * ra * 0.5 + cc * x.az * rz;
+    c[7] = h * rx * ry + cc * (x.ax * ry + x.ay * rx);
+    c[8] = h * rx * rz + cc * (x.ax * rz + x.az * rx);
+    c[9] = h * ry * rz + cc * (x.ay * rz + x.az * ry);
+  }
+  gx += jx;
+  gy += jy;
+  gz += jz;
+  c[0] = -jx;
+  c[1] = -jy;
+  c[2] = -jz;
+#pragma unroll
+  for (int q = 0; q < 10; q++) w.acc[q][k] += c[q];
+}
+
+// One P2P pair (target, staged source k): T = b I + (b'/r) d d^T with
+// d = x_k - x_i; the target gets -m_k T abar_i, the source +m_k T abar_i and
+// mbar_k += b d.abar_i.
+__device__ __forceinline__ void adj_p2p_pair(AdjWarp& w, int k, const AdjTarget& x, double& gx, double& gy,
+                                             double& gz) {
+  const double dx = w.st[0][k] - x.x, dy = w.st[1][k] - x.y, dz = w.st[2][k] - x.z;
+  const double r2 = dx * dx + dy * dy + dz * dz;
+  if (r2 == 0.0) return;
+  const double ir = rsqrt(r2);
+  double bb, db;
+  spline_b_db(r2, ir, w.st[4][k] + x.s, bb, db);
+  const double da = dx * x.ax + dy * x.ay + dz * x.az;
+  const double kk = db * ir * da;
+  const double mj = w.st[3][k];
+  const double sx = mj * (bb * x.ax + kk * dx), sy = mj * (bb * x.ay + kk * dy), sz = mj * (bb * x.az + kk * dz);
+  gx -= sx;
+  gy -= sy;
+  gz -= sz;
+  w.acc[0][k] += sx;
+  w.acc[1][k] += sy;
+  w.acc[2][k] += sz;
+  w.acc[3][k] += bb * da;
+}
+
+// The rotation over the n staged slots of a chunk (see AdjWarp); kP2C picks
+// the pair kind.  Every lane runs the same number of steps.
+template <bool kP2C>
+__device__ __forceinline__ void adj_rotate(AdjWarp& w, int n, const AdjTarget& x, double& gx, double& gy,
+                                           double& gz, unsigned* status) {
+  const int mg = (x.grp < x.G && x.grp < n) ? (n - x.grp + x.G - 1) / x.G : 0;  // this group's slots
+  const int mmax = (n + x.G - 1) / x.G;
+  const int L = max(x.nt, mmax);
+  for (int st = 0; st < L; st++) {
+    const int local = (st + x.t) % L;
+    if (x.act && local < mg) {
+      const int k = x.grp + x.G * local;
+      if (kP2C) adj_p2c_pair(w, k, x, gx, gy, gz, status);
+      else adj_p2p_pair(w, k, x, gx, gy, gz);
+    }
+    __syncwarp();
+  }
+}
+
 __global__ void __launch_bounds__(kAdjWarps * 32) adjoint_lists(AdjParams A) {
-  __shared__ double stage[kAdjWarps][5][32];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  double(*st)[32] = stage[wid];
+  __shared__ AdjWarp warps[kAdjWarps];
+  AdjWarp& w = warps[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
   while (true) {
     unsigned bi = 0;
     if (lane == 0) bi = atomicAdd(A.work, 1u);
@@ -71,133 +201,143 @@ __global__ void __launch_bounds__(kAdjWarps * 32) adjoint_lists(AdjParams A) {
     const int64_t b = (int64_t)bi;
     if (b >= A.nbuckets) break;
     const int tnode = A.buckets[b];
+    if (tnode < 0 || tnode >= A.nnodes) {
+      if (lane == 0) atomicOr(A.status, kErrCapacity);
+      continue;
+    }
     const int tbase = A.walk[tnode].pstart, ntot = A.walk[tnode].pcount;
     const int64_t e0 = A.list_off[b], e1 = A.list_off[b + 1];
     for (int tc = 0; tc < ntot; tc += 32) {
       const int t0 = tbase + tc, nt = min(32, ntot - tc);
-      const bool act = lane < nt;
-      double xi = 0.0, yi = 0.0, zi = 0.0, si = 0.0, ax = 0.0, ay = 0.0, az = 0.0;
-      if (act) {
-        const int i = t0 + lane;
-        xi = A.p.x[i]; yi = A.p.y[i]; zi = A.p.z[i]; si = A.p.soft[i];
-        ax = A.cax[i]; ay = A.cay[i]; az = A.caz[i];
+      AdjTarget x;
+      x.nt = nt;
+      x.t = lane % nt;
+      x.grp = lane / nt;
+      x.G = 32 / nt;
+      x.act = x.grp < x.G;
+      x.x = x.y = x.z = x.s = x.ax = x.ay = x.az = 0.0;
+      if (x.act) {
+        const int i = t0 + x.t;
+        x.x = A.p.x[i]; x.y = A.p.y[i]; x.z = A.p.z[i]; x.s = A.p.soft[i];
+        x.ax = A.cax[i]; x.ay = A.cay[i]; x.az = A.caz[i];
       }
-      double gxi = 0.0, gyi = 0.0, gzi = 0.0;
-      for (int64_t e = e0; e < e1; e++) {
-        const int node = A.list_node[e];
-        const int kind = A.list_kind[e];
-        if (node < 0 || node >= A.nnodes) {
-          if (lane == 0) atomicOr(A.status, kErrCapacity);
-          continue;
-        }
-        const WalkRec w = A.walk[node];
-        if (kind == 0) {  // P2P with the leaf's particles
-          for (int base = 0; base < w.pcount; base += 32) {
-            const int cnt = min(32, w.pcount - base);
-            __syncwarp();
-            if (lane < cnt) {
-              const int j = w.pstart + base + lane;
-              st[0][lane] = A.p.x[j]; st[1][lane] = A.p.y[j]; st[2][lane] = A.p.z[j];
-              st[3][lane] = A.p.m[j]; st[4][lane] = A.p.soft[j];
-            }
-            __syncwarp();
-            for (int jj = 0; jj < cnt; jj++) {
-              double sx = 0.0, sy = 0.0, sz = 0.0, sm = 0.0;
-              if (act) {
-                const double dx = st[0][jj] - xi, dy = st[1][jj] - yi, dz = st[2][jj] - zi;
-                const double r2 = dx * dx + dy * dy + dz * dz;
-                if (r2 != 0.0) {
-                  double bb, db;
-                  spline_b_db(r2, st[4][jj] + si, bb, db);
-                  const double da = dx * ax + dy * ay + dz * az;
-                  const double k = db / sqrt(r2) * da;
-                  const double mj = st[3][jj];
-                  const double tx = bb * ax + k * dx, ty = bb * ay + k * dy, tz = bb * az + k * dz;
-                  sx = mj * tx; sy = mj * ty; sz = mj * tz;
-                  gxi -= sx; gyi -= sy; gzi -= sz;
-                  sm = bb * da;
-                }
-              }
-              sx = wsum(sx); sy = wsum(sy); sz = wsum(sz); sm = wsum(sm);
-              if (lane == 0) {
-                const int j = w.pstart + base + jj;
-                atomicAdd(&A.gx[j], sx);
-                atomicAdd(&A.gy[j], sy);
-                atomicAdd(&A.gz[j], sz);
-                atomicAdd(&A.gm[j], sm);
-              }
-            }
+      double gx = 0.0, gy = 0.0, gz = 0.0;
+      // P2C: the list's nodes, 32 at a time
+      for (int64_t win = e0; win < e1; win += 32) {
+        const int64_t e = win + lane;
+        int node = -1, kind = 0;
+        if (e < e1) {
+          kind = A.list_kind[e];
+          node = A.list_node[e];
+          if (node < 0 || node >= A.nnodes) {
+            atomicOr(A.status, kErrCapacity);
+            kind = 0;
+          } else if (kind != 0 && A.walk[node].count == 0) {
+            kind = 0;  // node() of an empty node adds nothing
           }
-        } else {  // P2C: quadrupole (kind 1) or softened-overlap monopole (kind 2)
+        }
+        const bool sel = e < e1 && kind != 0;
+        const unsigned m = __ballot_sync(kAdjFull, sel);
+        const int n = __popc(m);
+        if (n == 0) continue;
+        __syncwarp();
+        if (sel) {
+          const int k = __popc(m & ((1u << lane) - 1u));
+          const WalkRec& r = A.walk[node];
           const QuadRec q = A.quad[node];
-          double c[10];
+          w.sidx[k] = node;
+          w.st[0][k] = r.cm[0]; w.st[1][k] = r.cm[1]; w.st[2][k] = r.cm[2];
+          w.st[3][k] = q.mass;
+          w.st[4][k] = q.xx; w.st[5][k] = q.xy; w.st[6][k] = q.xz;
+          w.st[7][k] = q.yy; w.st[8][k] = q.yz; w.st[9][k] = q.zz;
+          w.st[10][k] = (double)kind;
+          w.st[11][k] = q.soft;
+        }
 #pragma unroll
-          for (int k = 0; k < 10; k++) c[k] = 0.0;
-          if (act && w.count > 0) {
-            const double rx = xi - w.cm[0], ry = yi - w.cm[1], rz = zi - w.cm[2];
-            const double r2 = rx * rx + ry * ry + rz * rz;
-            const double ir = 1.0 / sqrt(r2);
-            const double ir2 = ir * ir;
-            const double ra = rx * ax + ry * ay + rz * az;
-            double jx, jy, jz;
-            if (kind == 2) {  // f = -M r / r^3
-              const double b3 = ir2 * ir;
-              const double t = 3.0 * b3 * ir2 * ra;
-              jx = -q.mass * (b3 * ax - t * rx);
-              jy = -q.mass * (b3 * ay - t * ry);
-              jz = -q.mass * (b3 * az - t * rz);
-              c[3] = -b3 * ra;
-            } else {
-              const double twoh = q.soft + si;
-              if (r2 < twoh * twoh) {
-                atomicOr(A.status, kErrAdjointSoftened);
-                jx = jy = jz = 0.0;
-              } else {
-                const double bb = ir2 * ir, cc = 3.0 * bb * ir2, dd = 5.0 * cc * ir2, ee = 7.0 * dd * ir2;
-                const double qx = q.xx * rx + q.xy * ry + q.xz * rz;
-                const double qy = q.xy * rx + q.yy * ry + q.yz * rz;
-                const double qz = q.xz * rx + q.yz * ry + q.zz * rz;
-                const double qq = 0.5 * (qx * rx + qy * ry + qz * rz);
-                const double tr = 0.5 * (q.xx + q.yy + q.zz);
-                const double s = bb * q.mass + dd * qq - cc * tr;
-                const double qra = qx * ax + qy * ay + qz * az;
-                const double qax = q.xx * ax + q.xy * ay + q.xz * az;
-                const double qay = q.xy * ax + q.yy * ay + q.yz * az;
-                const double qaz = q.xz * ax + q.yz * ay + q.zz * az;
-                const double k1 = (cc * q.mass + ee * qq - dd * tr) * ra - dd * qra;
-                jx = -s * ax + k1 * rx + cc * qax - dd * ra * qx;
-                jy = -s * ay + k1 * ry + cc * qay - dd * ra * qy;
-                jz = -s * az + k1 * rz + cc * qaz - dd * ra * qz;
-                c[3] = -bb * ra;
-                const double h = -dd * ra;
-                c[4] = h * 0.5 * rx * rx + cc * ra * 0.5 + cc * ax * rx;
-                c[5] = h * 0.5 * ry * ry + cc * ra * 0.5 + cc * ay * ry;
-                c[6] = h * 0.5 * rz * rz + cc * ra * 0.5 + cc * az * rz;
-                c[7] = h * rx * ry + cc * (ax * ry + ay * rx);
-                c[8] = h * rx * rz + cc * (ax * rz + az * rx);
-                c[9] = h * ry * rz + cc * (ay * rz + az * ry);
-              }
+        for (int q = 0; q < 10; q++) w.acc[q][lane] = 0.0;
+        __syncwarp();
+        adj_rotate<true>(w, n, x, gx, gy, gz, A.status);
+        if (lane < n) {
+          double* na = A.nadj + 10 * (int64_t)w.sidx[lane];
+#pragma unroll
+          for (int q = 0; q < 10; q++) atomicAdd(na + q, w.acc[q][lane]);
+        }
+        __syncwarp();
+      }
+      // P2P: the listed leaves' particles, 32 at a time
+      for (int64_t win = e0; win < e1; win += 32) {
+        const int64_t e = win + lane;
+        int node = -1;
+        bool sel = false;
+        if (e < e1 && A.list_kind[e] == 0) {
+          node = A.list_node[e];
+          sel = node >= 0 && node < A.nnodes;
+        }
+        const unsigned m = __ballot_sync(kAdjFull, sel);
+        const int nl = __popc(m);
+        if (nl == 0) continue;
+        const int cnt = sel ? A.walk[node].pcount : 0;
+        int inc = cnt;
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(kAdjFull, inc, o);
+          if (lane >= o) inc += y;
+        }
+        const int total = __shfl_sync(kAdjFull, inc, 31);
+        __syncwarp();
+        if (sel) {
+          const int k = __popc(m & ((1u << lane) - 1u));
+          w.lnode[k] = node;
+          w.lincl[k] = inc;
+        }
+        __syncwarp();
+        for (int cs = 0; cs < total; cs += 32) {
+          const int q = cs + lane;
+          const int n = min(32, total - cs);
+          if (q < total) {
+            int lo = 0, hi = nl - 1;  // the first leaf with inclusive prefix > q
+            while (lo < hi) {
+              const int mid = (lo + hi) >> 1;
+              if (w.lincl[mid] > q) hi = mid;
+              else lo = mid + 1;
             }
-            gxi += jx; gyi += jy; gzi += jz;
-            c[0] = -jx; c[1] = -jy; c[2] = -jz;
+            const int first = (lo == 0) ? 0 : w.lincl[lo - 1];
+            const int j = A.walk[w.lnode[lo]].pstart + (q - first);
+            w.sidx[lane] = j;
+            w.st[0][lane] = A.p.x[j]; w.st[1][lane] = A.p.y[j]; w.st[2][lane] = A.p.z[j];
+            w.st[3][lane] = A.p.m[j]; w.st[4][lane] = A.p.soft[j];
           }
 #pragma unroll
-          for (int k = 0; k < 10; k++) c[k] = wsum(c[k]);
-          if (lane < 10) {
-            double v = c[0];
-#pragma unroll
-            for (int k = 1; k < 10; k++)
-              if (lane == k) v = c[k];
-            atomicAdd(&A.nadj[10 * (int64_t)node + lane], v);
+          for (int r = 0; r < 4; r++) w.acc[r][lane] = 0.0;
+          __syncwarp();
+          adj_rotate<false>(w, n, x, gx, gy, gz, A.status);
+          if (lane < n) {
+            const int j = w.sidx[lane];
+            atomicAdd(&A.gx[j], w.acc[0][lane]);
+            atomicAdd(&A.gy[j], w.acc[1][lane]);
+            atomicAdd(&A.gz[j], w.acc[2][lane]);
+            atomicAdd(&A.gm[j], w.acc[3][lane]);
           }
+          __syncwarp();
         }
       }
-      if (act) {
+      // the target-side sums of the G groups
+      w.acc[0][lane] = gx;
+      w.acc[1][lane] = gy;
+      w.acc[2][lane] = gz;
+      __syncwarp();
+      if (lane < nt) {
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        for (int g = 0; g < x.G; g++) {
+          sx += w.acc[0][g * nt + lane];
+          sy += w.acc[1][g * nt + lane];
+          sz += w.acc[2][g * nt + lane];
+        }
         const int i = t0 + lane;
-        atomicAdd(&A.gx[i], gxi);
-        atomicAdd(&A.gy[i], gyi);
-        atomicAdd(&A.gz[i], gzi);
+        atomicAdd(&A.gx[i], sx);
+        atomicAdd(&A.gy[i], sy);
+        atomicAdd(&A.gz[i], sz);
       }
+      __syncwarp();
     }
   }
 }

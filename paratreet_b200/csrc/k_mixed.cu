@@ -589,11 +589,10 @@ void launch_prep_sources(const int32_t* buckets, int64_t nbuckets, const WalkRec
   prep_sources<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(buckets, nbuckets, walk, p, srcf, softf);
 }
 
-// variant: 0 = at most 6 CTAs/SM (80 registers), 1 = 5 CTAs/SM (no spills)
-void launch_traverse_mixed(const TravParams& P, const Mom* mom, int grid, int variant, cudaStream_t st) {
-  // 5 CTAs per SM (96 registers) by default; PT_MIXED_VARIANT=1 selects 6 CTAs (80 registers)
-  if (variant == 1) { note_launch(); traverse_mixed<6><<<grid, kMixWarps * 32, 0, st>>>(P, mom); }
-  else { note_launch(); traverse_mixed<5><<<grid, kMixWarps * 32, 0, st>>>(P, mom); }
+// 5 CTAs per SM (96 registers: at 80 the walk state spills)
+void launch_traverse_mixed(const TravParams& P, const Mom* mom, int grid, cudaStream_t st) {
+  note_launch();
+  traverse_mixed<5><<<grid, kMixWarps * 32, 0, st>>>(P, mom);
 }
 
 }  // namespace pt

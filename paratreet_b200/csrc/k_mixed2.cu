@@ -5,11 +5,14 @@
 // open / openSoftening, so the same leaf() and node() interactions) and
 // writes the bucket's interaction list to HBM: P2C node indices (bit 31 =
 // monopole, addGravity; bit 30 = near: a target may lie inside the node's
-// softening sphere) and P2P leaf indices (bit 31 = near: some pair may be
-// softened).  Each warp appends to regions it reserves from two global pools
-// at bucket boundaries, so every bucket's list is contiguous; a bucket that
-// outgrows what is left of its region sets kErrPool and the host repeats the
-// walk with larger regions.
+// softening sphere) and P2P leaf indices.  Whether a P2P leaf may hold a
+// softened pair, and how many source particles the leaves hold, are left to
+// eval_p2p, which reads every leaf record anyway: the walk is bound by its
+// instruction issue.  Each warp appends to regions it reserves from two global pools,
+// so every bucket's list is contiguous; a bucket that outgrows what is left of
+// its region moves its list so far to a new, larger region and goes on.  Only
+// a full pool sets kErrPool (the host then repeats the walk with larger
+// pools).
 //
 // Phase B (eval_p2c, eval_p2p): one warp per bucket streams its list in
 // chunks of 64 entries and evaluates them with the packed FP32 instructions
@@ -56,20 +59,46 @@ __device__ __forceinline__ bool ensure_region(Region& r, unsigned long long* cur
   return true;
 }
 
-// Write n buffered entries at the region cursor (false if they do not fit).
-__device__ __forceinline__ bool drain(const int32_t* buf, int n, Region& r, int32_t* __restrict__ pool, int lane) {
+// Append n buffered entries to the bucket's list, which occupies [start,
+// r.cur) of the warp's region.  When they do not fit, the list so far moves to
+// a new region of at least twice its new length (the rest of the old region
+// is left unused).  False only if the pool is full.  Every lane of the warp
+// calls it with the same arguments; the list's earlier entries were written
+// before the __syncwarp that ends each walk step.
+__device__ __forceinline__ bool drain(const int32_t* buf, int n, Region& r, unsigned long long& start,
+                                      int32_t* __restrict__ pool, unsigned long long* cursor, unsigned long long cap,
+                                      unsigned region, int lane) {
   if (n == 0) return true;
-  if (r.cur + (unsigned long long)n > r.end) return false;
+  if (r.cur + (unsigned long long)n > r.end) {
+    const unsigned long long len = r.cur - start;
+    const unsigned long long want = max((unsigned long long)region, 2ull * (len + (unsigned long long)n));
+    unsigned long long s = 0;
+    if (lane == 0) s = atomicAdd(cursor, want);
+    s = __shfl_sync(kFull, s, 0);
+    if (s + want > cap) {
+      r.cur = r.end = cap;
+      return false;
+    }
+    for (unsigned long long k = lane; k < len; k += 32) pool[s + k] = pool[start + k];
+    start = s;
+    r.cur = s + len;
+    r.end = s + want;
+  }
   for (int k = lane; k < n; k += 32) pool[r.cur + k] = buf[k];
   r.cur += (unsigned long long)n;
   return true;
 }
 
-__global__ void __launch_bounds__(kWlWarps * 32, 5) walk_lists(TravParams P, ListParams L, const Mom* __restrict__ mom) {
+// CTAs per SM of the walk (72 registers); 6 and 8 measured slower at N = 2^24
+#ifndef PT_WALK_MINB
+#define PT_WALK_MINB 7
+#endif
+__global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravParams P, ListParams L,
+                                                                         const Mom* __restrict__ mom) {
   __shared__ WalkWarp warps[kWlWarps];
   WalkWarp& w = warps[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
-  unsigned long long c_pp = 0, c_pc = 0, c_open = 0;
+  unsigned long long c_pc = 0, c_open = 0;
   unsigned max_len = 0;
   Region rpc{0, 0}, rpp{0, 0};
   bool pool_ok = true;
@@ -102,8 +131,8 @@ __global__ void __launch_bounds__(kWlWarps * 32, 5) walk_lists(TravParams P, Lis
     const BucketGeom g = w.geom;
     const double blo[3] = {g.lo[0], g.lo[1], g.lo[2]}, bhi[3] = {g.hi[0], g.hi[1], g.hi[2]};
     const int ntot = P.walk[tnode].pcount;
-    const unsigned long long pc0 = rpc.cur, pp0 = rpp.cur;
-    unsigned long long opens = 0, nsrc = 0;
+    unsigned long long pc0 = rpc.cur, pp0 = rpp.cur;  // the bucket's lists start here (moved on overflow)
+    unsigned long long opens = 0;
     int sp = 0, nc = 0, np = 0;
     int nexp = 1, pop = -1;
     bool ok = true, fits = true;
@@ -129,15 +158,11 @@ __global__ void __launch_bounds__(kWlWarps * 32, 5) walk_lists(TravParams P, Lis
       opens += (unsigned long long)__popc(__ballot_sync(kFull, node >= 0 && node < P.nnodes &&
                                                                     r.type == kTypeInternal));
       bool near = false;
-      if (cls == kClsP2P || cls == kClsQuad) {
-        // P2P: a pair may be softened; P2C: a target may be inside twoh of
-        // the centre (SPLINEQ's softened branch), with a relative margin.  A
-        // quadrupole node's box gap is the one its opening test measured.
-        if (cls == kClsP2P)
-          gap2 = box_gap2_exact(blo, bhi, __dadd_rn(r.cm[0], P.ox), __dadd_rn(r.cm[1], P.oy),
-                                __dadd_rn(r.cm[2], P.oz));
-        const double reach = (cls == kClsP2P) ? r.reach + r.soft_max + g.soft_max
-                                              : (r.soft + g.soft_max) * (1.0 + 1e-5);
+      if (cls == kClsQuad) {
+        // a target may be inside twoh of the centre (SPLINEQ's softened
+        // branch), with a relative margin; the box gap is the one the opening
+        // test measured
+        const double reach = (r.soft + g.soft_max) * (1.0 + 1e-5);
         near = !(gap2 > reach * reach);
       }
       {
@@ -151,9 +176,8 @@ __global__ void __launch_bounds__(kWlWarps * 32, 5) walk_lists(TravParams P, Lis
       {
         const bool pp = (cls == kClsP2P);
         const unsigned m = __ballot_sync(kFull, pp);
-        if (pp) w.ppbuf[np + __popc(m & ((1u << lane) - 1u))] = node | (near ? (int)0x80000000 : 0);
+        if (pp) w.ppbuf[np + __popc(m & ((1u << lane) - 1u))] = node;
         np += __popc(m);
-        nsrc += (unsigned long long)__reduce_add_sync(kFull, pp ? (unsigned)r.pcount : 0u);
       }
       {
         const bool op = (cls == kClsOpen);
@@ -168,11 +192,11 @@ __global__ void __launch_bounds__(kWlWarps * 32, 5) walk_lists(TravParams P, Lis
       __syncwarp();
       const bool last = (sp == 0);
       if (nc >= 32 || last) {
-        fits = drain(w.pcbuf, nc, rpc, L.pc_pool, lane) && fits;
+        fits = fits && drain(w.pcbuf, nc, rpc, pc0, L.pc_pool, L.cursor + 0, L.cap_pc, L.region, lane);
         nc = 0;
       }
       if (np >= 32 || last) {
-        fits = drain(w.ppbuf, np, rpp, L.pp_pool, lane) && fits;
+        fits = fits && drain(w.ppbuf, np, rpp, pp0, L.pp_pool, L.cursor + 1, L.cap_pp, L.region, lane);
         np = 0;
       }
       __syncwarp();
@@ -193,16 +217,14 @@ __global__ void __launch_bounds__(kWlWarps * 32, 5) walk_lists(TravParams P, Lis
     }
     max_len = max(max_len, max(npc, npp));
     c_pc += (unsigned long long)npc * (unsigned long long)ntot;
-    c_pp += nsrc * (unsigned long long)ntot;
     c_open += opens;
-    if (P.bucket_work && lane == 0) {
-      unsigned long long wk = ((unsigned long long)npc + nsrc) * (unsigned long long)ntot;
+    if (P.bucket_work && lane == 0) {  // eval_p2p adds the P2P pairs
+      unsigned long long wk = (unsigned long long)npc * (unsigned long long)ntot;
       if (P.accumulate) wk += P.bucket_work[b];
       P.bucket_work[b] = wk;
     }
   }
   if (lane == 0) {
-    atomicAdd(&P.counters[0], c_pp);
     atomicAdd(&P.counters[1], c_pc);
     atomicAdd(&P.counters[2], c_open);
     atomicMax(L.max_len, max_len);
@@ -211,13 +233,28 @@ __global__ void __launch_bounds__(kWlWarps * 32, 5) walk_lists(TravParams P, Lis
 
 // ---------------------------------------------------------------- phase B
 constexpr int kEvWarps = 4;
+// CTAs per SM of eval_p2c (80 registers); 7 and 8 fit without spills but
+// measured slower: their shared memory leaves less L1 for the node records
+#ifndef PT_P2C_MINB
+#define PT_P2C_MINB 6
+#endif
 
+// Per-warp shared memory of eval_p2p ...
 struct EvalWarp {
   BucketGeom geom;
-  float4 st[6][32];            // staged pairs: P2C six rows; P2P px, pz, pr
-  int32_t ps0[kWlBuf];         // P2P: first particle of each leaf - its stream position
-  float4 lof[kWlBuf];          // P2P: leaf offsets cm_leaf - cm_bucket (FP32)
-  int32_t lsel[kWlBuf];        // P2P: leaves of the current kind in a block
+  float4 st[6][32];            // staged source pairs px, pz, pr; rows 3-4 hold second-target sums
+  int32_t ps0[kWlBuf];         // first particle of each leaf - its stream position
+  float4 lof[kWlBuf];          // leaf offsets cm_leaf - cm_bucket (FP32)
+  int32_t lsel[kWlBuf];        // leaves of the current kind in a block
+};
+
+// ... and of eval_p2c (kept apart: shared memory taken from one kernel's
+// CTAs is L1 lost to its node records)
+struct EvalWarpC {
+  BucketGeom geom;
+  float4 st[6][32];            // staged node pairs, six rows
+  float4 ks[2][32];            // each lane's compensated sums and their compensations
+  int32_t spec[kWlBuf];        // the chunk's near and monopole entries (scalar pass)
 };
 
 // Per-lane target of a 32-target chunk, replicated over G lane groups (lanes
@@ -262,18 +299,17 @@ struct Kahan4 {
 
 // Two targets per lane (P2P): lane l of group l / h holds targets 2 (l % h)
 // and 2 (l % h) + 1 (h = ceil(nt / 2); t2 == nt when there is none), so each
-// staged source meets two targets per packed instruction.  Chosen for the
-// chunk sizes where it leaves fewer lanes idle than one target per lane.
+// staged source meets two targets per packed instruction.
 struct EvTarget2 {
   int t1, t2, grp, G, nt;
   float2 tx, ty, tz, ts;
 };
 
-__device__ __forceinline__ bool ev_two_targets(int nt) {
-  const int g1 = 32 / nt, it1 = (32 + g1 - 1) / g1;
-  const int h = (nt + 1) >> 1, g2 = 32 / h, it2 = 2 * ((32 + g2 - 1) / g2);
-  return it2 < it1;
-}
+// Two targets per lane wherever there are two: each staged source pair then
+// meets four targets' worth of work per iteration, which halves the shared-
+// memory loads and loop overhead per interaction (measured 1.7 ms faster at
+// N = 2^24 than choosing it only where it takes fewer iterations).
+__device__ __forceinline__ bool ev_two_targets(int nt) { return nt >= 2; }
 
 __device__ __forceinline__ EvTarget2 ev_target2(const Particles& p, const BucketGeom& g, int t0, int nt, int lane) {
   EvTarget2 x;
@@ -344,7 +380,8 @@ __device__ __forceinline__ void ev_finish2(EvalWarp& w, const Kahan4& K, const E
 // (p2c): pot_full gets every node's potential, pot the quadrupole node()
 // terms only (the reference's potential: pmono, the monopole nodes' part, is
 // left out); P2P adds to pot_full only (GravityVisitor::leaf applies none).
-__device__ __forceinline__ void ev_finish(EvalWarp& w, const Kahan4& K, float pmono, const EvTarget& x,
+template <class W>
+__device__ __forceinline__ void ev_finish(W& w, const Kahan4& K, float pmono, const EvTarget& x,
                                           const TravParams& P, int t0, int lane, bool p2c, bool store) {
   double* red = reinterpret_cast<double*>(&w.st[0][0]);
   __syncwarp();
@@ -395,67 +432,48 @@ __device__ __forceinline__ float4 node_offset(const WalkRec* __restrict__ walk, 
                      (float)((c2 + P.oz) - g.cm[2]), 0.f);
 }
 
-struct P2cPair {
-  float ax, ay, az, pf;  // both nodes' terms
-  float pm;              // the potential of the monopole nodes among them
+struct P2cTerm {
+  float ax, ay, az, pf;
 };
 
-// Both terms of a staged node pair in scalar form (the rare softened and
-// monopole cases; a monopole node carries NaN softening).
-__device__ __noinline__ P2cPair ev_p2c_pair_scalar(const EvalWarp& w, int k, float tx, float ty, float tz,
-                                                   float ts) {
-  const float4 P0 = w.st[0][k], P1 = w.st[1][k], P2 = w.st[2][k], P3 = w.st[3][k], P4 = w.st[4][k],
-               P5 = w.st[5][k];
-  float ax = 0.f, ay = 0.f, az = 0.f, pf = 0.f, pm = 0.f;
-  // rows: (ox, oy, oz, M), (xx, xy, xz, yy), (yz, zz, soft, half trace)
-  const float4 t[2][3] = {{make_float4(P0.x, P0.z, P1.x, P1.z), make_float4(P2.x, P2.z, P3.x, P3.z),
-                           make_float4(P4.x, P4.z, P5.z, fabsf(P5.x))},
-                          {make_float4(P0.y, P0.w, P1.y, P1.w), make_float4(P2.y, P2.w, P3.y, P3.w),
-                           make_float4(P4.y, P4.w, P5.w, fabsf(P5.y))}};
-  for (int s = 0; s < 2; s++) {
-    // r = t - o (GravityVisitor::node, examples/GravityVisitor.h:207-220, FP32)
-    const float4 A = t[s][0], B = t[s][1], Cc = t[s][2];
-    const float rx = tx - A.x, ry = ty - A.y, rz = tz - A.z;
-    const float r2 = rx * rx + ry * ry + rz * rz;
-    const float dir = rsqrtf(r2);
-    float a, b, c, d;
-    splineq_f32(dir, r2, Cc.z + ts, a, b, c, d);
-    const float qx = B.x * rx + B.y * ry + B.z * rz;
-    const float qy = B.y * rx + B.w * ry + Cc.x * rz;
-    const float qz = B.z * rx + Cc.x * ry + Cc.y * rz;
-    const float qir = 0.5f * (qx * rx + qy * ry + qz * rz);
-    const float qir3 = b * A.w + d * qir - c * Cc.w;
-    const float pt = -A.w * a - c * qir + b * Cc.w;
-    pf += pt;
-    if (isnan(Cc.z)) pm += pt;
-    ax += -qir3 * rx + c * qx;
-    ay += -qir3 * ry + c * qy;
-    az += -qir3 * rz + c * qz;
-  }
-  return P2cPair{ax, ay, az, pf, pm};
+// One P2C term in scalar form for the rare nodes the packed loop leaves out:
+// a node whose softening sphere may reach a target (SPLINEQ's softened
+// branch, GravityVisitor::node, examples/GravityVisitor.h:184-224) or a
+// monopole node (addGravity, :130-139: no second moments, never softened --
+// it is given a NaN softening, so SPLINEQ takes its unsoftened branch).
+__device__ __noinline__ P2cTerm ev_p2c_scalar(float ox, float oy, float oz, float M, float soft, float4 q0,
+                                              float2 q1, float tx, float ty, float tz, float ts) {
+  // q0 = (xx, xy, xz, yy), q1 = (yz, zz)
+  const float rx = tx - ox, ry = ty - oy, rz = tz - oz;
+  const float r2 = rx * rx + ry * ry + rz * rz;
+  const float dir = rsqrtf(r2);
+  float a, b, c, d;
+  splineq_f32(dir, r2, soft + ts, a, b, c, d);
+  const float qx = q0.x * rx + q0.y * ry + q0.z * rz;
+  const float qy = q0.y * rx + q0.w * ry + q1.x * rz;
+  const float qz = q0.z * rx + q1.x * ry + q1.y * rz;
+  const float qir = 0.5f * (qx * rx + qy * ry + qz * rz);
+  const float tr = 0.5f * (q0.x + q0.w + q1.y);
+  const float qir3 = b * M + d * qir - c * tr;
+  P2cTerm t;
+  t.pf = -M * a - c * qir + b * tr;
+  t.ax = -qir3 * rx + c * qx;
+  t.ay = -qir3 * ry + c * qy;
+  t.az = -qir3 * rz + c * qz;
+  return t;
 }
 
 // The staged node pairs k = grp, grp + G, ... of one chunk against this
 // lane's target (GravityVisitor::node, examples/GravityVisitor.h:184-224, in
-// packed FP32); pairs holding a near node take the scalar path.  (A loop
-// without that test for chunks with no near node, chosen per chunk, measured
-// slower: the second copy costs registers.)
-__device__ __forceinline__ void ev_p2c_pairs(const EvalWarp& w, const EvTarget& x, int npair, float2 ntx, float2 nty,
+// packed FP32).  Near and monopole nodes are staged as zero-mass padding and
+// evaluated apart (ev_p2c_specials), so this loop has no branch.
+__device__ __forceinline__ void ev_p2c_pairs(const EvalWarpC& w, const EvTarget& x, int npair, float2 ntx, float2 nty,
                                              float2 ntz, float2& ax2, float2& ay2, float2& az2, float2& pp2,
-                                             float2& mm2, float& pmono) {
+                                             float2& mm2) {
   const float2 mthree = make_float2(-3.f, -3.f), mfive = make_float2(-5.f, -5.f), half = make_float2(0.5f, 0.5f);
   const float4* sp = &w.st[0][x.grp];  // rows st[1..5] follow at +32 each
   for (int k = x.grp; k < npair; k += x.G, sp += x.G) {
     const float4 P5 = sp[160];
-    if ((__float_as_int(P5.x) | __float_as_int(P5.y)) < 0) {  // a near or monopole node: scalar
-      const P2cPair v = ev_p2c_pair_scalar(w, k, x.tx, x.ty, x.tz, x.ts);
-      ax2.x += v.ax;
-      ay2.x += v.ay;
-      az2.x += v.az;
-      pp2.x += v.pf;
-      pmono += v.pm;
-      continue;
-    }
     const float4 P0 = sp[0], P1 = sp[32];
     const float2 rx = __fadd2_rn(make_float2(P0.x, P0.y), ntx);  // r' = o - t = -r
     const float2 ry = __fadd2_rn(make_float2(P0.z, P0.w), nty);
@@ -487,13 +505,36 @@ __device__ __forceinline__ void ev_p2c_pairs(const EvalWarp& w, const EvTarget& 
   }
 }
 
+// The chunk's near and monopole entries w.spec[0..ns), spread over the lane
+// groups, in scalar form; a monopole node's potential also goes to pmono
+// (left out of the reference's potential).
+__device__ __forceinline__ void ev_p2c_specials(const EvalWarpC& w, const TravParams& P, const EvTarget& x, int ns,
+                                                float2& ax2, float2& ay2, float2& az2, float2& pp2, float& pmono) {
+  const float qnan = __int_as_float(0x7fc00000);
+  for (int j = x.grp; j < ns; j += x.G) {
+    const int e = w.spec[j];
+    const int node = e & 0x3fffffff;
+    const float4 o = node_offset(P.walk, node, P, w.geom);
+    const float4* rec = reinterpret_cast<const float4*>(P.quadf + node);
+    const float4 r0 = rec[0], r1 = rec[1];  // (mass, soft, xx, xy), (xz, yy, yz, zz)
+    const bool mono = e < 0;
+    const float4 q0 = mono ? make_float4(0.f, 0.f, 0.f, 0.f) : make_float4(r0.z, r0.w, r1.x, r1.y);
+    const float2 q1 = mono ? make_float2(0.f, 0.f) : make_float2(r1.z, r1.w);
+    const P2cTerm t = ev_p2c_scalar(o.x, o.y, o.z, r0.x, mono ? qnan : r0.y, q0, q1, x.tx, x.ty, x.tz, x.ts);
+    ax2.x += t.ax;
+    ay2.x += t.ay;
+    az2.x += t.az;
+    pp2.x += t.pf;
+    if (mono) pmono += t.pf;
+  }
+}
+
 template <int kMinBlocks>
 __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams P, ListParams L,
                                                                      const Mom* __restrict__ mom) {
-  __shared__ EvalWarp warps[kEvWarps];
-  EvalWarp& w = warps[threadIdx.x >> 5];
+  __shared__ EvalWarpC warps[kEvWarps];
+  EvalWarpC& w = warps[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
-  const float qnan = __int_as_float(0x7fc00000);
   const float kPad = 1.0e10f;
   int64_t b;
   int tnode;
@@ -510,8 +551,9 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams
       const int t0 = tbase + tc, nt = min(32, ntot - tc);
       const EvTarget x = ev_target(P.p, w.geom, t0, nt, lane);
       const float2 ntx = make_float2(-x.tx, -x.tx), nty = make_float2(-x.ty, -x.ty), ntz = make_float2(-x.tz, -x.tz);
-      Kahan4 K;
-      K.zero();
+      // compensated sums in shared memory (added to once every four chunks)
+      w.ks[0][lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+      w.ks[1][lane] = make_float4(0.f, 0.f, 0.f, 0.f);
       // plain packed sums over four chunks, then one compensated add
       float2 ax2 = make_float2(0.f, 0.f), ay2 = ax2, az2 = ax2, pp2 = ax2, mm2 = ax2;
       float pmono = 0.f;  // the monopole nodes' potential (left out of pot)
@@ -526,9 +568,10 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams
           en0 = (qn < count) ? L.pc_pool[start + qn] : 0;
           en1 = (qn + 1 < count) ? L.pc_pool[start + qn + 1] : 0;
         }
-        // stage this lane's two nodes as a pair
+        // stage this lane's two nodes as a pair; near and monopole nodes
+        // (bits 30 / 31) become zero-mass padding and go to the scalar list
         float4 o[2], r0[2], r1[2];
-        bool near[2] = {false, false}, mono[2] = {false, false};
+        bool spec[2] = {false, false};
 #pragma unroll
         for (int h = 0; h < 2; h++) {
           const int q = cs + 2 * lane + h;
@@ -537,40 +580,56 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams
           r1[h] = r0[h];
           if (q < count) {
             const int e = ec[h];
-            const int node = e & 0x3fffffff;
-            near[h] = (e & 0x40000000) != 0;
-            const float4* rec = reinterpret_cast<const float4*>(P.quadf + node);
-            o[h] = node_offset(P.walk, node, P, w.geom);
-            r0[h] = rec[0];  // mass, soft, xx, xy
-            r1[h] = rec[1];  // xz, yy, yz, zz
-            mono[h] = e < 0;
-            if (e < 0) {     // monopole: no second moments, NaN softening (never softened)
-              r0[h] = make_float4(r0[h].x, qnan, 0.f, 0.f);
-              r1[h] = make_float4(0.f, 0.f, 0.f, 0.f);
+            spec[h] = (e & 0xc0000000) != 0;
+            if (!spec[h]) {
+              const int node = e & 0x3fffffff;
+              const float4* rec = reinterpret_cast<const float4*>(P.quadf + node);
+              o[h] = node_offset(P.walk, node, P, w.geom);
+              r0[h] = rec[0];  // mass, soft, xx, xy
+              r1[h] = rec[1];  // xz, yy, yz, zz
             }
           }
         }
+        const unsigned m0 = __ballot_sync(kFull, spec[0]), m1 = __ballot_sync(kFull, spec[1]);
+        const int ns = __popc(m0) + __popc(m1);
         __syncwarp();
+        if (spec[0] || spec[1]) {  // chunk order: by lane, then h
+          const unsigned lt = (1u << lane) - 1u;
+          const int at = __popc(m0 & lt) + __popc(m1 & lt);
+          if (spec[0]) w.spec[at] = ec[0];
+          if (spec[1]) w.spec[at + (spec[0] ? 1 : 0)] = ec[1];
+        }
         w.st[0][lane] = make_float4(o[0].x, o[1].x, o[0].y, o[1].y);
         w.st[1][lane] = make_float4(o[0].z, o[1].z, r0[0].x, r0[1].x);
         w.st[2][lane] = make_float4(r0[0].z, r0[1].z, r0[0].w, r0[1].w);
         w.st[3][lane] = make_float4(r1[0].x, r1[1].x, r1[0].y, r1[1].y);
         w.st[4][lane] = make_float4(r1[0].z, r1[1].z, r1[0].w, r1[1].w);
-        {  // (tr_a, tr_b, soft_a, soft_b); a near node carries its half trace negated
+        {  // (tr_a, tr_b, soft_a, soft_b)
           const float tra = 0.5f * (r0[0].z + r1[0].y + r1[0].w), trb = 0.5f * (r0[1].z + r1[1].y + r1[1].w);
-          w.st[5][lane] = make_float4((near[0] || mono[0]) ? -tra : tra, (near[1] || mono[1]) ? -trb : trb,
-                                      r0[0].y, r0[1].y);
+          w.st[5][lane] = make_float4(tra, trb, r0[0].y, r0[1].y);
         }
         __syncwarp();
         const int npair = (min(64, count - cs) + 1) >> 1;
-        if (x.grp < x.G) ev_p2c_pairs(w, x, npair, ntx, nty, ntz, ax2, ay2, az2, pp2, mm2, pmono);
+        if (x.grp < x.G) {
+          ev_p2c_pairs(w, x, npair, ntx, nty, ntz, ax2, ay2, az2, pp2, mm2);
+          if (ns) ev_p2c_specials(w, P, x, ns, ax2, ay2, az2, pp2, pmono);
+        }
         if (((cs >> 6) & 3) == 3 || cs + 64 >= count) {
-          K.add(0, ax2.x + ax2.y);
-          K.add(1, ay2.x + ay2.y);
-          K.add(2, az2.x + az2.y);
-          K.add(3, (pp2.x + pp2.y) - (mm2.x + mm2.y));
+          float4 ks = w.ks[0][lane], kc = w.ks[1][lane];
+          kahan_add(ks.x, kc.x, ax2.x + ax2.y);
+          kahan_add(ks.y, kc.y, ay2.x + ay2.y);
+          kahan_add(ks.z, kc.z, az2.x + az2.y);
+          kahan_add(ks.w, kc.w, (pp2.x + pp2.y) - (mm2.x + mm2.y));
+          w.ks[0][lane] = ks;
+          w.ks[1][lane] = kc;
           ax2 = ay2 = az2 = pp2 = mm2 = make_float2(0.f, 0.f);
         }
+      }
+      Kahan4 K;
+      {
+        const float4 ks = w.ks[0][lane], kc = w.ks[1][lane];
+        K.s[0] = ks.x; K.s[1] = ks.y; K.s[2] = ks.z; K.s[3] = ks.w;
+        K.c[0] = kc.x; K.c[1] = kc.y; K.c[2] = kc.z; K.c[3] = kc.w;
       }
       ev_finish(w, K, pmono, x, P, t0, lane, true, P.accumulate == 0);
     }
@@ -784,6 +843,30 @@ __device__ __forceinline__ void ev_p2p_leaves(EvalWarp& w, int nleaves, const Tr
   __syncwarp();
 }
 
+// Marks the leaves of a bucket's P2P list that may hold a softened pair
+// (bit 31 of the entry, p2p_leaf_near: the same exact test for every form)
+// and returns the source particles of all its leaves.  Out of line, so that
+// its FP64 temporaries do not add to the evaluation loops' registers (a
+// separate kernel between the walk and the evaluations measured 0.6 ms
+// slower at N = 2^24).
+__device__ __noinline__ unsigned long long mark_near_leaves(const WalkRec* __restrict__ walk, const BucketGeom* g,
+                                                            double ox, double oy, double oz,
+                                                            int32_t* __restrict__ list, int count, int lane) {
+  unsigned long long nsrc = 0;
+  for (int k0 = 0; k0 < count; k0 += 32) {
+    const int k = k0 + lane;
+    unsigned cnt = 0;
+    if (k < count) {
+      const int e = list[k] & 0x7fffffff;
+      cnt = (unsigned)walk[e].pcount;
+      list[k] = p2p_leaf_near(walk, e, g->lo, g->hi, g->soft_max, ox, oy, oz) ? (e | (int)0x80000000) : e;
+    }
+    nsrc += __reduce_add_sync(kFull, cnt);
+  }
+  __syncwarp();  // the marked entries are read back by other lanes
+  return nsrc;
+}
+
 // The bucket's P2P list in blocks of 64 entries: far leaves, then near ones.
 template <bool kTwo, class Tgt>
 __device__ __forceinline__ void ev_p2p_blocks(EvalWarp& w, const TravParams& P, const ListParams& L, const Tgt& x,
@@ -816,6 +899,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2p(TravParams
   __shared__ EvalWarp warps[kEvWarps];
   EvalWarp& w = warps[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
+  unsigned long long c_pp = 0;
   int64_t b;
   int tnode;
   while (next_bucket(P, lane, b, tnode)) {
@@ -827,6 +911,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2p(TravParams
     if (lane == 0) load_bucket_geom(mom, tnode, w.geom);
     __syncwarp();
     const int tbase = P.walk[tnode].pstart, ntot = P.walk[tnode].pcount;
+    const unsigned long long nsrc = mark_near_leaves(P.walk, &w.geom, P.ox, P.oy, P.oz, L.pp_pool + start, count, lane);
     for (int tc = 0; tc < ntot; tc += 32) {
       const int t0 = tbase + tc, nt = min(32, ntot - tc);
       if (ev_two_targets(nt)) {
@@ -844,12 +929,16 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2p(TravParams
       ev_p2p_blocks<false>(w, P, L, x, start, count, lane, K);
       ev_finish(w, K, 0.f, x, P, t0, lane, false, false);
     }
+    // P2P pairs as the reference counts them (n_src * n_tgt per leaf(),
+    // src/Traverser.h:27); the walk wrote the bucket's P2C work before
+    c_pp += nsrc * (unsigned long long)ntot;
+    if (P.bucket_work && lane == 0) P.bucket_work[b] += nsrc * (unsigned long long)ntot;
   }
+  if (lane == 0) atomicAdd(&P.counters[0], c_pp);
 }
 
-
 // ---------------------------------------------------------------- launchers
-int walk_lists_grid(int sms) { return sms * 5; }  // the CTAs resident at 96 registers
+int walk_lists_grid(int sms) { return sms * PT_WALK_MINB; }  // the CTAs resident
 
 void launch_walk_lists(const TravParams& P, const ListParams& L, const Mom* mom, int grid, cudaStream_t st) {
   note_launch();
@@ -863,7 +952,7 @@ void launch_eval_lists(const TravParams& P, const ListParams& L, const Mom* mom,
   TravParams Q = P;
   Q.work = work2;
   note_launch();
-  eval_p2c<6><<<grid, kEvWarps * 32, 0, st>>>(P, L, mom);
+  eval_p2c<PT_P2C_MINB><<<grid, kEvWarps * 32, 0, st>>>(P, L, mom);
   note_launch();
   eval_p2p<8><<<grid, kEvWarps * 32, 0, st>>>(Q, L, mom);
 }

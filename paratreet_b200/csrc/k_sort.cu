@@ -20,7 +20,11 @@
 //              consecutive threads on consecutive destinations.
 // The look-back only waits on tiles that claimed their index earlier and
 // publish their counts before waiting on anything, so it always ends; the spin
-// is still bounded and reports kErrSort instead of hanging.
+// is still bounded (spin_limit polls of an unpublished tile, 2^21 by default)
+// and reports kErrSort instead of hanging.  A look-back cut short only
+// under-counts a digit's exclusive prefix, so every destination stays inside
+// [0, n), but the output is then not a permutation: the caller checks the
+// status word before it uses the sorted indices.
 #include <algorithm>
 
 #include "pt_internal.cuh"
@@ -33,7 +37,6 @@ constexpr int kSortRounds = 16;                        // rounds of 32 keys per 
 constexpr int kSortTile = kSortThreads * kSortRounds;  // 4096 keys per CTA
 constexpr unsigned long long kFlagAggregate = 1ull << 32;
 constexpr unsigned long long kFlagInclusive = 2ull << 32;
-constexpr long kSpinLimit = 1L << 21;
 
 __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
   unsigned long long v;
@@ -97,7 +100,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) radix_onesweep(const uint64_t
                                                                   const uint32_t* __restrict__ gofs,
                                                                   uint32_t* __restrict__ counter,
                                                                   unsigned long long* __restrict__ look,
-                                                                  unsigned* __restrict__ status) {
+                                                                  unsigned* __restrict__ status, long long spin_limit) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   OnesweepShared& S = *reinterpret_cast<OnesweepShared*>(smem_raw);
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -143,12 +146,12 @@ __global__ void __launch_bounds__(kSortThreads, 2) radix_onesweep(const uint64_t
     st_relaxed_u64(my, kFlagAggregate | total);
     // decoupled look-back over the earlier tiles
     int64_t pt = tile - 1;
-    long spins = 0;
+    long long spins = 0;
     while (pt >= 0) {
       const unsigned long long s = ld_relaxed_u64(look + pt * 256 + d);
       const unsigned long long f = s & (3ull << 32);
       if (f == 0) {
-        if (++spins > kSpinLimit) {
+        if (++spins > spin_limit) {
           atomicOr(status, kErrSort);
           break;
         }
@@ -307,7 +310,7 @@ size_t sort_scratch_bytes(int64_t n) {
 
 // Sorts (k0, v0) in place by full 64-bit key using (k1, v1) as alternates.
 int radix_sort_pairs(uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, int64_t n, void* scratch,
-                     unsigned* status, int sms, cudaStream_t st) {
+                     unsigned* status, int sms, long long spin_limit, cudaStream_t st) {
   if (n <= 1) return 0;
   const int tiles = (int)((n + kSortTile - 1) / kSortTile);
   unsigned char* b = static_cast<unsigned char*>(scratch);
@@ -331,7 +334,7 @@ int radix_sort_pairs(uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, int
     cudaMemsetAsync(look, 0, look_bytes, st);
     note_launch();
     radix_onesweep<<<tiles, kSortThreads, sizeof(OnesweepShared), st>>>(
-        ka, va, kb, vb, n, 8 * pass, ghist + 256 * pass, counters + pass, look, status);
+        ka, va, kb, vb, n, 8 * pass, ghist + 256 * pass, counters + pass, look, status, spin_limit);
     uint64_t* tk = ka; ka = kb; kb = tk;
     uint32_t* tv = va; va = vb; vb = tv;
   }

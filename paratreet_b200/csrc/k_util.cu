@@ -81,4 +81,122 @@ void launch_map_index(const int32_t* inv, const int32_t* in, int32_t* out, int64
   if (n > 0) { note_launch(); map_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(inv, in, out, n); }
 }
 
+// ------------------------------------------------- interaction-list digests
+// Order-independent digest of one bucket's interaction list: the sum (mod
+// 2^64) of a 64-bit mix of (node, class) over its entries, class 0 = P2P leaf,
+// 1 = quadrupole P2C node, 2 = monopole P2C node (the near flags of the
+// two-phase lists are not part of it).  Equal lists give equal digests
+// whatever their order.
+__device__ __forceinline__ unsigned long long entry_mix(unsigned node, unsigned cls) {
+  unsigned long long z = (((unsigned long long)node << 2) | cls) + 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Recorded lists (CSR: list_off, node, kind 0 / 1 / 2), one warp per bucket.
+__global__ void __launch_bounds__(256) digest_recorded(const int64_t* __restrict__ off,
+                                                       const int32_t* __restrict__ node,
+                                                       const int8_t* __restrict__ kind, int64_t nb,
+                                                       unsigned long long* __restrict__ dig,
+                                                       int64_t* __restrict__ cnt) {
+  const int lane = threadIdx.x & 31;
+  const int64_t b = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  if (b >= nb) return;
+  const int64_t e0 = off[b], e1 = off[b + 1];
+  unsigned long long s = 0;
+  for (int64_t e = e0 + lane; e < e1; e += 32) s += entry_mix((unsigned)node[e], (unsigned)kind[e]);
+  s = warp_sum_u64(s);
+  if (lane == 0) {
+    dig[b] = s;
+    cnt[b] = e1 - e0;
+  }
+}
+
+// Two-phase lists: per bucket a P2C run (bit 31 monopole, bit 30 near) and a
+// P2P run (bit 31 near) in the pools, one warp per bucket.
+__global__ void __launch_bounds__(256) digest_two_phase(const int32_t* __restrict__ pc_pool,
+                                                        const int32_t* __restrict__ pp_pool,
+                                                        const int64_t* __restrict__ pc_start,
+                                                        const int32_t* __restrict__ pc_count,
+                                                        const int64_t* __restrict__ pp_start,
+                                                        const int32_t* __restrict__ pp_count, int64_t nb,
+                                                        unsigned long long* __restrict__ dig,
+                                                        int64_t* __restrict__ cnt) {
+  const int lane = threadIdx.x & 31;
+  const int64_t b = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  if (b >= nb) return;
+  unsigned long long s = 0;
+  const int64_t c0 = pc_start[b], p0 = pp_start[b];
+  const int nc = pc_count[b], np = pp_count[b];
+  for (int k = lane; k < nc; k += 32) {
+    const int e = pc_pool[c0 + k];
+    s += entry_mix((unsigned)(e & 0x3fffffff), e < 0 ? 2u : 1u);
+  }
+  for (int k = lane; k < np; k += 32) s += entry_mix((unsigned)(pp_pool[p0 + k] & 0x7fffffff), 0u);
+  s = warp_sum_u64(s);
+  if (lane == 0) {
+    dig[b] = s;
+    cnt[b] = (int64_t)nc + np;
+  }
+}
+
+// The two-phase pools as CSR lists: per bucket its P2P leaves (kind 0), then
+// its P2C nodes (kind 1 quadrupole, 2 monopole), one warp per bucket.
+__global__ void __launch_bounds__(256) pools_to_csr(const int32_t* __restrict__ pc_pool,
+                                                    const int32_t* __restrict__ pp_pool,
+                                                    const int64_t* __restrict__ pc_start,
+                                                    const int32_t* __restrict__ pc_count,
+                                                    const int64_t* __restrict__ pp_start,
+                                                    const int32_t* __restrict__ pp_count, int64_t nb,
+                                                    const int64_t* __restrict__ off, int32_t* __restrict__ node,
+                                                    int8_t* __restrict__ kind) {
+  const int lane = threadIdx.x & 31;
+  const int64_t b = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  if (b >= nb) return;
+  const int64_t o = off[b], c0 = pc_start[b], p0 = pp_start[b];
+  const int nc = pc_count[b], np = pp_count[b];
+  for (int k = lane; k < np; k += 32) {
+    node[o + k] = pp_pool[p0 + k] & 0x7fffffff;
+    kind[o + k] = 0;
+  }
+  for (int k = lane; k < nc; k += 32) {
+    const int e = pc_pool[c0 + k];
+    node[o + np + k] = e & 0x3fffffff;
+    kind[o + np + k] = (int8_t)(e < 0 ? 2 : 1);
+  }
+}
+
+void launch_pools_to_csr(const int32_t* pc_pool, const int32_t* pp_pool, const int64_t* pc_start,
+                         const int32_t* pc_count, const int64_t* pp_start, const int32_t* pp_count, int64_t nb,
+                         const int64_t* off, int32_t* node, int8_t* kind, cudaStream_t st) {
+  if (nb > 0) {
+    note_launch();
+    pools_to_csr<<<(unsigned)((nb * 32 + 255) / 256), 256, 0, st>>>(pc_pool, pp_pool, pc_start, pc_count, pp_start,
+                                                                   pp_count, nb, off, node, kind);
+  }
+}
+
+void launch_digest_recorded(const int64_t* off, const int32_t* node, const int8_t* kind, int64_t nb,
+                            unsigned long long* dig, int64_t* cnt, cudaStream_t st) {
+  if (nb > 0) {
+    note_launch();
+    digest_recorded<<<(unsigned)((nb * 32 + 255) / 256), 256, 0, st>>>(off, node, kind, nb, dig, cnt);
+  }
+}
+void launch_digest_two_phase(const int32_t* pc_pool, const int32_t* pp_pool, const int64_t* pc_start,
+                             const int32_t* pc_count, const int64_t* pp_start, const int32_t* pp_count, int64_t nb,
+                             unsigned long long* dig, int64_t* cnt, cudaStream_t st) {
+  if (nb > 0) {
+    note_launch();
+    digest_two_phase<<<(unsigned)((nb * 32 + 255) / 256), 256, 0, st>>>(pc_pool, pp_pool, pc_start, pc_count,
+                                                                       pp_start, pp_count, nb, dig, cnt);
+  }
+}
+
 }  // namespace pt

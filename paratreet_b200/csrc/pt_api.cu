@@ -62,8 +62,10 @@ struct pt_handle {
   int64_t* list_off = nullptr;
   int32_t* list_node = nullptr;
   int8_t* list_kind = nullptr;
-  int64_t list_total = 0, list_cap = 0, list_nb = 0;
+  int64_t list_total = 0, list_cap = 0, list_nb = 0;  // list_nb = recorded buckets + 1
+  int64_t list_off_cap = 0;                              // entries of list_count / list_off
   bool lists_valid = false;
+  bool tp_lists_valid = false;  // the two-phase pools hold the last pass's lists of every bucket
 
   double* dsum = nullptr;  // direct-sum scratch (caller-order copies + partials)
   int64_t dsum_cap = 0;
@@ -77,8 +79,8 @@ struct pt_handle {
   int32_t *l_pc_count = nullptr, *l_pp_count = nullptr;
   int64_t l_nb_cap = 0;
   unsigned long long* d_lcur = nullptr;  // [0] P2C cursor, [1] P2P cursor, [2] longest list
-  unsigned* d_work3 = nullptr;           // bucket queues of the three kernels
-  unsigned l_thresh = 4096;
+  unsigned* d_work3 = nullptr;           // bucket queues of the list kernels (walk, P2C, P2P)
+  unsigned l_region = 32768;  // entries per warp region of the list pools
 
   double* sph = nullptr;  // SPH density pass: density, ball^2 (2n), neighbours (k n int32 + k n double)
   int64_t sph_cap = 0, sph_nbr_cap = 0;
@@ -96,12 +98,12 @@ struct pt_handle {
   int64_t ewd_cap = 0;
 
   cudaEvent_t ev[7]{};
+  long long sort_spin_limit = 1LL << 21;  // pt_set_sort_spin_limit
   pt_counters last{};
   double last_dt = 0.0;
   bool have_forces = false;     // a force pass ran since the particles were set
   bool forces_current = false;  // ... and the positions have not moved since
   bool trav_range_partial = false;
-  int mixed_variant = 0;  // occupancy variant of the mixed traversal (PT_MIXED_VARIANT)
 
   double* adj = nullptr;  // adjoint scratch: cotangent (3N) and gradients (4N), sorted + caller order
   int64_t adj_cap = 0;
@@ -111,6 +113,14 @@ struct pt_handle {
 
 namespace pt {
 namespace {
+
+// Scratch owned by one call (freed on every return path).
+struct DevBuf {
+  double* p = nullptr;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
 std::atomic<unsigned long long> g_launches{0};
 }
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
@@ -268,8 +278,12 @@ int keys_and_sort(pt_handle* h) {
   launch_keys(h->p.x, h->p.y, h->p.z, n, h->d_uni, h->p.key, h->idx, g, st);
   CK(cudaGetLastError());
   CK(cudaEventRecord(h->ev[1], st));
-  if (radix_sort_pairs(h->p.key, h->idx, h->key_alt, h->idx_alt, n, h->sort_scratch, h->d_status, h->sms, st))
+  if (radix_sort_pairs(h->p.key, h->idx, h->key_alt, h->idx_alt, n, h->sort_scratch, h->d_status, h->sms,
+                       h->sort_spin_limit, st))
     return fail(h, PT_E_CUDA, "radix sort: could not set the shared-memory attribute");
+  // a look-back that gave up leaves indices that are not a permutation: stop
+  // before the gather, so the particle arrays keep their last consistent state
+  CKR(read_status(h));
   double** fields[] = {&h->p.x, &h->p.y, &h->p.z, &h->p.vx, &h->p.vy, &h->p.vz, &h->p.m, &h->p.soft};
   for (auto f : fields) {
     gather_f64(*f, h->tmp_d, h->idx, n, g, st);
@@ -428,8 +442,10 @@ int ewald_correction_pass(pt_handle* h, int64_t b0, int64_t b1) {
 
 // Two-phase mixed evaluation: walk_lists writes every bucket's interaction
 // list to the pools, then eval_p2c and eval_p2p evaluate them.  Pools are
-// sized from the previous pass; a pass whose lists outgrow their regions or
-// pools is repeated (counters restored) with larger ones.
+// sized from the previous pass with a quarter of headroom (a bucket whose list
+// outgrows its warp's region moves it to a new region inside the walk); only
+// a pass whose lists fill a pool is repeated (counters restored) with pools
+// twice as large, which happens at most on the first passes of a handle.
 int run_two_phase(pt_handle* h, TravParams& P) {
   cudaStream_t st = h->stream;
   const int64_t nb = P.b_end - P.b_begin;
@@ -449,7 +465,7 @@ int run_two_phase(pt_handle* h, TravParams& P) {
   CK(cudaStreamSynchronize(st));
   ListParams L{};
   for (int attempt = 0;; attempt++) {
-    const unsigned region = 2 * h->l_thresh;
+    const unsigned region = h->l_region;
     const unsigned long long slack = (unsigned long long)wgrid * 4 * region;
     const unsigned long long need_pc =
         std::max<unsigned long long>(h->want_pc ? h->want_pc + slack : 0, 1024ull * nb + slack);
@@ -479,7 +495,8 @@ int run_two_phase(pt_handle* h, TravParams& P) {
         dfree(h->pool_pp);
         h->two_phase = false;
         CK(cudaMemcpyAsync(h->d_counters, c0, sizeof(c0), cudaMemcpyHostToDevice, st));
-        launch_traverse_mixed(P, h->nd.mom, h->sms * 16, h->mixed_variant, st);
+        if (h->cfg.precision == PT_FP64_LISTS) launch_traverse_f64(P, h->nd.mom, h->sms * 16, st);
+        else launch_traverse_mixed(P, h->nd.mom, h->sms * 16, st);
         CK(cudaGetLastError());
         return PT_OK;
       }
@@ -492,7 +509,7 @@ int run_two_phase(pt_handle* h, TravParams& P) {
     L.cap_pc = h->cap_pc;
     L.cap_pp = h->cap_pp;
     L.region = region;
-    L.thresh = h->l_thresh;
+    L.thresh = region / 8;
     L.pc_start = h->l_pc_start;
     L.pc_count = h->l_pc_count;
     L.pp_start = h->l_pp_start;
@@ -517,30 +534,65 @@ int run_two_phase(pt_handle* h, TravParams& P) {
       h->want_pp = std::max<unsigned long long>(h->want_pp, used_pp + used_pp / 4);
       break;
     }
-    if (attempt >= 4) return fail(h, PT_E_NOMEM, "interaction lists outgrow their pools");
-    // repeat the walk with larger regions and pools
+    if (attempt >= 6) return fail(h, PT_E_NOMEM, "interaction lists outgrow their pools");
+    // repeat the walk with larger pools (the cursors under-count the need: warps
+    // stop reserving once their pool is full)
     status &= ~kErrPool;
     CK(cudaMemcpyAsync(h->d_status, &status, sizeof(unsigned), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(h->d_counters, c0, sizeof(c0), cudaMemcpyHostToDevice, st));
-    const unsigned longest = (unsigned)cur[2];
-    while (h->l_thresh < 2 * longest + 64) h->l_thresh *= 2;
-    h->l_thresh *= 2;
-    h->want_pc = 2 * h->cap_pc;
-    h->want_pp = 2 * h->cap_pp;
+    h->want_pc = std::max(2 * h->cap_pc, cur[0] + cur[0] / 2);
+    h->want_pp = std::max(2 * h->cap_pp, cur[1] + cur[1] / 2);
   }
   TravParams E = P;
   E.work = h->d_work3 + 1;
-  launch_eval_lists(E, L, h->nd.mom, h->sms * 16, st, h->d_work3 + 2);
+  if (h->cfg.precision == PT_FP64_LISTS) launch_eval_lists_f64(E, L, h->nd.mom, h->sms * 16, st, h->d_work3 + 2);
+  else launch_eval_lists(E, L, h->nd.mom, h->sms * 16, st, h->d_work3 + 2);
   CK(cudaGetLastError());
+  h->tp_lists_valid = (P.b_begin == 0 && P.b_end == h->nbuckets && !h->cfg.periodic);
   return PT_OK;
 }
 
 int run_traversal(pt_handle* h, TravParams& P, int grid) {
-  if (h->cfg.precision == PT_MIXED && P.mode == 0 && h->two_phase) return run_two_phase(h, P);
+  const bool lists_form = h->cfg.precision == PT_MIXED || h->cfg.precision == PT_FP64_LISTS;
+  if (lists_form && P.mode == 0 && h->two_phase) return run_two_phase(h, P);
   if (h->cfg.precision == PT_MIXED && P.mode != 1)
-    launch_traverse_mixed(P, h->nd.mom, grid, h->mixed_variant, h->stream);
+    launch_traverse_mixed(P, h->nd.mom, grid, h->stream);
   else launch_traverse_f64(P, h->nd.mom, grid, h->stream);
   CK(cudaGetLastError());
+  return PT_OK;
+}
+
+// CSR lists (list_off / list_node / list_kind, kinds 0 P2P, 1 quadrupole,
+// 2 monopole) of every bucket from the two-phase pools of the pass just
+// made: per bucket its P2P leaves, then its P2C nodes, in the two-phase
+// walk's order.
+int lists_from_pools(pt_handle* h) {
+  cudaStream_t st = h->stream;
+  const int64_t nb = h->nbuckets;
+  if (nb + 1 > h->list_off_cap) {
+    CKR(dalloc(h, &h->list_count, nb + 1));
+    CKR(dalloc(h, &h->list_off, nb + 1));
+    h->list_off_cap = nb + 1;
+  }
+  std::vector<int32_t> cpc(nb), cpp(nb);
+  std::vector<int64_t> off(nb + 1);
+  CK(cudaMemcpyAsync(cpc.data(), h->l_pc_count, nb * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(cpp.data(), h->l_pp_count, nb * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  off[0] = 0;
+  for (int64_t i = 0; i < nb; i++) off[i + 1] = off[i] + cpc[i] + cpp[i];
+  h->list_total = off[nb];
+  if (h->list_total > h->list_cap) {
+    CKR(dalloc(h, &h->list_node, h->list_total));
+    CKR(dalloc(h, &h->list_kind, h->list_total));
+    h->list_cap = h->list_total;
+  }
+  CK(cudaMemcpyAsync(h->list_off, off.data(), (nb + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+  launch_pools_to_csr(h->pool_pc, h->pool_pp, h->l_pc_start, h->l_pc_count, h->l_pp_start, h->l_pp_count, nb,
+                      h->list_off, h->list_node, h->list_kind, st);
+  CK(cudaGetLastError());
+  h->list_nb = nb + 1;
+  h->lists_valid = true;
   return PT_OK;
 }
 
@@ -575,12 +627,20 @@ int traverse(pt_handle* h, int64_t b0, int64_t b1) {
   CK(cudaMemsetAsync(h->d_counters, 0, 3 * sizeof(unsigned long long), st));
   const int64_t nb = b1 - b0;
   h->lists_valid = false;
-  if (h->cfg.record_lists && nb > 0) {
-    if (nb + 1 > h->list_nb) {
+  h->tp_lists_valid = false;
+  // The two-phase forms record a full pass's lists from their own pools
+  // (lists_from_pools, after the pass); the FP64 form records them in the
+  // reference's walk order with a counting and a recording walk.
+  const bool two_phase_record = h->cfg.record_lists && nb > 0 && h->two_phase && !h->cfg.periodic &&
+                                b0 == 0 && b1 == h->nbuckets &&
+                                (h->cfg.precision == PT_MIXED || h->cfg.precision == PT_FP64_LISTS);
+  if (h->cfg.record_lists && nb > 0 && !two_phase_record) {
+    if (nb + 1 > h->list_off_cap) {
       CKR(dalloc(h, &h->list_count, nb + 1));
       CKR(dalloc(h, &h->list_off, nb + 1));
-      h->list_nb = nb + 1;
+      h->list_off_cap = nb + 1;
     }
+    h->list_nb = nb + 1;
     P.mode = 1;
     P.list_count = h->list_count;
     CK(cudaMemsetAsync(h->d_work, 0, sizeof(unsigned), st));
@@ -602,8 +662,8 @@ int traverse(pt_handle* h, int64_t b0, int64_t b1) {
     P.list_off = h->list_off;
     P.list_node = h->list_node;
     P.list_kind = h->list_kind;
-    if (h->cfg.precision == PT_MIXED) {
-      // lists come from the FP64 walk (identical for both forms); evaluate mixed
+    if (h->cfg.precision == PT_MIXED || h->cfg.precision == PT_FP64_LISTS) {
+      // lists come from the FP64 walk (identical for every form); then the two-phase pass
       P.mode = 2;
       CK(cudaMemsetAsync(h->d_work, 0, sizeof(unsigned), st));
       launch_traverse_f64(P, h->nd.mom, grid, st);  // records lists (and FP64 forces)
@@ -634,6 +694,7 @@ int traverse(pt_handle* h, int64_t b0, int64_t b1) {
       }
   if (h->cfg.periodic) CKR(ewald_correction_pass(h, b0, b1));
   CK(cudaEventRecord(h->ev[6], st));
+  if (two_phase_record && h->tp_lists_valid) CKR(lists_from_pools(h));
   return PT_OK;
 }
 
@@ -748,7 +809,7 @@ int pt_create(const pt_config* cfg, pt_handle** out) {
   if (!cfg || !out) return PT_E_ARG;
   *out = nullptr;
   if (!(cfg->theta > 0.0) || cfg->bucket < 1 || cfg->bucket > 32) return PT_E_ARG;
-  if (cfg->precision != PT_FP64 && cfg->precision != PT_MIXED) return PT_E_ARG;
+  if (cfg->precision != PT_FP64 && cfg->precision != PT_MIXED && cfg->precision != PT_FP64_LISTS) return PT_E_ARG;
   if (cfg->traversal != PT_TRANSPOSED_DOWN && cfg->traversal != PT_BASIC_DOWN) return PT_E_ARG;
   if (cfg->integrator != PT_KKD && cfg->integrator != PT_KDK) return PT_E_ARG;
   if (cfg->periodic && (!(cfg->period > 0.0) || cfg->n_replicas < 0 || cfg->n_replicas > 8 ||
@@ -768,7 +829,6 @@ int pt_create(const pt_config* cfg, pt_handle** out) {
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess) return bail(PT_E_CUDA);
   h->sms = prop.multiProcessorCount;
-  if (const char* v = std::getenv("PT_MIXED_VARIANT")) h->mixed_variant = std::atoi(v);
   if (const char* v = std::getenv("PT_MIXED_FUSED")) h->two_phase = std::atoi(v) == 0;
   if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) return bail(PT_E_CUDA);
   h->stream = h->own_stream;
@@ -828,8 +888,14 @@ int pt_set_theta(pt_handle* h, double theta) {
 }
 
 int pt_set_precision(pt_handle* h, int precision) {
-  if (!h || (precision != PT_FP64 && precision != PT_MIXED)) return PT_E_ARG;
+  if (!h || (precision != PT_FP64 && precision != PT_MIXED && precision != PT_FP64_LISTS)) return PT_E_ARG;
   h->cfg.precision = precision;
+  return PT_OK;
+}
+
+int pt_set_sort_spin_limit(pt_handle* h, int64_t polls) {
+  if (!h || polls < 0) return PT_E_ARG;
+  h->sort_spin_limit = (long long)polls;
   return PT_OK;
 }
 
@@ -1234,6 +1300,32 @@ int pt_get_lists(pt_handle* h, int64_t* offsets, uint64_t* keys, int32_t* kinds)
   return PT_OK;
 }
 
+int pt_get_list_digests(pt_handle* h, int which, uint64_t* digest, int64_t* count) {
+  if (!h || (which != 0 && which != 1)) return PT_E_ARG;
+  const int64_t nb = h->nbuckets;
+  if (which == 0 && !(h->lists_valid && !h->trav_range_partial && h->list_nb - 1 == nb))
+    return fail(h, PT_E_STATE, "no interaction lists recorded for every bucket (config.record_lists)");
+  if (which == 1 && !h->tp_lists_valid)
+    return fail(h, PT_E_STATE, "the last pass was not a two-phase mixed pass over every bucket");
+  if (nb == 0) return PT_OK;
+  cudaSetDevice(h->cfg.device);
+  cudaStream_t st = h->stream;
+  DevBuf buf;
+  CK(cudaMalloc((void**)&buf.p, 2 * nb * sizeof(double)));
+  unsigned long long* d_dig = reinterpret_cast<unsigned long long*>(buf.p);
+  int64_t* d_cnt = reinterpret_cast<int64_t*>(buf.p + nb);
+  if (which == 0)
+    launch_digest_recorded(h->list_off, h->list_node, h->list_kind, nb, d_dig, d_cnt, st);
+  else
+    launch_digest_two_phase(h->pool_pc, h->pool_pp, h->l_pc_start, h->l_pc_count, h->l_pp_start, h->l_pp_count, nb,
+                            d_dig, d_cnt, st);
+  CK(cudaGetLastError());
+  if (digest) CK(cudaMemcpyAsync(digest, d_dig, nb * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  if (count) CK(cudaMemcpyAsync(count, d_cnt, nb * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return PT_OK;
+}
+
 int pt_get_counters(pt_handle* h, pt_counters* c) {
   if (!h || !c) return PT_E_ARG;
   *c = h->last;
@@ -1539,13 +1631,6 @@ int chain_forces(pt_handle* h, double* A) {
   CK(cudaGetLastError());
   return PT_OK;
 }
-
-struct DevBuf {
-  double* p = nullptr;
-  ~DevBuf() {
-    if (p) cudaFree(p);
-  }
-};
 
 }  // namespace
 

@@ -22,9 +22,10 @@ size_t scan_scratch_bytes(int64_t n);
 void scan_exclusive(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* scratch, uint32_t* total,
                     cudaStream_t st);
 size_t sort_scratch_bytes(int64_t n);
-// 0 on success, -1 if the kernel attribute could not be set
+// 0 on success, -1 if the kernel attribute could not be set; spin_limit =
+// polls of an unpublished tile before the look-back gives up (kErrSort)
 int radix_sort_pairs(uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, int64_t n, void* scratch,
-                     unsigned* status, int sms, cudaStream_t st);
+                     unsigned* status, int sms, long long spin_limit, cudaStream_t st);
 void gather_f64(const double* in, double* out, const uint32_t* idx, int64_t n, int grid, cudaStream_t st);
 void gather_i32(const int32_t* in, int32_t* out, const uint32_t* idx, int64_t n, int grid, cudaStream_t st);
 
@@ -52,7 +53,7 @@ void launch_direct_sum(const double* x, const double* y, const double* z, const 
 // k_mixed.cu
 void launch_prep_sources(const int32_t* buckets, int64_t nbuckets, const WalkRec* walk, Particles p, float4* srcf,
                          float* softf, cudaStream_t st);
-void launch_traverse_mixed(const TravParams& P, const Mom* mom, int grid, int variant, cudaStream_t st);
+void launch_traverse_mixed(const TravParams& P, const Mom* mom, int grid, cudaStream_t st);
 
 // k_ewald.cu
 void launch_ewald_correction(Particles p, int64_t i0, int64_t i1, const EwaldRoot& R, const double4* htab,
@@ -73,6 +74,9 @@ void launch_walk_lists(const TravParams& P, const ListParams& L, const Mom* mom,
 // bucket queue from P.work and work2 respectively (zeroed by the caller)
 void launch_eval_lists(const TravParams& P, const ListParams& L, const Mom* mom, int grid, cudaStream_t st,
                        unsigned* work2);
+// k_f64lists.cu
+void launch_eval_lists_f64(const TravParams& P, const ListParams& L, const Mom* mom, int grid, cudaStream_t st,
+                           unsigned* work2);
 
 // k_sph.cu
 int sph_k();
@@ -92,6 +96,14 @@ void launch_sph_density(Particles p, int64_t n, const Mom* mom, const WalkRec* w
 void launch_adjoint(const AdjParams& A, int grid, cudaStream_t st);
 
 // k_util.cu
+void launch_pools_to_csr(const int32_t* pc_pool, const int32_t* pp_pool, const int64_t* pc_start,
+                         const int32_t* pc_count, const int64_t* pp_start, const int32_t* pp_count, int64_t nb,
+                         const int64_t* off, int32_t* node, int8_t* kind, cudaStream_t st);
+void launch_digest_recorded(const int64_t* off, const int32_t* node, const int8_t* kind, int64_t nb,
+                            unsigned long long* dig, int64_t* cnt, cudaStream_t st);
+void launch_digest_two_phase(const int32_t* pc_pool, const int32_t* pp_pool, const int64_t* pc_start,
+                             const int32_t* pc_count, const int64_t* pp_start, const int32_t* pp_count, int64_t nb,
+                             unsigned long long* dig, int64_t* cnt, cudaStream_t st);
 void launch_scatter_f64(const double* in, double* out, const int32_t* order, int64_t n, int grid, cudaStream_t st);
 void launch_scatter_u64(const uint64_t* in, uint64_t* out, const int32_t* order, int64_t n, int grid,
                         cudaStream_t st);

@@ -93,6 +93,21 @@ __device__ __forceinline__ bool open_softening_exact(double scx, double scy, dou
   return open_softening_gap(scx, scy, scz, ssoft, tcx, tcy, tcz, tsoft, box_gap2_exact(lo, hi, scx, scy, scz));
 }
 
+// Whether a P2P leaf may hold a pair that GravityVisitor::leaf softens (or
+// the target itself): the box gap between the target bucket's particle box
+// and the leaf's centre (plus offset) is within the leaf's reach plus both
+// sides' largest softening.  Conservative: a leaf for which it is false has
+// every pair at r >= soft_i + soft_j > 0.  rec = the leaf's WalkRec.
+__device__ __forceinline__ bool p2p_leaf_near(const WalkRec* __restrict__ walk, int leaf, const double lo[3],
+                                              const double hi[3], double tsoft_max, double ox, double oy,
+                                              double oz) {
+  const double2* r = reinterpret_cast<const double2*>(walk + leaf);
+  const double2 c01 = r[0], c2reach = r[1], smax = r[2];
+  const double gap2 = box_gap2_exact(lo, hi, __dadd_rn(c01.x, ox), __dadd_rn(c01.y, oy), __dadd_rn(c2reach.x, oz));
+  const double reach = c2reach.y + smax.x + tsoft_max;
+  return !(gap2 > reach * reach);
+}
+
 struct BucketGeom {
   double lo[3], hi[3];  // target bucket's particle bbox (CentroidData::box)
   double cm[3];         // target bucket's centre of mass

@@ -26,7 +26,7 @@ import numpy as np
 
 from . import _lib as L
 
-PRECISIONS = {"fp64": L.PT_FP64, "mixed": L.PT_MIXED}
+PRECISIONS = {"fp64": L.PT_FP64, "mixed": L.PT_MIXED, "fp64_lists": L.PT_FP64_LISTS}
 INTEGRATORS = {"kkd": L.PT_KKD, "kdk": L.PT_KDK}
 
 
@@ -147,6 +147,11 @@ class GravitySimulation:
         self._check(self._lib.pt_set_precision(self._h, PRECISIONS[precision]))
         self.conf.precision = precision
 
+    def set_sort_spin_limit(self, polls: int = 1 << 21):
+        """Failure-path control of the key sort (tests): the polls a look-back
+        makes on an unpublished tile before the pass gives up with an error."""
+        self._check(self._lib.pt_set_sort_spin_limit(self._h, int(polls)))
+
     # -- particles ----------------------------------------------------------
     def set_particles(self, p: dict):
         arrs = [np.ascontiguousarray(p[k], dtype=np.float64) for k in _FIELDS]
@@ -250,6 +255,17 @@ class GravitySimulation:
         kinds = np.empty(max(tot.value, 1), np.int32)
         self._check(self._lib.pt_get_lists(self._h, L.ptr(off), L.ptr(keys), L.ptr(kinds)))
         return InteractionLists(bk, off, keys[: tot.value], kinds[: tot.value])
+
+    def list_digests(self, which: str = "two_phase"):
+        """Per bucket (DFS order): an order-independent digest of its
+        interaction list in the last pass and the list's length.  which =
+        "recorded" (record_lists) or "two_phase" (the mixed form's lists)."""
+        nb = self.bucket_keys().size
+        dig = np.empty(max(nb, 1), np.uint64)
+        cnt = np.empty(max(nb, 1), np.int64)
+        self._check(self._lib.pt_get_list_digests(self._h, {"recorded": 0, "two_phase": 1}[which],
+                                                   L.ptr(dig), L.ptr(cnt)))
+        return dig[:nb], cnt[:nb]
 
     def counters(self) -> dict:
         c = L.PtCounters()

@@ -143,7 +143,16 @@ def test_mixed_matches_fp64(gen, n, bucket):
         sm.start_down()
         am = sm.accelerations()
         Lm = sm.lists()
-    assert np.array_equal(L64.keys, Lm.keys) and np.array_equal(L64.offsets, Lm.offsets)
+    # the same interactions per bucket: the mixed form records its two-phase
+    # walk's lists (leaves first, then nodes, in that walk's order), the FP64
+    # form the reference's pre-order
+    assert np.array_equal(L64.offsets, Lm.offsets)
+    for b in range(L64.offsets.size - 1):
+        o0, o1 = L64.offsets[b], L64.offsets[b + 1]
+        k64 = np.lexsort((L64.keys[o0:o1], L64.kinds[o0:o1]))
+        km = np.lexsort((Lm.keys[o0:o1], Lm.kinds[o0:o1]))
+        assert np.array_equal(L64.keys[o0:o1][k64], Lm.keys[o0:o1][km]), b
+        assert np.array_equal(L64.kinds[o0:o1][k64], Lm.kinds[o0:o1][km]), b
     e = rel_err((am["ax"], am["ay"], am["az"]), (a64["ax"], a64["ay"], a64["az"]))
     assert np.sqrt(np.mean(e ** 2)) < 1e-5
     assert np.max(e) < 1e-3
@@ -158,21 +167,57 @@ def test_mixed_matches_fp64(gen, n, bucket):
 def test_mixed_matches_fp64_full_size():
     """The 2^24 Plummer workload (eps 1e-3, bucket 32, theta 0.7): both forms
     make the same interactions (P2P pairs, P2C evaluations and opening tests
-    counted on the device) and the mixed accelerations stay within 1e-5 RMS
-    of the FP64 ones over all particles."""
+    counted on the device, and every bucket's list: the FP64 walk's recorded
+    list and the mixed form's two-phase list have equal order-independent
+    digests and lengths) and the mixed accelerations stay within 1e-5 RMS of
+    the FP64 ones over all particles."""
     p = ics.plummer(1 << 24, seed=42, soft=1e-3)
     out = {}
     for prec in ("fp64", "mixed"):
-        with sim(max_particles_per_leaf=32, theta=0.7, precision=prec) as s:
+        with sim(max_particles_per_leaf=32, theta=0.7, precision=prec, record_lists=(prec == "fp64")) as s:
             s.set_particles(p)
             s.start_down()
-            out[prec] = (s.accelerations(), s.counters())
-    (a64, c64), (am, cm) = out["fp64"], out["mixed"]
+            dig = s.list_digests("recorded" if prec == "fp64" else "two_phase")
+            out[prec] = (s.accelerations(), s.counters(), dig, s.bucket_keys())
+    (a64, c64, d64, k64), (am, cm, dm, km) = out["fp64"], out["mixed"]
     for k in ("n_pp", "n_pc", "n_open", "n_nodes", "n_buckets"):
         assert c64[k] == cm[k], k
+    assert np.array_equal(k64, km)
+    assert np.array_equal(d64[1], dm[1]), "list lengths differ"
+    assert np.array_equal(d64[0], dm[0]), "list digests differ"
     assert all(np.all(np.isfinite(am[k])) for k in ("ax", "ay", "az", "pot", "pot_full"))
     e = rel_err((am["ax"], am["ay"], am["az"]), (a64["ax"], a64["ay"], a64["az"]))
     assert np.sqrt(np.mean(e ** 2)) < 1e-5
+
+
+@pytest.mark.parametrize("gen,n,bucket,soft,theta", [("plummer", 200000, 32, 1e-3, 0.7),
+                                                      ("mixture", 150000, 16, 1e-4, 0.7),
+                                                      ("hernquist", 50000, 16, 0.05, 0.5)])
+def test_fp64_lists_matches_ordered_fp64(gen, n, bucket, soft, theta):
+    """The FP64 comparator of the mixed form (PT_FP64_LISTS: the two-phase
+    lists evaluated in FP64) against the ordered FP64 walk (bit-exact with the
+    reference): the same interactions, and accelerations and potentials equal
+    up to the order of each particle's sums."""
+    p = getattr(ics, gen)(n, seed=9, soft=soft)
+    out = {}
+    for prec in ("fp64", "fp64_lists"):
+        with sim(max_particles_per_leaf=bucket, theta=theta, precision=prec) as s:
+            s.set_particles(p)
+            s.start_down()
+            s.start_down()
+            out[prec] = (s.accelerations(), s.counters())
+    (a, c), (b, cl) = out["fp64"], out["fp64_lists"]
+    assert (c["n_pp"], c["n_pc"], c["n_open"]) == (cl["n_pp"], cl["n_pc"], cl["n_open"])
+    da = np.sqrt((b["ax"] - a["ax"]) ** 2 + (b["ay"] - a["ay"]) ** 2 + (b["az"] - a["az"]) ** 2)
+    am = np.sqrt(a["ax"] ** 2 + a["ay"] ** 2 + a["az"] ** 2)
+    rel = da / am
+    print(f"fp64_lists vs fp64 {gen} n={n}: acc rel rms {np.sqrt(np.mean(rel ** 2)):.2e} max {rel.max():.2e}; "
+          f"|da| max / rms|a| {da.max() / np.sqrt(np.mean(am ** 2)):.2e}")
+    assert np.sqrt(np.mean(rel ** 2)) < 1e-13
+    assert rel.max() < 1e-11
+    for k in ("pot", "pot_full"):
+        dp = np.abs(b[k] - a[k]) / np.abs(a["pot_full"])
+        assert dp.max() < 1e-12, k
 
 
 @pytest.mark.parametrize("gen,n,bucket", [("plummer", 60000, 32), ("mixture", 40000, 16)])
