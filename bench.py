@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--theta", type=float, default=0.7)
     ap.add_argument("--bucket", type=int, default=32)
     ap.add_argument("--soft", type=float, default=1e-3)
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64", "fp64_lists"])
     ap.add_argument("--targets", type=int, default=4096)
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-extras", action="store_true", help="skip e2e, fp64 comparison, errors, cpu baseline")
@@ -311,11 +311,11 @@ def main():
     hbm = peaks.get("hbm_gbs") or 6650.0
     roofline = {"bound": "fp32" if a.precision == "mixed" else "fp64", "achieved": achieved,
                 "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf, "traffic": traffic,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "
-                                  "(profiles/traffic_traverse_mixed_plummer_16m.md)" if traffic else None,
+                "traffic_source": TRAVERSE_MIXED_DRAM_SOURCE if traffic else None,
                 "dram_gbs": (traffic / t_trav / 1e9) if traffic else None,
                 "dram_frac_of_hbm": (traffic / t_trav / 1e9 / hbm) if traffic else None,
-                "kernel": "walk_lists + eval_p2c + eval_p2p" if a.precision == "mixed" else "traverse_f64",
+                "kernel": {"mixed": "walk_lists + eval_p2c + eval_p2p", "fp64": "traverse_f64",
+                           "fp64_lists": "walk_lists + eval_p2c_f64 + eval_p2p_f64"}[a.precision],
                 "flops_per_launch": flops,
                 "flop_model": "20 per P2P pair + 66 per P2C evaluation",
                 "peak_source": f"nominal: {nsm} SMs x {lanes} {'FP32' if lanes == 128 else 'FP64'} lanes x 2 x "
@@ -346,18 +346,27 @@ def main():
     return 0
 
 
-# DRAM bytes (read + write) of one mixed traversal on the default workload
-# (Plummer N = 2^24, bucket 32, theta 0.7): walk_lists + eval_p2c + eval_p2p,
-# from ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum (1 pass);
-# profiles/traffic_traverse_mixed_plummer_16m.md holds the command and figures.
-TRAVERSE_MIXED_TRAFFIC_16M = (517378560 + 8313764352) + (8061403904 + 662865664) + (3190561280 + 539555840)
+# DRAM bytes (read + write) per particle of the three kernels of one mixed
+# traversal, Plummer sphere, bucket 32, theta 0.7, eps 1e-3: ncu
+# dram__bytes_read.sum + dram__bytes_write.sum of one launch of each kernel on
+# the N = 2^21 pass, divided by N (profiles/traversal_kernels_plummer_2m.md
+# holds the command and the figures).  Every kernel reads and writes in
+# proportion to the interactions, which grow with N in the same proportion at
+# fixed theta, so the per-particle figure scales to the bench size.
+TRAVERSE_MIXED_DRAM_PER_PARTICLE = {
+    "walk_lists": (60522752 + 892398848) / 2097152.0,
+    "eval_p2c": (899716864 + 79135488) / 2097152.0,
+    "eval_p2p": (412065024 + 64519936) / 2097152.0,
+}
+TRAVERSE_MIXED_DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of each kernel at "
+                              "N = 2^21, scaled by N (profiles/traversal_kernels_plummer_2m.md)")
 
 
 def traversal_traffic(a):
-    """Measured DRAM bytes per traversal launch, scaled by particles from the
-    captured workload; None for other workloads."""
+    """DRAM bytes of one mixed traversal at the bench size, from the
+    per-particle figures measured at N = 2^21; None for other workloads."""
     if (a.workload, a.theta, a.bucket, a.precision, a.soft) == ("plummer", 0.7, 32, "mixed", 1e-3):
-        return TRAVERSE_MIXED_TRAFFIC_16M * a.n / float(1 << 24)
+        return sum(TRAVERSE_MIXED_DRAM_PER_PARTICLE.values()) * a.n
     return None
 
 

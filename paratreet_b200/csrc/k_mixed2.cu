@@ -233,10 +233,15 @@ __global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravPa
 
 // ---------------------------------------------------------------- phase B
 constexpr int kEvWarps = 4;
-// CTAs per SM of eval_p2c (80 registers); 7 and 8 fit without spills but
-// measured slower: their shared memory leaves less L1 for the node records
+// CTAs per SM of eval_p2c (72 registers, no spills; 6 and 8 measured 0.2 and
+// 0.3 ms slower at N = 2^24: more CTAs take shared memory from the L1 that
+// holds the node records)
 #ifndef PT_P2C_MINB
-#define PT_P2C_MINB 6
+#define PT_P2C_MINB 7
+#endif
+// CTAs per SM of eval_p2p (64 registers; 7 measured 0.5 ms slower)
+#ifndef PT_P2P_MINB
+#define PT_P2P_MINB 8
 #endif
 
 // Per-warp shared memory of eval_p2p ...
@@ -252,7 +257,7 @@ struct EvalWarp {
 // CTAs is L1 lost to its node records)
 struct EvalWarpC {
   BucketGeom geom;
-  float4 st[6][32];            // staged node pairs, six rows
+  float4 st[5][32];            // staged node pairs, five rows (offset, mass, traceless moments)
   float4 ks[2][32];            // each lane's compensated sums and their compensations
   int32_t spec[kWlBuf];        // the chunk's near and monopole entries (scalar pass)
 };
@@ -467,13 +472,21 @@ __device__ __noinline__ P2cTerm ev_p2c_scalar(float ox, float oy, float oz, floa
 // lane's target (GravityVisitor::node, examples/GravityVisitor.h:184-224, in
 // packed FP32).  Near and monopole nodes are staged as zero-mass padding and
 // evaluated apart (ev_p2c_specials), so this loop has no branch.
+//
+// The moments are staged traceless, Qt = Q - (trace Q / 3) I.  With
+// a = 1/r, b = a^3, c = 3 b a^2, d = 5 c a^2 the reference's unsoftened terms
+// (qir = r.Q.r / 2, tr = trace Q / 2)
+//   pot = -M a - c qir + b tr,  acc = -(b M + d qir - c tr) r + c Q r
+// equal, since c r^2 = 3 b and d r^2 = 5 c,
+//   pot = -M a - c qt,          acc = -(b M + d qt) r + c Qt r
+// with qt = r.Qt.r / 2: the trace terms cancel exactly, which saves three of
+// 37 operations per evaluation and one staged row.
 __device__ __forceinline__ void ev_p2c_pairs(const EvalWarpC& w, const EvTarget& x, int npair, float2 ntx, float2 nty,
                                              float2 ntz, float2& ax2, float2& ay2, float2& az2, float2& pp2,
                                              float2& mm2) {
-  const float2 mthree = make_float2(-3.f, -3.f), mfive = make_float2(-5.f, -5.f), half = make_float2(0.5f, 0.5f);
-  const float4* sp = &w.st[0][x.grp];  // rows st[1..5] follow at +32 each
+  const float2 mthree = make_float2(-3.f, -3.f), m25 = make_float2(-2.5f, -2.5f), half = make_float2(0.5f, 0.5f);
+  const float4* sp = &w.st[0][x.grp];  // rows st[1..4] follow at +32 each
   for (int k = x.grp; k < npair; k += x.G, sp += x.G) {
-    const float4 P5 = sp[160];
     const float4 P0 = sp[0], P1 = sp[32];
     const float2 rx = __fadd2_rn(make_float2(P0.x, P0.y), ntx);  // r' = o - t = -r
     const float2 ry = __fadd2_rn(make_float2(P0.z, P0.w), nty);
@@ -486,21 +499,20 @@ __device__ __forceinline__ void ev_p2c_pairs(const EvalWarpC& w, const EvTarget&
     const float2 d2 = __fmul2_rn(a, a);
     const float2 bb = __fmul2_rn(a, d2);                       // b = 1/r^3
     const float2 nc = __fmul2_rn(__fmul2_rn(bb, d2), mthree);  // -c = -3/r^5
-    const float2 d = __fmul2_rn(__fmul2_rn(nc, d2), mfive);    // d = 15/r^7
     const float2 xx = make_float2(P2.x, P2.y), xy = make_float2(P2.z, P2.w);
     const float2 xz = make_float2(P3.x, P3.y), yy = make_float2(P3.z, P3.w);
     const float2 yz = make_float2(P4.x, P4.y), zz = make_float2(P4.z, P4.w);
-    const float2 qx = __ffma2_rn(xz, rz, __ffma2_rn(xy, ry, __fmul2_rn(xx, rx)));  // q' = -q
+    const float2 qx = __ffma2_rn(xz, rz, __ffma2_rn(xy, ry, __fmul2_rn(xx, rx)));  // q' = Qt r' = -Qt r
     const float2 qy = __ffma2_rn(yz, rz, __ffma2_rn(yy, ry, __fmul2_rn(xy, rx)));
     const float2 qz = __ffma2_rn(zz, rz, __ffma2_rn(yz, ry, __fmul2_rn(xz, rx)));
-    const float2 qir = __fmul2_rn(half, __ffma2_rn(qz, rz, __ffma2_rn(qy, ry, __fmul2_rn(qx, rx))));
-    const float2 M = make_float2(P1.z, P1.w), tr = make_float2(P5.x, P5.y);
-    // qir3 = b M + d qir - c tr; acc += qir3 r' - c q'; pot += b tr - c qir - M a
-    const float2 qir3 = __ffma2_rn(nc, tr, __ffma2_rn(d, qir, __fmul2_rn(bb, M)));
-    ax2 = __ffma2_rn(nc, qx, __ffma2_rn(qir3, rx, ax2));
-    ay2 = __ffma2_rn(nc, qy, __ffma2_rn(qir3, ry, ay2));
-    az2 = __ffma2_rn(nc, qz, __ffma2_rn(qir3, rz, az2));
-    pp2 = __ffma2_rn(nc, qir, __ffma2_rn(bb, tr, pp2));
+    const float2 cq = __fmul2_rn(nc, __ffma2_rn(qz, rz, __ffma2_rn(qy, ry, __fmul2_rn(qx, rx))));  // -2 c qt
+    const float2 M = make_float2(P1.z, P1.w);
+    // A = b M + d qt = b M - (5 / 2) a^2 (-2 c qt); acc += A r' - c q'; pot += -c qt - M a
+    const float2 A = __ffma2_rn(__fmul2_rn(d2, m25), cq, __fmul2_rn(bb, M));
+    ax2 = __ffma2_rn(nc, qx, __ffma2_rn(A, rx, ax2));
+    ay2 = __ffma2_rn(nc, qy, __ffma2_rn(A, ry, ay2));
+    az2 = __ffma2_rn(nc, qz, __ffma2_rn(A, rz, az2));
+    pp2 = __ffma2_rn(half, cq, pp2);
     mm2 = __ffma2_rn(M, a, mm2);
   }
 }
@@ -599,15 +611,18 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams
           if (spec[0]) w.spec[at] = ec[0];
           if (spec[1]) w.spec[at + (spec[0] ? 1 : 0)] = ec[1];
         }
+#pragma unroll
+        for (int h = 0; h < 2; h++) {  // traceless moments: xx, yy, zz less a third of the trace
+          const float t3 = (r0[h].z + r1[h].y + r1[h].w) * (1.0f / 3.0f);
+          r0[h].z -= t3;
+          r1[h].y -= t3;
+          r1[h].w -= t3;
+        }
         w.st[0][lane] = make_float4(o[0].x, o[1].x, o[0].y, o[1].y);
         w.st[1][lane] = make_float4(o[0].z, o[1].z, r0[0].x, r0[1].x);
         w.st[2][lane] = make_float4(r0[0].z, r0[1].z, r0[0].w, r0[1].w);
         w.st[3][lane] = make_float4(r1[0].x, r1[1].x, r1[0].y, r1[1].y);
         w.st[4][lane] = make_float4(r1[0].z, r1[1].z, r1[0].w, r1[1].w);
-        {  // (tr_a, tr_b, soft_a, soft_b)
-          const float tra = 0.5f * (r0[0].z + r1[0].y + r1[0].w), trb = 0.5f * (r0[1].z + r1[1].y + r1[1].w);
-          w.st[5][lane] = make_float4(tra, trb, r0[0].y, r0[1].y);
-        }
         __syncwarp();
         const int npair = (min(64, count - cs) + 1) >> 1;
         if (x.grp < x.G) {
@@ -944,9 +959,6 @@ void launch_walk_lists(const TravParams& P, const ListParams& L, const Mom* mom,
   note_launch();
   walk_lists<<<grid, kWlWarps * 32, 0, st>>>(P, L, mom);
 }
-// eval_p2c keeps 80 registers (6 CTAs per SM; at 64 it spills), eval_p2p
-// 64 (8 CTAs per SM; its two-target path spills 52 bytes there, and still
-// measured faster than at 72 registers and 7 CTAs per SM)
 void launch_eval_lists(const TravParams& P, const ListParams& L, const Mom* mom, int grid, cudaStream_t st,
                        unsigned* work2) {
   TravParams Q = P;
@@ -954,7 +966,7 @@ void launch_eval_lists(const TravParams& P, const ListParams& L, const Mom* mom,
   note_launch();
   eval_p2c<PT_P2C_MINB><<<grid, kEvWarps * 32, 0, st>>>(P, L, mom);
   note_launch();
-  eval_p2p<8><<<grid, kEvWarps * 32, 0, st>>>(Q, L, mom);
+  eval_p2p<PT_P2P_MINB><<<grid, kEvWarps * 32, 0, st>>>(Q, L, mom);
 }
 
 }  // namespace pt

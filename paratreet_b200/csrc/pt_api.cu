@@ -335,9 +335,12 @@ int build_tree(pt_handle* h) {
   CK(cudaStreamSynchronize(st));
   h->nbuckets = nl;
   if (nl > h->cap_buckets) {
-    CKR(dalloc(h, &h->buckets, nl));
-    CKR(dalloc(h, &h->bucket_work, nl));
-    h->cap_buckets = nl;
+    // an eighth of headroom: the bucket count drifts from pass to pass as the
+    // particles move, and a cudaFree on every new maximum would stall the device
+    const int64_t cap = (int64_t)nl + nl / 8 + 64;
+    CKR(dalloc(h, &h->buckets, cap));
+    CKR(dalloc(h, &h->bucket_work, cap));
+    h->cap_buckets = cap;
   }
   launch_assign_buckets(h->nd, h->nnodes, h->buckets, nl, st);
   CK(cudaGetLastError());
@@ -451,11 +454,12 @@ int run_two_phase(pt_handle* h, TravParams& P) {
   const int64_t nb = P.b_end - P.b_begin;
   if (nb <= 0) return PT_OK;
   if (nb > h->l_nb_cap) {
-    CKR(dalloc(h, &h->l_pc_start, nb));
-    CKR(dalloc(h, &h->l_pp_start, nb));
-    CKR(dalloc(h, &h->l_pc_count, nb));
-    CKR(dalloc(h, &h->l_pp_count, nb));
-    h->l_nb_cap = nb;
+    const int64_t cap = nb + nb / 8 + 64;  // headroom, as for the bucket arrays
+    CKR(dalloc(h, &h->l_pc_start, cap));
+    CKR(dalloc(h, &h->l_pp_start, cap));
+    CKR(dalloc(h, &h->l_pc_count, cap));
+    CKR(dalloc(h, &h->l_pp_count, cap));
+    h->l_nb_cap = cap;
   }
   if (!h->d_lcur) CKR(dalloc(h, &h->d_lcur, 3));
   if (!h->d_work3) CKR(dalloc(h, &h->d_work3, 3));
