@@ -432,7 +432,8 @@ def driver_step_rate(a, sim, stream, steps=20):
     return {"s_per_step": step / 1e3, "s_per_step_mean": float(np.mean(ts)) / 1e3,
             "s_per_step_max": float(np.max(ts)) / 1e3, "max_over_median": float(np.max(ts)) / step,
             "force_pass_ms": force, "rest_ms": step - force,
-            "steps_ms": [round(t, 3) for t in ts], "warmup_steps": 2,
+            "steps_ms": [round(t, 3) for t in ts], "force_pass_ms_per_step": [round(t, 3) for t in tf],
+            "warmup_steps": 2,
             "note": f"median, mean and max of {steps} consecutive steps; rest = time step (max-speed "
                     "reduction) + kick/perturb kernel + host synchronisation of the median step"}
 
@@ -571,10 +572,11 @@ def accuracy_clause(a, sim, tgt, direct, stream, bound=1e-4, lo=0.35, hi=0.50):
 def adjoint_cost(a, stream):
     """Cost of one adjoint force pass against one forward pass on the
     differentiation workload (Hernquist N = 262,144, seed 3, eps 0.01,
-    theta 0.6, bucket 16): the forward pass that records the interaction
-    lists the adjoint differentiates (mixed form), the plain two-phase mixed
-    pass, and pt_adjoint (cotangent in and gradients out through host
-    memory), each the mean of 3 after one untimed call."""
+    theta 0.6, bucket 16), each through the C ABI with its host data: the
+    forward pass with its accelerations read back (the plain two-phase mixed
+    pass, and the pass that also records the interaction lists the adjoint
+    differentiates), and pt_adjoint with the cotangent in and the gradients
+    out.  Each the mean of 5 calls after two untimed ones."""
     import torch
     from paratreet_b200 import ics
     from paratreet_b200.gravity import GravitySimulation
@@ -582,7 +584,8 @@ def adjoint_cost(a, stream):
     q = ics.hernquist(n, seed=3, soft=0.01)
     cot = np.random.default_rng(64).normal(size=(3, n))
 
-    def timed(f, reps=3):
+    def timed(f, reps=5):
+        f()
         f()
         s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s0.record(stream)
@@ -592,15 +595,21 @@ def adjoint_cost(a, stream):
         torch.cuda.synchronize()
         return s0.elapsed_time(s1) / reps
 
-    out = {"workload": "hernquist N=262144 eps=0.01 bucket=16 theta=0.6"}
+    def forward(sim):
+        sim.start_down()
+        sim.accelerations()
+
+    out = {"workload": "hernquist N=262144 eps=0.01 bucket=16 theta=0.6",
+           "note": "each call through the C ABI with its host data (accelerations read back; cotangent in, "
+                   "gradients out)"}
     with GravitySimulation(max_particles_per_leaf=16, theta=0.6, precision="mixed") as plain:
         plain.set_stream(stream.cuda_stream)
         plain.set_particles(q)
-        out["forward_ms_two_phase"] = timed(plain.start_down)
+        out["forward_ms_two_phase"] = timed(lambda: forward(plain))
     with GravitySimulation(max_particles_per_leaf=16, theta=0.6, precision="mixed", record_lists=True) as s:
         s.set_stream(stream.cuda_stream)
         s.set_particles(q)
-        out["forward_ms_recording_lists"] = timed(s.start_down)
+        out["forward_ms_recording_lists"] = timed(lambda: forward(s))
         s.start_down()
         out["adjoint_ms"] = timed(lambda: s.adjoint(*cot))
     out["adjoint_over_recording_forward"] = out["adjoint_ms"] / out["forward_ms_recording_lists"]

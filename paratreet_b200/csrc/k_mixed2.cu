@@ -93,6 +93,10 @@ __device__ __forceinline__ bool drain(const int32_t* buf, int n, Region& r, unsi
 #ifndef PT_WALK_MINB
 #define PT_WALK_MINB 7
 #endif
+// kOffset: the replica offset (P.ox, P.oy, P.oz) may be non-zero (periodic
+// walks); without it the walk skips three FP64 adds at the head of every
+// classification's dependent chain (c + 0.0 == c, so the tests are unchanged).
+template <bool kOffset>
 __global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravParams P, ListParams L,
                                                                          const Mom* __restrict__ mom) {
   __shared__ WalkWarp warps[kWlWarps];
@@ -152,7 +156,8 @@ __global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravPa
           atomicOr(P.status, kErrCapacity);
         } else {
           r = P.walk[node];
-          cls = classify_node_gap(r, blo, bhi, g, P.ox, P.oy, P.oz, gap2);
+          if (kOffset) cls = classify_node_gap(r, blo, bhi, g, P.ox, P.oy, P.oz, gap2);
+          else cls = classify_node_gap_nooff(r, blo, bhi, g, gap2);
         }
       }
       opens += (unsigned long long)__popc(__ballot_sync(kFull, node >= 0 && node < P.nnodes &&
@@ -871,10 +876,10 @@ __device__ __noinline__ unsigned long long mark_near_leaves(const WalkRec* __res
   for (int k0 = 0; k0 < count; k0 += 32) {
     const int k = k0 + lane;
     unsigned cnt = 0;
-    if (k < count) {
-      const int e = list[k] & 0x7fffffff;
+    if (k < count) {  // the walk wrote the entries with bit 31 clear: only near leaves are stored
+      const int e = list[k];
       cnt = (unsigned)walk[e].pcount;
-      list[k] = p2p_leaf_near(walk, e, g->lo, g->hi, g->soft_max, ox, oy, oz) ? (e | (int)0x80000000) : e;
+      if (p2p_leaf_near(walk, e, g->lo, g->hi, g->soft_max, ox, oy, oz)) list[k] = e | (int)0x80000000;
     }
     nsrc += __reduce_add_sync(kFull, cnt);
   }
@@ -957,7 +962,8 @@ int walk_lists_grid(int sms) { return sms * PT_WALK_MINB; }  // the CTAs residen
 
 void launch_walk_lists(const TravParams& P, const ListParams& L, const Mom* mom, int grid, cudaStream_t st) {
   note_launch();
-  walk_lists<<<grid, kWlWarps * 32, 0, st>>>(P, L, mom);
+  if (P.ox == 0.0 && P.oy == 0.0 && P.oz == 0.0) walk_lists<false><<<grid, kWlWarps * 32, 0, st>>>(P, L, mom);
+  else walk_lists<true><<<grid, kWlWarps * 32, 0, st>>>(P, L, mom);
 }
 void launch_eval_lists(const TravParams& P, const ListParams& L, const Mom* mom, int grid, cudaStream_t st,
                        unsigned* work2) {

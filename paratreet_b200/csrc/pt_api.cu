@@ -105,7 +105,8 @@ struct pt_handle {
   bool forces_current = false;  // ... and the positions have not moved since
   bool trav_range_partial = false;
 
-  double* adj = nullptr;  // adjoint scratch: cotangent (3N) and gradients (4N), sorted + caller order
+  double* adj = nullptr;  // adjoint scratch: cotangent (3N) and gradients (4N), sorted + caller order,
+                          // then pt_adjoint's caller-order input and output (7N)
   int64_t adj_cap = 0;
   double* nadj = nullptr;  // 10 adjoint values per node
   int64_t nadj_cap = 0;
@@ -1458,7 +1459,7 @@ int pt_ewald_direct_sum(pt_handle* h, int64_t nt, const int32_t* targets, double
 namespace {
 
 int ensure_adjoint(pt_handle* h) {
-  const int64_t need = 14 * std::max<int64_t>(h->n, 1);
+  const int64_t need = 21 * std::max<int64_t>(h->n, 1);
   if (need > h->adj_cap) {
     CKR(dalloc(h, &h->adj, need));
     h->adj_cap = need;
@@ -1591,8 +1592,7 @@ int pt_adjoint(pt_handle* h, const double* cax, const double* cay, const double*
   const int64_t n = h->n;
   if (n == 0) return PT_OK;
   CKR(ensure_adjoint(h));
-  double* buf = nullptr;  // caller-order cotangent (3N) and gradients (4N)
-  CK(cudaMalloc((void**)&buf, 7 * n * sizeof(double)));
+  double* buf = h->adj + 14 * n;  // caller-order cotangent (3N) and gradients (4N), kept by the handle
   const double* hin[3] = {cax, cay, caz};
   for (int k = 0; k < 3; k++) {
     CK(cudaMemcpyAsync(buf + k * n, hin[k], n * sizeof(double), cudaMemcpyHostToDevice, st));
@@ -1601,10 +1601,9 @@ int pt_adjoint(pt_handle* h, const double* cax, const double* cay, const double*
   if (rc == PT_OK) {
     double* hout[4] = {gx, gy, gz, gm};
     for (int k = 0; k < 4; k++)
-      if (hout[k]) cudaMemcpyAsync(hout[k], buf + (3 + k) * n, n * sizeof(double), cudaMemcpyDeviceToHost, st);
-    cudaStreamSynchronize(st);
+      if (hout[k]) CK(cudaMemcpyAsync(hout[k], buf + (3 + k) * n, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
   }
-  cudaFree(buf);
   return rc;
 }
 

@@ -141,6 +141,19 @@ __device__ __forceinline__ int classify_node_gap(const WalkRec& w, const double 
   return open_softening_gap(cx, cy, cz, w.soft, g.cm[0], g.cm[1], g.cm[2], g.soft, gap2) ? kClsMono : kClsQuad;
 }
 
+// The same without a replica offset (the node's centre as it is).
+__device__ __forceinline__ int classify_node_gap_nooff(const WalkRec& w, const double lo[3], const double hi[3],
+                                                       const BucketGeom& g, double& gap2) {
+  gap2 = -1.0;
+  if (w.type == kTypeLeaf) return kClsP2P;
+  if (w.type != kTypeInternal) return kClsNone;
+  if (w.count <= kMinParticleNode) return kClsOpen;
+  gap2 = box_gap2_exact(lo, hi, w.cm[0], w.cm[1], w.cm[2]);
+  if (gap2 <= w.orsq) return kClsOpen;
+  return open_softening_gap(w.cm[0], w.cm[1], w.cm[2], w.soft, g.cm[0], g.cm[1], g.cm[2], g.soft, gap2) ? kClsMono
+                                                                                                       : kClsQuad;
+}
+
 __device__ __forceinline__ int classify_node_gap(const WalkRec& w, const BucketGeom& g, double ox, double oy,
                                                  double oz, double& gap2) {
   return classify_node_gap(w, g.lo, g.hi, g, ox, oy, oz, gap2);

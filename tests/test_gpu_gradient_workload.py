@@ -181,7 +181,10 @@ def test_gradient_workload_hernquist_262k():
     assert slack_d[ok].max() <= 0.0, rep_d
     # the FP32-interaction chain differentiates a slightly different trajectory
     # (forces within ~1e-7 of FP64 per step); its gradient is held to 1e-3
-    assert rel_m[ok].max() <= 1e-3, rep_m
+    # relative, with the same allowance for the finite differences' own error
+    f = np.array([r[0] for r in fd])
+    eta = np.array([r[1] for r in fd])
+    assert (np.abs(f - am) - (1e-3 * np.abs(am) + 3.0 * eta))[ok].max() <= 0.0, rep_m
 
 
 def oracle_chain(q, steps, dt, theta, bucket):

@@ -11,7 +11,9 @@ The net force on a displaced lattice is a small residual (rms |a| ~ 0.011
 G M / L^2 here) and shrinks as 1 / ngrid, while the tree's absolute error at a
 given theta does not (about 8e-3 G M / L^2 at theta 0.7 for 16^3 to 64^3 in the
 C oracle), so the per-particle relative error of the reference method is of
-order one at this size; rms |da| / rms |a| is reported beside it."""
+order one at this size.  The error is therefore also stated relative to the
+rms force, |da| / rms|a| (rms and p99), at theta 0.7 and at theta 0.4, where
+it falls by a factor of seven."""
 import json
 import os
 import time
@@ -86,5 +88,10 @@ def test_periodic_lattice_workload():
     for prec in ("fp64", "mixed"):
         # the error relative to the rms force falls with theta at this size
         assert e[f"{prec}_theta0.4"]["abs_rms_over_force_rms"] < 0.5 * e[f"{prec}_theta0.7"]["abs_rms_over_force_rms"]
-    if NGRID == 256:  # measured on B200: see the module docstring
-        assert e["fp64_theta0.7"]["abs_rms"] < 2e-2
+    if NGRID == 256:
+        # measured on B200 (both forms): |da| / rms|a| rms 0.714 (p99 1.38) at
+        # theta 0.7 and 0.101 (p99 0.198) at theta 0.4; held within a tenth
+        for prec in ("fp64", "mixed"):
+            assert e[f"{prec}_theta0.7"]["abs_rms_over_force_rms"] < 0.79
+            assert e[f"{prec}_theta0.4"]["abs_rms_over_force_rms"] < 0.111
+            assert e[f"{prec}_theta0.4"]["abs_p99_over_force_rms"] < 0.22
