@@ -105,6 +105,7 @@ __global__ void __launch_bounds__(kE64Warps * 32) eval_p2c_f64(TravParams P, Lis
     const int64_t lb = b - P.b_begin;
     const int64_t start = L.pc_start[lb];
     const int count = L.pc_count[lb];
+    if (count == 0 && P.accumulate) continue;  // nothing to add (the first walk stores, even zeros)
     const int tbase = P.walk[tnode].pstart, ntot = P.walk[tnode].pcount;
     for (int tc = 0; tc < ntot; tc += 32) {
       const int t0 = tbase + tc, nt = min(32, ntot - tc);
@@ -258,6 +259,7 @@ __global__ void __launch_bounds__(kE64Warps * 32) eval_p2p_f64(TravParams P, Lis
     const int64_t lb = b - P.b_begin;
     const int64_t start = L.pp_start[lb];
     const int count = L.pp_count[lb];
+    if (count == 0) continue;  // P2P only adds
     const int tbase = P.walk[tnode].pstart, ntot = P.walk[tnode].pcount;
     BucketGeom g;
     load_bucket_geom(mom, tnode, g);

@@ -560,6 +560,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams
     const int64_t lb = b - P.b_begin;
     const int64_t start = L.pc_start[lb];
     const int count = L.pc_count[lb];
+    if (count == 0 && P.accumulate) continue;  // nothing to add (the first walk stores, even zeros)
     __syncwarp();
     if (lane == 0) load_bucket_geom(mom, tnode, w.geom);
     __syncwarp();
@@ -927,6 +928,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2p(TravParams
     const int64_t lb = b - P.b_begin;
     const int64_t start = L.pp_start[lb];
     const int count = L.pp_count[lb];
+    if (count == 0) continue;  // P2P only adds (the outer replica walks leave most lists empty)
     __syncwarp();
     if (lane == 0) load_bucket_geom(mom, tnode, w.geom);
     __syncwarp();
