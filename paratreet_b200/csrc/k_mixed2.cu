@@ -26,6 +26,25 @@
 
 namespace pt {
 
+// Phase timers of a diagnostic build (PT_PROF=1): lane 0 adds the clock
+// cycles since the previous mark to a per-warp slot in shared memory; the
+// slots are summed into g_prof when the warp exits.
+#ifndef PT_PROF
+#define PT_PROF 0
+#endif
+#if PT_PROF
+__device__ unsigned long long g_prof[32];
+#define PROF_FIELDS unsigned prof[6]; unsigned tlast;
+#define PROF_START(w) if (lane == 0) { for (int i_ = 0; i_ < 6; i_++) (w).prof[i_] = 0; (w).tlast = (unsigned)clock(); }
+#define PROF_MARK(w, i) if (lane == 0) { const unsigned t_ = (unsigned)clock(); (w).prof[i] += t_ - (w).tlast; (w).tlast = t_; }
+#define PROF_FLUSH(w, base) if (lane == 0) { for (int i_ = 0; i_ < 6; i_++) atomicAdd(&g_prof[(base) + i_], (unsigned long long)(w).prof[i_]); }
+#else
+#define PROF_FIELDS
+#define PROF_START(w)
+#define PROF_MARK(w, i)
+#define PROF_FLUSH(w, base)
+#endif
+
 constexpr int kWlWarps = 4;
 constexpr int kWlStack = 640;  // opened nodes pending (as the fused walk)
 constexpr int kWlBuf = 64;
@@ -35,6 +54,7 @@ struct WalkWarp {
   int32_t stack[kWlStack];
   int32_t pcbuf[kWlBuf];  // P2C entries waiting to be written
   int32_t ppbuf[kWlBuf];  // P2P entries waiting to be written
+  PROF_FIELDS
 };
 
 // Per-warp region of one pool: [cur, end).
@@ -89,6 +109,45 @@ __device__ __forceinline__ bool drain(const int32_t* buf, int n, Region& r, unsi
   return true;
 }
 
+#ifndef PT_SMQ_BATCH
+#define PT_SMQ_BATCH 32
+#endif
+// The next bucket index of a warp (lane 0 grabs, all lanes receive it).  With
+// smq, the warps of one SM take consecutive buckets from a batch of
+// PT_SMQ_BATCH that the SM's queue holds, so the warps resident on an SM work
+// on neighbouring buckets: their targets, results and most of their node
+// records share cache lines.  (On the periodic 256^3 lattice pass, whose outer
+// replica walks leave little work per bucket besides loading its targets and
+// adding to its results, this measured 239.5 -> 214.4 ms; the Plummer pass at
+// N = 2^24 is unchanged.)  A queue word is (batch start + 1) << 32 | next
+// index; zero = no batch yet.
+// The warp that draws index 0 of an empty queue, or the index one past the
+// batch, takes a new batch from the global counter (keeping its first bucket);
+// warps that draw past the batch meanwhile take single buckets.
+__device__ __forceinline__ unsigned grab_bucket(unsigned* work, unsigned long long* smq, int lane) {
+  unsigned bi = 0;
+  if (lane == 0) {
+    if (smq == nullptr) {
+      bi = atomicAdd(work, 1u);
+    } else {
+      unsigned sm;
+      asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+      unsigned long long* q = smq + (sm & 255u);
+      const unsigned long long old = atomicAdd(q, 1ull);
+      const unsigned hi = (unsigned)(old >> 32), idx = (unsigned)old;
+      if (hi != 0u && idx < (unsigned)PT_SMQ_BATCH) {
+        bi = hi - 1u + idx;
+      } else if (hi == 0u ? idx == 0u : idx == (unsigned)PT_SMQ_BATCH) {
+        bi = atomicAdd(work, (unsigned)PT_SMQ_BATCH);
+        atomicExch(q, ((unsigned long long)(bi + 1u) << 32) | 1ull);
+      } else {
+        bi = atomicAdd(work, 1u);
+      }
+    }
+  }
+  return __shfl_sync(kFull, bi, 0);
+}
+
 // CTAs per SM of the walk (72 registers); 6 and 8 measured slower at N = 2^24
 #ifndef PT_WALK_MINB
 #define PT_WALK_MINB 7
@@ -106,10 +165,9 @@ __global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravPa
   unsigned max_len = 0;
   Region rpc{0, 0}, rpp{0, 0};
   bool pool_ok = true;
+  PROF_START(w);
   while (true) {
-    unsigned bi = 0;
-    if (lane == 0) bi = atomicAdd(P.work, 1u);
-    bi = __shfl_sync(kFull, bi, 0);
+    const unsigned bi = grab_bucket(P.work, P.smq, lane);
     const int64_t b = P.b_begin + (int64_t)bi;
     if (b >= P.b_end) break;
     const int64_t lb = b - P.b_begin;
@@ -140,6 +198,7 @@ __global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravPa
     int sp = 0, nc = 0, np = 0;
     int nexp = 1, pop = -1;
     bool ok = true, fits = true;
+    PROF_MARK(w, 0);
     while (true) {
       const int e = lane >> 3, c = lane & 7;
       int node = -1;
@@ -170,6 +229,7 @@ __global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravPa
         const double reach = (r.soft + g.soft_max) * (1.0 + 1e-5);
         near = !(gap2 > reach * reach);
       }
+      PROF_MARK(w, 1);
       {
         const bool pc = (cls == kClsQuad || cls == kClsMono);
         const unsigned m = __ballot_sync(kFull, pc);
@@ -195,6 +255,7 @@ __global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravPa
         sp += __popc(m);
       }
       __syncwarp();
+      PROF_MARK(w, 2);
       const bool last = (sp == 0);
       if (nc >= 32 || last) {
         fits = fits && drain(w.pcbuf, nc, rpc, pc0, L.pc_pool, L.cursor + 0, L.cap_pc, L.region, lane);
@@ -205,6 +266,7 @@ __global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravPa
         np = 0;
       }
       __syncwarp();
+      PROF_MARK(w, 3);
       if (last) break;
       nexp = sp < 4 ? sp : 4;
       sp -= nexp;
@@ -228,7 +290,10 @@ __global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravPa
       if (P.accumulate) wk += P.bucket_work[b];
       P.bucket_work[b] = wk;
     }
+    PROF_MARK(w, 4);
   }
+  PROF_MARK(w, 5);
+  PROF_FLUSH(w, 16);
   if (lane == 0) {
     atomicAdd(&P.counters[1], c_pc);
     atomicAdd(&P.counters[2], c_open);
@@ -256,6 +321,7 @@ struct EvalWarp {
   int32_t ps0[kWlBuf];         // first particle of each leaf - its stream position
   float4 lof[kWlBuf];          // leaf offsets cm_leaf - cm_bucket (FP32)
   int32_t lsel[kWlBuf];        // leaves of the current kind in a block
+  PROF_FIELDS
 };
 
 // ... and of eval_p2c (kept apart: shared memory taken from one kernel's
@@ -265,6 +331,7 @@ struct EvalWarpC {
   float4 st[5][32];            // staged node pairs, five rows (offset, mass, traceless moments)
   float4 ks[2][32];            // each lane's compensated sums and their compensations
   int32_t spec[kWlBuf];        // the chunk's near and monopole entries (scalar pass)
+  PROF_FIELDS
 };
 
 // Per-lane target of a 32-target chunk, replicated over G lane groups (lanes
@@ -422,9 +489,7 @@ __device__ __forceinline__ void ev_finish(W& w, const Kahan4& K, float pmono, co
 }
 
 __device__ __forceinline__ bool next_bucket(const TravParams& P, int lane, int64_t& b, int& tnode) {
-  unsigned bi = 0;
-  if (lane == 0) bi = atomicAdd(P.work, 1u);
-  bi = __shfl_sync(kFull, bi, 0);
+  const unsigned bi = grab_bucket(P.work, P.smq, lane);
   b = P.b_begin + (int64_t)bi;
   if (b >= P.b_end) return false;
   tnode = P.buckets[b];
@@ -555,6 +620,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams
   const float kPad = 1.0e10f;
   int64_t b;
   int tnode;
+  PROF_START(w);
   while (next_bucket(P, lane, b, tnode)) {
     if (tnode < 0 || tnode >= P.nnodes) continue;
     const int64_t lb = b - P.b_begin;
@@ -579,6 +645,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams
       // the node records wait at staging time
       int en0 = (2 * lane < count) ? L.pc_pool[start + 2 * lane] : 0;
       int en1 = (2 * lane + 1 < count) ? L.pc_pool[start + 2 * lane + 1] : 0;
+      PROF_MARK(w, 0);
       for (int cs = 0; cs < count; cs += 64) {
         const int ec[2] = {en0, en1};
         if (cs + 64 < count) {
@@ -631,9 +698,12 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams
         w.st[4][lane] = make_float4(r1[0].z, r1[1].z, r1[0].w, r1[1].w);
         __syncwarp();
         const int npair = (min(64, count - cs) + 1) >> 1;
+        PROF_MARK(w, 1);
         if (x.grp < x.G) {
           ev_p2c_pairs(w, x, npair, ntx, nty, ntz, ax2, ay2, az2, pp2, mm2);
+          PROF_MARK(w, 2);
           if (ns) ev_p2c_specials(w, P, x, ns, ax2, ay2, az2, pp2, pmono);
+          PROF_MARK(w, 3);
         }
         if (((cs >> 6) & 3) == 3 || cs + 64 >= count) {
           float4 ks = w.ks[0][lane], kc = w.ks[1][lane];
@@ -653,8 +723,11 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams
         K.c[0] = kc.x; K.c[1] = kc.y; K.c[2] = kc.z; K.c[3] = kc.w;
       }
       ev_finish(w, K, pmono, x, P, t0, lane, true, P.accumulate == 0);
+      PROF_MARK(w, 4);
     }
   }
+  PROF_MARK(w, 5);
+  PROF_FLUSH(w, 0);
 }
 
 // One source of a near leaf: Newtonian beyond the softening reach, the spline
@@ -721,6 +794,7 @@ __device__ __forceinline__ void ev_p2p_leaves(EvalWarp& w, int nleaves, const Tr
   if (__any_sync(kFull, (lane < nleaves && na == 0) || (lane + 32 < nleaves && nb == 0)) && lane == 0)
     atomicOr(P.status, kErrCapacity);
   __syncwarp();
+  PROF_MARK(w, 1);
   const float kPadPos = 1.0e10f;
   const float gs = (float)w.geom.soft_max;
   float2 ntx, nty, ntz;
@@ -777,6 +851,7 @@ __device__ __forceinline__ void ev_p2p_leaves(EvalWarp& w, int nleaves, const Tr
       __syncwarp();
     }
     const int np = (min(64, total - cs) + 1) >> 1;
+    PROF_MARK(w, 2);
     if constexpr (kTwo) {
       if (x.grp < x.G) {
         const float4* sp = &w.st[0][x.grp];
@@ -842,6 +917,7 @@ __device__ __forceinline__ void ev_p2p_leaves(EvalWarp& w, int nleaves, const Tr
       }
     }
     }
+    PROF_MARK(w, 3);
   }
   if constexpr (kTwo) {
     K.add(0, ax2.x);
@@ -923,6 +999,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2p(TravParams
   unsigned long long c_pp = 0;
   int64_t b;
   int tnode;
+  PROF_START(w);
   while (next_bucket(P, lane, b, tnode)) {
     if (tnode < 0 || tnode >= P.nnodes) continue;
     const int64_t lb = b - P.b_begin;
@@ -934,6 +1011,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2p(TravParams
     __syncwarp();
     const int tbase = P.walk[tnode].pstart, ntot = P.walk[tnode].pcount;
     const unsigned long long nsrc = mark_near_leaves(P.walk, &w.geom, P.ox, P.oy, P.oz, L.pp_pool + start, count, lane);
+    PROF_MARK(w, 0);
     for (int tc = 0; tc < ntot; tc += 32) {
       const int t0 = tbase + tc, nt = min(32, ntot - tc);
       if (ev_two_targets(nt)) {
@@ -943,6 +1021,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2p(TravParams
         K.zero();
         ev_p2p_blocks<true>(w, P, L, x, start, count, lane, K);
         ev_finish2(w, K, x, P, t0, lane);
+        PROF_MARK(w, 4);
         continue;
       }
       const EvTarget x = ev_target(P.p, w.geom, t0, nt, lane);
@@ -950,14 +1029,25 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2p(TravParams
       K.zero();
       ev_p2p_blocks<false>(w, P, L, x, start, count, lane, K);
       ev_finish(w, K, 0.f, x, P, t0, lane, false, false);
+      PROF_MARK(w, 4);
     }
     // P2P pairs as the reference counts them (n_src * n_tgt per leaf(),
     // src/Traverser.h:27); the walk wrote the bucket's P2C work before
     c_pp += nsrc * (unsigned long long)ntot;
     if (P.bucket_work && lane == 0) P.bucket_work[b] += nsrc * (unsigned long long)ntot;
   }
+  PROF_MARK(w, 5);
+  PROF_FLUSH(w, 8);
   if (lane == 0) atomicAdd(&P.counters[0], c_pp);
 }
+
+#if PT_PROF
+extern "C" int pt_debug_prof(unsigned long long* out) {
+  if (cudaMemcpyFromSymbol(out, g_prof, sizeof(g_prof)) != cudaSuccess) return -1;
+  unsigned long long z[32] = {};
+  return cudaMemcpyToSymbol(g_prof, z, sizeof(z)) == cudaSuccess ? 0 : -1;
+}
+#endif
 
 // ---------------------------------------------------------------- launchers
 int walk_lists_grid(int sms) { return sms * PT_WALK_MINB; }  // the CTAs resident
@@ -971,6 +1061,7 @@ void launch_eval_lists(const TravParams& P, const ListParams& L, const Mom* mom,
                        unsigned* work2) {
   TravParams Q = P;
   Q.work = work2;
+  if (P.smq) Q.smq = P.smq + 256;  // P2P's queues follow P2C's
   note_launch();
   eval_p2c<PT_P2C_MINB><<<grid, kEvWarps * 32, 0, st>>>(P, L, mom);
   note_launch();

@@ -80,6 +80,7 @@ struct pt_handle {
   int64_t l_nb_cap = 0;
   unsigned long long* d_lcur = nullptr;  // [0] P2C cursor, [1] P2P cursor, [2] longest list
   unsigned* d_work3 = nullptr;           // bucket queues of the list kernels (walk, P2C, P2P)
+  unsigned long long* d_smq = nullptr;   // their per-SM batches, 256 words per kernel
   unsigned l_region = 32768;  // entries per warp region of the list pools
 
   double* sph = nullptr;  // SPH density pass: density, ball^2 (2n), neighbours (k n int32 + k n double)
@@ -464,6 +465,7 @@ int run_two_phase(pt_handle* h, TravParams& P) {
   }
   if (!h->d_lcur) CKR(dalloc(h, &h->d_lcur, 3));
   if (!h->d_work3) CKR(dalloc(h, &h->d_work3, 3));
+  if (!h->d_smq) CKR(dalloc(h, &h->d_smq, 3 * 256));
   const int wgrid = (int)std::max<int64_t>(1, std::min<int64_t>(walk_lists_grid(h->sms), (nb + 3) / 4));
   unsigned long long c0[3];
   CK(cudaMemcpyAsync(c0, h->d_counters, sizeof(c0), cudaMemcpyDeviceToHost, st));
@@ -522,8 +524,10 @@ int run_two_phase(pt_handle* h, TravParams& P) {
     L.max_len = reinterpret_cast<unsigned*>(h->d_lcur + 2);
     CK(cudaMemsetAsync(h->d_lcur, 0, 3 * sizeof(unsigned long long), st));
     CK(cudaMemsetAsync(h->d_work3, 0, 3 * sizeof(unsigned), st));
+    if (h->d_smq) CK(cudaMemsetAsync(h->d_smq, 0, 3 * 256 * sizeof(unsigned long long), st));
     TravParams A = P;
     A.work = h->d_work3;
+    A.smq = h->d_smq;
     launch_walk_lists(A, L, h->nd.mom, wgrid, st);
     CK(cudaGetLastError());
     unsigned status = 0;
@@ -550,6 +554,7 @@ int run_two_phase(pt_handle* h, TravParams& P) {
   }
   TravParams E = P;
   E.work = h->d_work3 + 1;
+  E.smq = h->d_smq ? h->d_smq + 256 : nullptr;
   if (h->cfg.precision == PT_FP64_LISTS) launch_eval_lists_f64(E, L, h->nd.mom, h->sms * 16, st, h->d_work3 + 2);
   else launch_eval_lists(E, L, h->nd.mom, h->sms * 16, st, h->d_work3 + 2);
   CK(cudaGetLastError());
@@ -870,7 +875,7 @@ int pt_destroy(pt_handle* h) {
   dfree(h->list_kind); dfree(h->dsum); dfree(h->adj); dfree(h->nadj); dfree(h->d_htab); dfree(h->ewd); dfree(h->sph); dfree(h->sph_nbr); dfree(h->sph_nd2);
   dfree(h->sph_list_d); dfree(h->sph_list_i); dfree(h->sph_state);
   dfree(h->pool_pc); dfree(h->pool_pp); dfree(h->l_pc_start); dfree(h->l_pp_start); dfree(h->l_pc_count);
-  dfree(h->l_pp_count); dfree(h->d_lcur); dfree(h->d_work3);
+  dfree(h->l_pp_count); dfree(h->d_lcur); dfree(h->d_work3); dfree(h->d_smq);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);

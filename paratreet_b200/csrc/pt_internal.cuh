@@ -123,6 +123,7 @@ struct TravParams {
   unsigned long long* counters;  // n_pp, n_pc, n_open
   unsigned int* work;     // dynamic bucket counter
   unsigned int* status;
+  unsigned long long* smq;  // per-SM bucket batches (list kernels; null: one bucket per grab)
 };
 
 // Interaction lists of the two-phase mixed traversal (k_mixed2.cu): two pools

@@ -336,12 +336,14 @@ class GravitySimulation:
         self._check(self._lib.pt_forces_frozen(self._h, *[L.ptr(a) for a in arrs]))
         return self.accelerations()
 
-    def adjoint(self, cax, cay, caz):
-        """Gradient of sum_i cot_i . a_i w.r.t. positions and masses (fixed lists)."""
+    def adjoint(self, cax, cay, caz, out=None):
+        """Gradient of sum_i cot_i . a_i w.r.t. positions and masses (fixed lists);
+        ``out`` may hold preallocated arrays "gx", "gy", "gz", "gm"."""
         c = [np.ascontiguousarray(a, dtype=np.float64) for a in (cax, cay, caz)]
-        out = [np.empty(self.n) for _ in range(4)]
-        self._check(self._lib.pt_adjoint(self._h, *[L.ptr(a) for a in c], *[L.ptr(o) for o in out]))
-        return {"gx": out[0], "gy": out[1], "gz": out[2], "gm": out[3]}
+        out = out or {k: np.empty(self.n) for k in ("gx", "gy", "gz", "gm")}
+        self._check(self._lib.pt_adjoint(self._h, *[L.ptr(a) for a in c],
+                                         *[L.ptr(out[k]) for k in ("gx", "gy", "gz", "gm")]))
+        return out
 
     def chain_grad(self, nsteps: int, dt: float, targets, ckpt_every: int = 0):
         """Loss 0.5 sum |x(T) - y|^2 after nsteps KDK steps and its gradient w.r.t.
