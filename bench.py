@@ -314,7 +314,7 @@ def main():
                 "traffic_source": TRAVERSE_MIXED_DRAM_SOURCE if traffic else None,
                 "dram_gbs": (traffic / t_trav / 1e9) if traffic else None,
                 "dram_frac_of_hbm": (traffic / t_trav / 1e9 / hbm) if traffic else None,
-                "kernel": {"mixed": "walk_lists + eval_p2c + eval_p2p", "fp64": "traverse_f64",
+                "kernel": {"mixed": "walk_lists + eval_p2c2 + eval_p2p", "fp64": "traverse_f64",
                            "fp64_lists": "walk_lists + eval_p2c_f64 + eval_p2p_f64"}[a.precision],
                 "flops_per_launch": flops,
                 "flop_model": "20 per P2P pair + 66 per P2C evaluation",

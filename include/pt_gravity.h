@@ -144,6 +144,14 @@ int pt_set_precision(pt_handle* h, int precision);
  * poll of an unpublished tile.  polls < 0 is PT_E_ARG. */
 int pt_set_sort_spin_limit(pt_handle* h, int64_t polls);
 
+/* Entries per warp region of the two-phase list pools (PT_MIXED and
+ * PT_FP64_LISTS; default 32768).  Each warp of the list walk reserves regions
+ * of this size; a bucket's list that outgrows what is left of its region
+ * moves to a new region of at least twice its length, so smaller regions move
+ * lists more often (the lists and results are the same).  A tuning and testing
+ * knob; entries < 64 is PT_E_ARG. */
+int pt_set_list_region(pt_handle* h, int64_t entries);
+
 /* Particles -------------------------------------------------------------- */
 /* Replaces Reader::load + the universe reduction (src/Reader.C:11-107,
  * src/Driver.h:96-107): copies FP64 host SoA to the device.  soft is the

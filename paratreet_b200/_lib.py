@@ -82,6 +82,7 @@ SIGNATURES = {
     "pt_set_theta": (C.c_int, [_vp, C.c_double]),
     "pt_set_precision": (C.c_int, [_vp, C.c_int]),
     "pt_set_sort_spin_limit": (C.c_int, [_vp, _i64]),
+    "pt_set_list_region": (C.c_int, [_vp, _i64]),
     "pt_set_particles": (C.c_int, [_vp, _i64] + [_vp] * 8),
     "pt_set_particles_device": (C.c_int, [_vp, _i64] + [_vp] * 8),
     "pt_num_particles": (_i64, [_vp]),

@@ -217,6 +217,11 @@ __global__ void __launch_bounds__(256) finalize_records(Nodes nd, int64_t nnodes
   w.pcount = nd.pcount[i];
   w.pad = 0;
   nd.walk[i] = w;
+  if (i >= 1) {
+    nd.walks[walk_sib_index(i, 0)] = make_double2(w.cm[0], w.cm[1]);
+    nd.walks[walk_sib_index(i, 1)] = make_double2(w.cm[2], w.orsq);
+    nd.walks[walk_sib_index(i, 2)] = make_double2(w.soft, __hiloint2double((min(w.count, 1 << 27) << 3) | w.type, w.first_child));
+  }
   QuadRec r;
   r.mass = q.mass; r.soft = q.soft;
   r.xx = q.xx; r.xy = q.xy; r.xz = q.xz; r.yy = q.yy; r.yz = q.yz; r.zz = q.zz;

@@ -7,18 +7,23 @@
 // monopole, addGravity; bit 30 = near: a target may lie inside the node's
 // softening sphere) and P2P leaf indices.  Whether a P2P leaf may hold a
 // softened pair, and how many source particles the leaves hold, are left to
-// eval_p2p, which reads every leaf record anyway: the walk is bound by its
-// instruction issue.  Each warp appends to regions it reserves from two global pools,
-// so every bucket's list is contiguous; a bucket that outgrows what is left of
-// its region moves its list so far to a new, larger region and goes on.  Only
-// a full pool sets kErrPool (the host then repeats the walk with larger
-// pools).
+// eval_p2p, which reads every leaf record anyway.  The walk reads the
+// classification fields from the sibling blocks (walk_sib_index), so the
+// eight lanes that classify one node's children load one 128-byte line per
+// field row (with the 64-byte walk records the walk was bound by the L1 data
+// pipe's wavefronts, not by arithmetic).  Each warp writes its terminals
+// straight to regions it reserves
+// from two global pools, so every bucket's list is contiguous; a bucket that
+// outgrows what is left of its region moves its list so far to a new, larger
+// region and goes on.  Only a full pool sets kErrPool (the host then repeats
+// the walk with larger pools).
 //
-// Phase B (eval_p2c, eval_p2p): one warp per bucket streams its list in
-// chunks of 64 entries and evaluates them with the packed FP32 instructions
-// (two interactions per issue slot) on offsets relative to the bucket's
-// centre of mass, as the fused kernel does, but without the walk's state in
-// registers, so more warps fit on an SM.  eval_p2c stores (or, for replica
+// Phase B (eval_p2c2 / eval_p2c, eval_p2p): one warp per bucket streams its
+// list in chunks of 64 entries and evaluates them with the packed FP32
+// instructions (two interactions per issue slot) on offsets relative to the
+// bucket's centre of mass.  Each staged node or source meets two targets per
+// packed instruction, so it is read from shared memory once for two (P2C)
+// or four (P2P) evaluations.  The P2C evaluation stores (or, for replica
 // walks after the first, adds) and eval_p2p adds.
 #include "pt_internal.cuh"
 #include "pt_walk.cuh"
@@ -52,8 +57,6 @@ constexpr int kWlBuf = 64;
 struct WalkWarp {
   BucketGeom geom;
   int32_t stack[kWlStack];
-  int32_t pcbuf[kWlBuf];  // P2C entries waiting to be written
-  int32_t ppbuf[kWlBuf];  // P2P entries waiting to be written
   PROF_FIELDS
 };
 
@@ -76,36 +79,6 @@ __device__ __forceinline__ bool ensure_region(Region& r, unsigned long long* cur
   }
   r.cur = s;
   r.end = s + region;
-  return true;
-}
-
-// Append n buffered entries to the bucket's list, which occupies [start,
-// r.cur) of the warp's region.  When they do not fit, the list so far moves to
-// a new region of at least twice its new length (the rest of the old region
-// is left unused).  False only if the pool is full.  Every lane of the warp
-// calls it with the same arguments; the list's earlier entries were written
-// before the __syncwarp that ends each walk step.
-__device__ __forceinline__ bool drain(const int32_t* buf, int n, Region& r, unsigned long long& start,
-                                      int32_t* __restrict__ pool, unsigned long long* cursor, unsigned long long cap,
-                                      unsigned region, int lane) {
-  if (n == 0) return true;
-  if (r.cur + (unsigned long long)n > r.end) {
-    const unsigned long long len = r.cur - start;
-    const unsigned long long want = max((unsigned long long)region, 2ull * (len + (unsigned long long)n));
-    unsigned long long s = 0;
-    if (lane == 0) s = atomicAdd(cursor, want);
-    s = __shfl_sync(kFull, s, 0);
-    if (s + want > cap) {
-      r.cur = r.end = cap;
-      return false;
-    }
-    for (unsigned long long k = lane; k < len; k += 32) pool[s + k] = pool[start + k];
-    start = s;
-    r.cur = s + len;
-    r.end = s + want;
-  }
-  for (int k = lane; k < n; k += 32) pool[r.cur + k] = buf[k];
-  r.cur += (unsigned long long)n;
   return true;
 }
 
@@ -146,6 +119,31 @@ __device__ __forceinline__ unsigned grab_bucket(unsigned* work, unsigned long lo
     }
   }
   return __shfl_sync(kFull, bi, 0);
+}
+
+// Room for n more entries of the bucket's list, which occupies [start,
+// r.cur) of the warp's region: when they do not fit, the list so far moves to
+// a new region of at least twice its new length.  False only if the pool is
+// full.  Warp-uniform; the list's entries were written before the __syncwarp
+// that ends each walk step.
+__device__ __forceinline__ bool make_room(int n, Region& r, unsigned long long& start, int32_t* __restrict__ pool,
+                                          unsigned long long* cursor, unsigned long long cap, unsigned region,
+                                          int lane) {
+  if (r.cur + (unsigned long long)n <= r.end) return true;
+  const unsigned long long len = r.cur - start;
+  const unsigned long long want = max((unsigned long long)region, 2ull * (len + (unsigned long long)n));
+  unsigned long long s = 0;
+  if (lane == 0) s = atomicAdd(cursor, want);
+  s = __shfl_sync(kFull, s, 0);
+  if (s + want > cap) {
+    r.cur = r.end = cap;
+    return false;
+  }
+  for (unsigned long long k = lane; k < len; k += 32) pool[s + k] = pool[start + k];
+  start = s;
+  r.cur = s + len;
+  r.end = s + want;
+  return true;
 }
 
 // CTAs per SM of the walk (72 registers); 6 and 8 measured slower at N = 2^24
@@ -195,7 +193,7 @@ __global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravPa
     const int ntot = P.walk[tnode].pcount;
     unsigned long long pc0 = rpc.cur, pp0 = rpp.cur;  // the bucket's lists start here (moved on overflow)
     unsigned long long opens = 0;
-    int sp = 0, nc = 0, np = 0;
+    int sp = 0;
     int nexp = 1, pop = -1;
     bool ok = true, fits = true;
     PROF_MARK(w, 0);
@@ -214,7 +212,21 @@ __global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravPa
         if (node >= P.nnodes) {
           atomicOr(P.status, kErrCapacity);
         } else {
-          r = P.walk[node];
+          if (node == 0) {
+            r = P.walk[0];
+          } else {  // the classification fields from the sibling blocks (3 lines per 8 lanes)
+            const double2* sb = P.walks + walk_sib_index(node, 0);
+            const double2 v0 = sb[0], v1 = sb[8], v2 = sb[16];
+            r.cm[0] = v0.x;
+            r.cm[1] = v0.y;
+            r.cm[2] = v1.x;
+            r.orsq = v1.y;
+            r.soft = v2.x;
+            const int tc = __double2hiint(v2.y);
+            r.first_child = __double2loint(v2.y);
+            r.type = tc & 7;
+            r.count = tc >> 3;
+          }
           if (kOffset) cls = classify_node_gap(r, blo, bhi, g, P.ox, P.oy, P.oz, gap2);
           else cls = classify_node_gap_nooff(r, blo, bhi, g, gap2);
         }
@@ -230,19 +242,26 @@ __global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravPa
         near = !(gap2 > reach * reach);
       }
       PROF_MARK(w, 1);
-      {
+      {  // terminals go straight to the bucket's lists
+        const unsigned lt = (1u << lane) - 1u;
         const bool pc = (cls == kClsQuad || cls == kClsMono);
         const unsigned m = __ballot_sync(kFull, pc);
-        if (pc)
-          w.pcbuf[nc + __popc(m & ((1u << lane) - 1u))] =
-              node | (cls == kClsMono ? (int)0x80000000 : 0) | (near ? 0x40000000 : 0);
-        nc += __popc(m);
-      }
-      {
+        const int n = __popc(m);
+        if (n && fits) {
+          fits = make_room(n, rpc, pc0, L.pc_pool, L.cursor + 0, L.cap_pc, L.region, lane);
+          if (fits && pc)
+            L.pc_pool[rpc.cur + __popc(m & lt)] =
+                node | (cls == kClsMono ? (int)0x80000000 : 0) | (near ? 0x40000000 : 0);
+          if (fits) rpc.cur += (unsigned long long)n;
+        }
         const bool pp = (cls == kClsP2P);
-        const unsigned m = __ballot_sync(kFull, pp);
-        if (pp) w.ppbuf[np + __popc(m & ((1u << lane) - 1u))] = node;
-        np += __popc(m);
+        const unsigned mp = __ballot_sync(kFull, pp);
+        const int npp = __popc(mp);
+        if (npp && fits) {
+          fits = make_room(npp, rpp, pp0, L.pp_pool, L.cursor + 1, L.cap_pp, L.region, lane);
+          if (fits && pp) L.pp_pool[rpp.cur + __popc(mp & lt)] = node;
+          if (fits) rpp.cur += (unsigned long long)npp;
+        }
       }
       {
         const bool op = (cls == kClsOpen);
@@ -256,18 +275,7 @@ __global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravPa
       }
       __syncwarp();
       PROF_MARK(w, 2);
-      const bool last = (sp == 0);
-      if (nc >= 32 || last) {
-        fits = fits && drain(w.pcbuf, nc, rpc, pc0, L.pc_pool, L.cursor + 0, L.cap_pc, L.region, lane);
-        nc = 0;
-      }
-      if (np >= 32 || last) {
-        fits = fits && drain(w.ppbuf, np, rpp, pp0, L.pp_pool, L.cursor + 1, L.cap_pp, L.region, lane);
-        np = 0;
-      }
-      __syncwarp();
-      PROF_MARK(w, 3);
-      if (last) break;
+      if (sp == 0) break;
       nexp = sp < 4 ? sp : 4;
       sp -= nexp;
       pop = sp;
@@ -730,6 +738,232 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams
   PROF_FLUSH(w, 0);
 }
 
+// eval_p2c with two targets per lane: each staged node meets the lane's two
+// targets in one packed instruction, so a node is read from shared memory
+// once for two evaluations.  The chunk's nodes are staged one per entry:
+// na = (offset x, y, z, mass), nq = traceless (xx, xy, xz, yy), nr =
+// traceless (yz, zz): 40 bytes per node instead of 40 bytes per evaluation.
+struct EvalWarpC2 {
+  BucketGeom geom;
+  float4 na[64];
+  float4 nq[64];
+  float2 nr[64];
+  float4 ks[4][32];  // compensated sums: target 1 (sum, compensation), target 2 (sum, compensation)
+  int32_t spec[kWlBuf];
+  PROF_FIELDS
+};
+
+// The chunk's nodes k = grp, grp + G, ... < nn against the lane's two
+// targets (halves of every packed value); the same terms as ev_p2c_pairs.
+__device__ __forceinline__ void ev_p2c_nodes2(const EvalWarpC2& w, const EvTarget2& x, int nn, float2 ntx,
+                                              float2 nty, float2 ntz, float2& ax2, float2& ay2, float2& az2,
+                                              float2& pp2, float2& mm2) {
+  const float2 mthree = make_float2(-3.f, -3.f), m25 = make_float2(-2.5f, -2.5f), half = make_float2(0.5f, 0.5f);
+  for (int k = x.grp; k < nn; k += x.G) {
+    const float4 A = w.na[k];
+    const float2 rx = __fadd2_rn(make_float2(A.x, A.x), ntx);  // r' = o - t = -r
+    const float2 ry = __fadd2_rn(make_float2(A.y, A.y), nty);
+    const float2 rz = __fadd2_rn(make_float2(A.z, A.z), ntz);
+    float2 r2 = __fmul2_rn(rx, rx);
+    r2 = __ffma2_rn(ry, ry, r2);
+    r2 = __ffma2_rn(rz, rz, r2);
+    const float4 Q = w.nq[k];
+    const float2 Q2 = w.nr[k];
+    const float2 a = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+    const float2 d2 = __fmul2_rn(a, a);
+    const float2 bb = __fmul2_rn(a, d2);
+    const float2 nc = __fmul2_rn(__fmul2_rn(bb, d2), mthree);
+    const float2 xx = make_float2(Q.x, Q.x), xy = make_float2(Q.y, Q.y), xz = make_float2(Q.z, Q.z);
+    const float2 yy = make_float2(Q.w, Q.w), yz = make_float2(Q2.x, Q2.x), zz = make_float2(Q2.y, Q2.y);
+    const float2 qx = __ffma2_rn(xz, rz, __ffma2_rn(xy, ry, __fmul2_rn(xx, rx)));
+    const float2 qy = __ffma2_rn(yz, rz, __ffma2_rn(yy, ry, __fmul2_rn(xy, rx)));
+    const float2 qz = __ffma2_rn(zz, rz, __ffma2_rn(yz, ry, __fmul2_rn(xz, rx)));
+    const float2 cq = __fmul2_rn(nc, __ffma2_rn(qz, rz, __ffma2_rn(qy, ry, __fmul2_rn(qx, rx))));
+    const float2 M = make_float2(A.w, A.w);
+    const float2 AA = __ffma2_rn(__fmul2_rn(d2, m25), cq, __fmul2_rn(bb, M));
+    ax2 = __ffma2_rn(nc, qx, __ffma2_rn(AA, rx, ax2));
+    ay2 = __ffma2_rn(nc, qy, __ffma2_rn(AA, ry, ay2));
+    az2 = __ffma2_rn(nc, qz, __ffma2_rn(AA, rz, az2));
+    pp2 = __ffma2_rn(half, cq, pp2);
+    mm2 = __ffma2_rn(M, a, mm2);
+  }
+}
+
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c2(TravParams P, ListParams L,
+                                                                      const Mom* __restrict__ mom) {
+  __shared__ EvalWarpC2 warps[kEvWarps];
+  EvalWarpC2& w = warps[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const float kPad = 1.0e10f;
+  const float qnan = __int_as_float(0x7fc00000);
+  int64_t b;
+  int tnode;
+  PROF_START(w);
+  while (next_bucket(P, lane, b, tnode)) {
+    if (tnode < 0 || tnode >= P.nnodes) continue;
+    const int64_t lb = b - P.b_begin;
+    const int64_t start = L.pc_start[lb];
+    const int count = L.pc_count[lb];
+    if (count == 0 && P.accumulate) continue;  // nothing to add (the first walk stores, even zeros)
+    __syncwarp();
+    if (lane == 0) load_bucket_geom(mom, tnode, w.geom);
+    __syncwarp();
+    const int tbase = P.walk[tnode].pstart, ntot = P.walk[tnode].pcount;
+    for (int tc = 0; tc < ntot; tc += 32) {
+      const int t0 = tbase + tc, nt = min(32, ntot - tc);
+      const EvTarget2 x = ev_target2(P.p, w.geom, t0, nt, lane);
+      const bool two = x.t2 < nt;  // the lane has a second target
+      const float2 ntx = make_float2(-x.tx.x, -x.tx.y), nty = make_float2(-x.ty.x, -x.ty.y),
+                   ntz = make_float2(-x.tz.x, -x.tz.y);
+#pragma unroll
+      for (int r = 0; r < 4; r++) w.ks[r][lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+      float2 ax2 = make_float2(0.f, 0.f), ay2 = ax2, az2 = ax2, pp2 = ax2, mm2 = ax2;
+      float2 pmono = make_float2(0.f, 0.f);  // the monopole nodes' potential (left out of pot)
+      int en0 = (2 * lane < count) ? L.pc_pool[start + 2 * lane] : 0;
+      int en1 = (2 * lane + 1 < count) ? L.pc_pool[start + 2 * lane + 1] : 0;
+      PROF_MARK(w, 0);
+      for (int cs = 0; cs < count; cs += 64) {
+        const int ec[2] = {en0, en1};
+        if (cs + 64 < count) {
+          const int qn = cs + 64 + 2 * lane;
+          en0 = (qn < count) ? L.pc_pool[start + qn] : 0;
+          en1 = (qn + 1 < count) ? L.pc_pool[start + qn + 1] : 0;
+        }
+        float4 o[2], r0[2], r1[2];
+        bool spec[2] = {false, false};
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int q = cs + 2 * lane + h;
+          o[h] = make_float4(kPad, kPad, kPad, 0.f);
+          r0[h] = make_float4(0.f, 0.f, 0.f, 0.f);
+          r1[h] = r0[h];
+          if (q < count) {
+            const int e = ec[h];
+            spec[h] = (e & 0xc0000000) != 0;
+            if (!spec[h]) {
+              const int node = e & 0x3fffffff;
+              const float4* rec = reinterpret_cast<const float4*>(P.quadf + node);
+              o[h] = node_offset(P.walk, node, P, w.geom);
+              r0[h] = rec[0];  // mass, soft, xx, xy
+              r1[h] = rec[1];  // xz, yy, yz, zz
+            }
+          }
+        }
+        const unsigned m0 = __ballot_sync(kFull, spec[0]), m1 = __ballot_sync(kFull, spec[1]);
+        const int ns = __popc(m0) + __popc(m1);
+        __syncwarp();
+        if (spec[0] || spec[1]) {  // chunk order: by lane, then h
+          const unsigned lt = (1u << lane) - 1u;
+          const int at = __popc(m0 & lt) + __popc(m1 & lt);
+          if (spec[0]) w.spec[at] = ec[0];
+          if (spec[1]) w.spec[at + (spec[0] ? 1 : 0)] = ec[1];
+        }
+#pragma unroll
+        for (int h = 0; h < 2; h++) {  // traceless moments: xx, yy, zz less a third of the trace
+          const float t3 = (r0[h].z + r1[h].y + r1[h].w) * (1.0f / 3.0f);
+          w.na[2 * lane + h] = make_float4(o[h].x, o[h].y, o[h].z, r0[h].x);
+          w.nq[2 * lane + h] = make_float4(r0[h].z - t3, r0[h].w, r1[h].x, r1[h].y - t3);
+          w.nr[2 * lane + h] = make_float2(r1[h].z, r1[h].w - t3);
+        }
+        __syncwarp();
+        const int nn = min(64, count - cs);
+        PROF_MARK(w, 1);
+        if (x.grp < x.G) {
+          ev_p2c_nodes2(w, x, nn, ntx, nty, ntz, ax2, ay2, az2, pp2, mm2);
+          PROF_MARK(w, 2);
+          for (int j = x.grp; j < ns; j += x.G) {  // near and monopole nodes, scalar
+            const int e = w.spec[j];
+            const int node = e & 0x3fffffff;
+            const float4 of = node_offset(P.walk, node, P, w.geom);
+            const float4* rec = reinterpret_cast<const float4*>(P.quadf + node);
+            const float4 q0r = rec[0], q1r = rec[1];
+            const bool mono = e < 0;
+            const float4 q0 = mono ? make_float4(0.f, 0.f, 0.f, 0.f) : make_float4(q0r.z, q0r.w, q1r.x, q1r.y);
+            const float2 q1 = mono ? make_float2(0.f, 0.f) : make_float2(q1r.z, q1r.w);
+            const float sf = mono ? qnan : q0r.y;
+            const P2cTerm t = ev_p2c_scalar(of.x, of.y, of.z, q0r.x, sf, q0, q1, x.tx.x, x.ty.x, x.tz.x, x.ts.x);
+            ax2.x += t.ax;
+            ay2.x += t.ay;
+            az2.x += t.az;
+            pp2.x += t.pf;
+            if (mono) pmono.x += t.pf;
+            if (two) {
+              const P2cTerm u = ev_p2c_scalar(of.x, of.y, of.z, q0r.x, sf, q0, q1, x.tx.y, x.ty.y, x.tz.y, x.ts.y);
+              ax2.y += u.ax;
+              ay2.y += u.ay;
+              az2.y += u.az;
+              pp2.y += u.pf;
+              if (mono) pmono.y += u.pf;
+            }
+          }
+          PROF_MARK(w, 3);
+        }
+        if (((cs >> 6) & 3) == 3 || cs + 64 >= count) {
+          float4 s1 = w.ks[0][lane], c1 = w.ks[1][lane], s2 = w.ks[2][lane], c2 = w.ks[3][lane];
+          kahan_add(s1.x, c1.x, ax2.x);
+          kahan_add(s1.y, c1.y, ay2.x);
+          kahan_add(s1.z, c1.z, az2.x);
+          kahan_add(s1.w, c1.w, pp2.x - mm2.x);
+          kahan_add(s2.x, c2.x, ax2.y);
+          kahan_add(s2.y, c2.y, ay2.y);
+          kahan_add(s2.z, c2.z, az2.y);
+          kahan_add(s2.w, c2.w, pp2.y - mm2.y);
+          w.ks[0][lane] = s1;
+          w.ks[1][lane] = c1;
+          w.ks[2][lane] = s2;
+          w.ks[3][lane] = c2;
+          ax2 = ay2 = az2 = pp2 = mm2 = make_float2(0.f, 0.f);
+        }
+      }
+      // per target slot (group, target): ax, ay, az, pot_full, monopole part
+      double* red = reinterpret_cast<double*>(&w.na[0]);  // na, nq, nr: 2560 bytes = 64 slots x 5
+      const float4 s1 = w.ks[0][lane], c1 = w.ks[1][lane], s2 = w.ks[2][lane], c2 = w.ks[3][lane];
+      __syncwarp();
+      if (x.grp < x.G) {
+        double* r1 = red + 5 * (x.grp * nt + x.t1);
+        r1[0] = (double)s1.x - (double)c1.x;
+        r1[1] = (double)s1.y - (double)c1.y;
+        r1[2] = (double)s1.z - (double)c1.z;
+        r1[3] = (double)s1.w - (double)c1.w;
+        r1[4] = (double)pmono.x;
+        if (two) {
+          double* r2 = red + 5 * (x.grp * nt + x.t2);
+          r2[0] = (double)s2.x - (double)c2.x;
+          r2[1] = (double)s2.y - (double)c2.y;
+          r2[2] = (double)s2.z - (double)c2.z;
+          r2[3] = (double)s2.w - (double)c2.w;
+          r2[4] = (double)pmono.y;
+        }
+      }
+      __syncwarp();
+      if (lane < nt) {
+        double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int gg = 0; gg < x.G; gg++)
+          for (int k = 0; k < 5; k++) v[k] += red[5 * (gg * nt + lane) + k];
+        const int i = t0 + lane;
+        if (P.accumulate == 0) {
+          P.p.ax[i] = v[0];
+          P.p.ay[i] = v[1];
+          P.p.az[i] = v[2];
+          P.p.pot[i] = v[3] - v[4];
+          P.p.potf[i] = v[3];
+        } else {
+          P.p.ax[i] += v[0];
+          P.p.ay[i] += v[1];
+          P.p.az[i] += v[2];
+          P.p.pot[i] += v[3] - v[4];
+          P.p.potf[i] += v[3];
+        }
+      }
+      __syncwarp();  // red is the next chunk's staging area
+      PROF_MARK(w, 4);
+    }
+  }
+  PROF_MARK(w, 5);
+  PROF_FLUSH(w, 0);
+}
+
 // One source of a near leaf: Newtonian beyond the softening reach, the spline
 // inside it, nothing for the particle itself (r2 == 0).  pp sums +m a.
 __device__ __forceinline__ void ev_near_source(float m, float dx, float dy, float dz, float r2, float reach2,
@@ -753,6 +987,24 @@ __device__ __forceinline__ void ev_near_source(float m, float dx, float dy, floa
     pp += m * a;
   }
 }
+
+// Leaf of chunk positions 2 lane and 2 lane + 1 (chunk start cs): the leaf
+// covering position cs plus the leaves that start in (cs, q] -- one bit per
+// start position, OR-reduced over the warp, counted with popc.  preA / preB =
+// stream position of the lane's leaves lane and lane + 32.  Warp-uniform.
+__device__ __forceinline__ void chunk_leaves(int cs, int preA, int preB, int lane, int& lo, int& lo1) {
+  unsigned long long bits = 0ull;
+  const int pa = preA - cs, pb = preB - cs;
+  if (pa > 0 && pa < 64) bits |= 1ull << pa;
+  if (pb > 0 && pb < 64) bits |= 1ull << pb;
+  const unsigned long long starts =
+      ((unsigned long long)__reduce_or_sync(kFull, (unsigned)(bits >> 32)) << 32) |
+      __reduce_or_sync(kFull, (unsigned)bits);
+  const int b0 = __popc(__ballot_sync(kFull, preA <= cs)) + __popc(__ballot_sync(kFull, preB <= cs)) - 1;
+  lo = b0 + __popcll(starts & ((2ull << (2 * lane)) - 1ull));
+  lo1 = lo + (int)((starts >> (2 * lane + 1)) & 1ull);
+}
+
 
 // P2P of the selected leaves w.lsel[0..nleaves) (GravityVisitor::leaf,
 // examples/GravityVisitor.h:144-160, in FP32): their sources are staged 64
@@ -812,19 +1064,8 @@ __device__ __forceinline__ void ev_p2p_leaves(EvalWarp& w, int nleaves, const Tr
   for (int cs = 0; cs < total; cs += 64) {
     {  // stage this lane's two sources
       const int q0 = cs + 2 * lane;
-      // leaf of chunk positions 2 lane and 2 lane + 1: the leaf covering
-      // position cs plus the leaves that start in (cs, q] -- one bit per start
-      // position, OR-reduced over the warp, counted with popc
-      unsigned long long bits = 0ull;
-      const int pa = preA - cs, pb = preB - cs;
-      if (pa > 0 && pa < 64) bits |= 1ull << pa;
-      if (pb > 0 && pb < 64) bits |= 1ull << pb;
-      const unsigned long long starts =
-          ((unsigned long long)__reduce_or_sync(kFull, (unsigned)(bits >> 32)) << 32) |
-          __reduce_or_sync(kFull, (unsigned)bits);
-      const int b0 = __popc(__ballot_sync(kFull, preA <= cs)) + __popc(__ballot_sync(kFull, preB <= cs)) - 1;
-      const int lo = b0 + __popcll(starts & ((2ull << (2 * lane)) - 1ull));
-      const int lo1 = lo + (int)((starts >> (2 * lane + 1)) & 1ull);
+      int lo, lo1;
+      chunk_leaves(cs, preA, preB, lane, lo, lo1);
       float4 ra = make_float4(kPadPos, kPadPos, kPadPos, 0.f), rb = ra;
       float4 oa = make_float4(0.f, 0.f, 0.f, 0.f), ob = oa;
       float sa = 0.f, sb = 0.f;
@@ -1063,7 +1304,13 @@ void launch_eval_lists(const TravParams& P, const ListParams& L, const Mom* mom,
   Q.work = work2;
   if (P.smq) Q.smq = P.smq + 256;  // P2P's queues follow P2C's
   note_launch();
-  eval_p2c<PT_P2C_MINB><<<grid, kEvWarps * 32, 0, st>>>(P, L, mom);
+  // the replica walks after the first (periodic passes) leave short P2C
+  // lists, where the one-target kernel's smaller per-bucket work measured
+  // faster (256^3 lattice pass 212 against 220 ms); the first walk and every
+  // non-periodic pass take the two-target kernel (Plummer N = 2^24: 3.5 ms
+  // faster)
+  if (P.accumulate) eval_p2c<PT_P2C_MINB><<<grid, kEvWarps * 32, 0, st>>>(P, L, mom);
+  else eval_p2c2<PT_P2C_MINB><<<grid, kEvWarps * 32, 0, st>>>(P, L, mom);
   note_launch();
   eval_p2p<PT_P2P_MINB><<<grid, kEvWarps * 32, 0, st>>>(Q, L, mom);
 }

@@ -212,6 +212,7 @@ int grow_nodes(pt_handle* h, int64_t need) {
   CKR(dalloc(h, &nn.count, nc));
   CKR(dalloc(h, &nn.mom, nc));
   CKR(dalloc(h, &nn.walk, nc));
+  CKR(dalloc(h, &nn.walks, walk_sib_size(nc)));
   CKR(dalloc(h, &nn.quad, nc));
   CKR(dalloc(h, &nn.quadf, nc));
   CKR(dalloc(h, &nn.fifo, nc));
@@ -233,7 +234,7 @@ int grow_nodes(pt_handle* h, int64_t need) {
     CK(cudaStreamSynchronize(st));
   }
   dfree(o.key); dfree(o.type); dfree(o.depth); dfree(o.pstart); dfree(o.pcount); dfree(o.parent);
-  dfree(o.first_child); dfree(o.count); dfree(o.mom); dfree(o.walk); dfree(o.quad); dfree(o.quadf);
+  dfree(o.first_child); dfree(o.count); dfree(o.mom); dfree(o.walk); dfree(o.walks); dfree(o.quad); dfree(o.quadf);
   dfree(o.fifo); dfree(o.nleaf_sub); dfree(o.nempty_sub); dfree(o.leaf_base); dfree(o.empty_base);
   h->nd = nn;
   // flags holds the current level's child ranks while the build is running:
@@ -618,6 +619,7 @@ int traverse(pt_handle* h, int64_t b0, int64_t b1) {
   TravParams P{};
   P.p = h->p;
   P.walk = h->nd.walk;
+  P.walks = h->nd.walks;
   P.quad = h->nd.quad;
   P.quadf = h->nd.quadf;
   P.srcf = h->srcf;
@@ -869,7 +871,7 @@ int pt_destroy(pt_handle* h) {
   dfree(h->d_status); dfree(h->d_counters); dfree(h->d_work); dfree(h->d_vmax2); dfree(h->srcf); dfree(h->softf);
   Nodes& o = h->nd;
   dfree(o.key); dfree(o.type); dfree(o.depth); dfree(o.pstart); dfree(o.pcount); dfree(o.parent);
-  dfree(o.first_child); dfree(o.count); dfree(o.mom); dfree(o.walk); dfree(o.quad); dfree(o.quadf);
+  dfree(o.first_child); dfree(o.count); dfree(o.mom); dfree(o.walk); dfree(o.walks); dfree(o.quad); dfree(o.quadf);
   dfree(o.fifo); dfree(o.nleaf_sub); dfree(o.nempty_sub); dfree(o.leaf_base); dfree(o.empty_base);
   dfree(h->flags); dfree(h->buckets); dfree(h->bucket_work); dfree(h->list_count); dfree(h->list_off); dfree(h->list_node);
   dfree(h->list_kind); dfree(h->dsum); dfree(h->adj); dfree(h->nadj); dfree(h->d_htab); dfree(h->ewd); dfree(h->sph); dfree(h->sph_nbr); dfree(h->sph_nd2);
@@ -906,6 +908,12 @@ int pt_set_precision(pt_handle* h, int precision) {
 int pt_set_sort_spin_limit(pt_handle* h, int64_t polls) {
   if (!h || polls < 0) return PT_E_ARG;
   h->sort_spin_limit = (long long)polls;
+  return PT_OK;
+}
+
+int pt_set_list_region(pt_handle* h, int64_t entries) {
+  if (!h || entries < 64 || entries > (1 << 30)) return PT_E_ARG;
+  h->l_region = (unsigned)entries;
   return PT_OK;
 }
 
@@ -1572,6 +1580,7 @@ int pt_forces_frozen(pt_handle* h, const double* x, const double* y, const doubl
   TravParams P{};
   P.p = h->p;
   P.walk = h->nd.walk;
+  P.walks = h->nd.walks;
   P.quad = h->nd.quad;
   P.buckets = h->buckets;
   P.b_begin = 0;

@@ -58,6 +58,18 @@ struct __align__(16) WalkRec {
   int32_t pcount;       // particles in the node's key range
   int32_t pad;
 };
+
+// Sibling blocks: the 8 children of an internal node are contiguous and start
+// at 1 + 8k (the build allocates every level in groups of 8 after the root),
+// so group k of nodes 1 + 8k .. 8 + 8k is stored as 3 rows of 8 x 16 bytes:
+// row 0 (cm.x, cm.y), row 1 (cm.z, orsq | reach), row 2 (soft | soft_max,
+// first_child and type | count << 3 as one 8-byte word).  Eight lanes that
+// classify the children of one node read each row as one 128-byte line
+// instead of eight 64-byte records.  Node 0 (the root) has no block.
+__host__ __device__ __forceinline__ int64_t walk_sib_index(int64_t node, int row) {
+  return ((node - 1) >> 3) * 24 + row * 8 + ((node - 1) & 7);
+}
+__host__ __device__ __forceinline__ int64_t walk_sib_size(int64_t nodes) { return ((nodes + 7) >> 3) * 24 + 24; }
 static_assert(sizeof(WalkRec) == 64, "WalkRec is one 64-byte record");
 
 // Per-node P2C record (FP64): mass, soft and the 6 second moments.
@@ -92,6 +104,7 @@ struct Nodes {
   int32_t* count;       // CentroidData::count
   Mom* mom;
   WalkRec* walk;
+  double2* walks;       // sibling-block copy of walk's classification fields (walk_sib_index)
   QuadRec* quad;
   QuadRecF* quadf;
   uint64_t* fifo;       // upward-pass FIFO position key (depth-of-chain << 40 | rank)
@@ -104,6 +117,7 @@ struct Nodes {
 struct TravParams {
   Particles p;
   const WalkRec* walk;
+  const double2* walks;   // sibling blocks of walk (list walk)
   const QuadRec* quad;
   const QuadRecF* quadf;
   const float4* srcf;     // mixed: per-particle (x,y,z) relative to its leaf's cm, mass

@@ -152,6 +152,11 @@ class GravitySimulation:
         makes on an unpublished tile before the pass gives up with an error."""
         self._check(self._lib.pt_set_sort_spin_limit(self._h, int(polls)))
 
+    def set_list_region(self, entries: int = 32768):
+        """Entries per warp region of the two-phase list pools (tuning and
+        tests: smaller regions move the buckets' lists more often)."""
+        self._check(self._lib.pt_set_list_region(self._h, int(entries)))
+
     # -- particles ----------------------------------------------------------
     def set_particles(self, p: dict):
         arrs = [np.ascontiguousarray(p[k], dtype=np.float64) for k in _FIELDS]

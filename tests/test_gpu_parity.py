@@ -190,6 +190,31 @@ def test_mixed_matches_fp64_full_size():
     assert np.sqrt(np.mean(e ** 2)) < 1e-5
 
 
+@pytest.mark.parametrize("prec", ["mixed", "fp64_lists"])
+def test_list_relocation_keeps_lists(prec):
+    """Warp regions of 64 entries instead of 32768: nearly every bucket's list
+    outgrows what is left of its region and moves while the walk writes it.
+    The lists (order-independent digests and lengths), the counts and the
+    accelerations and potentials are the same bit for bit."""
+    p = ics.plummer(200000, seed=21, soft=1e-3)
+    res = []
+    for region in (32768, 64):
+        with sim(max_particles_per_leaf=32, theta=0.5, precision=prec) as s:
+            s.set_list_region(region)
+            s.set_particles(p)
+            s.start_down()
+            s.start_down()
+            res.append((s.accelerations(), s.counters(), s.list_digests("two_phase")))
+    (a, c, d), (b, cb, db) = res
+    assert (c["n_pp"], c["n_pc"], c["n_open"]) == (cb["n_pp"], cb["n_pc"], cb["n_open"])
+    assert np.array_equal(d[1], db[1]) and np.array_equal(d[0], db[0])
+    for k in ("ax", "ay", "az", "pot", "pot_full"):
+        assert np.array_equal(a[k], b[k]), k
+    with sim() as s:
+        with pytest.raises(Exception):
+            s.set_list_region(63)
+
+
 @pytest.mark.parametrize("gen,n,bucket,soft,theta", [("plummer", 200000, 32, 1e-3, 0.7),
                                                       ("mixture", 150000, 16, 1e-4, 0.7),
                                                       ("hernquist", 50000, 16, 0.05, 0.5)])
