@@ -31,6 +31,20 @@ namespace pt {
 constexpr int kAdjWarps = 4;
 constexpr unsigned kAdjFull = 0xffffffffu;
 
+// Phase timers of a diagnostic build (PT_PROF=1), summed per phase into
+// g_prof_adj: P2C windows, P2P windows, the target-side sums.
+#ifndef PT_PROF
+#define PT_PROF 0
+#endif
+#if PT_PROF
+__device__ unsigned long long g_prof_adj[8];
+#define ADJ_T0 unsigned t_prev_ = (unsigned)clock();
+#define ADJ_MARK(i) if (lane == 0) { const unsigned t_ = (unsigned)clock(); atomicAdd(&g_prof_adj[i], (unsigned long long)(t_ - t_prev_)); t_prev_ = t_; }
+#else
+#define ADJ_T0
+#define ADJ_MARK(i)
+#endif
+
 
 __device__ __forceinline__ double wsum(double v) {
 #pragma unroll
@@ -78,38 +92,48 @@ struct AdjWarp {
   int32_t lincl[32];   // P2P: inclusive prefix of their particle counts
 };
 
-struct AdjTarget {
-  int t, grp, G, nt;
-  bool act;
+#ifndef PT_ADJ_TWO
+#define PT_ADJ_TWO 0
+#endif
+
+// One target of a lane: position, softening and cotangent.
+struct AdjTgt {
   double x, y, z, s, ax, ay, az;
 };
 
-// One P2C pair (target, staged node k): target-side Jacobian term j (added to
-// the target's registers) and the ten node-side terms (added to row k).
-__device__ __forceinline__ void adj_p2c_pair(AdjWarp& w, int k, const AdjTarget& x, double& gx, double& gy,
-                                             double& gz, unsigned* status) {
+// The lane's targets: with two targets per lane (PT_ADJ_TWO), lane l of
+// group l / h holds targets 2 (l mod h) and 2 (l mod h) + 1 (h = ceil(n_t / 2),
+// t2 == n_t when there is none), so every staged slot is read, and its row
+// updated, once for two pairs; otherwise h = n_t and t2 == n_t.
+struct AdjTarget {
+  int t1, t2, tl, h, grp, G, nt;
+  bool act, two;
+  AdjTgt a, b;
+};
+
+// P2C terms of one (target, staged node k) pair: the target-side Jacobian
+// term j (returned in jx, jy, jz) and the ten node-side terms added to c.
+// False for the softened quadrupole branch (reported, not differentiated).
+__device__ __forceinline__ bool adj_p2c_terms(const AdjWarp& w, int k, const AdjTgt& x, double& jx, double& jy,
+                                              double& jz, double c[10], unsigned* status) {
   const double rx = x.x - w.st[0][k], ry = x.y - w.st[1][k], rz = x.z - w.st[2][k];
   const double M = w.st[3][k];
   const double r2 = rx * rx + ry * ry + rz * rz;
   const double ir = rsqrt(r2);
   const double ir2 = ir * ir;
   const double ra = rx * x.ax + ry * x.ay + rz * x.az;
-  double c[10];
-  double jx, jy, jz;
   if (w.st[10][k] == 2.0) {  // monopole: f = -M r / r^3
     const double b3 = ir2 * ir;
     const double t = 3.0 * b3 * ir2 * ra;
     jx = -M * (b3 * x.ax - t * rx);
     jy = -M * (b3 * x.ay - t * ry);
     jz = -M * (b3 * x.az - t * rz);
-#pragma unroll
-    for (int q = 4; q < 10; q++) c[q] = 0.0;
-    c[3] = -b3 * ra;
+    c[3] += -b3 * ra;
   } else {
     const double twoh = w.st[11][k] + x.s;
     if (r2 < twoh * twoh) {  // the softened quadrupole branch: reported, not differentiated
       atomicOr(status, kErrAdjointSoftened);
-      return;
+      return false;
     }
     const double xx = w.st[4][k], xy = w.st[5][k], xz = w.st[6][k];
     const double yy = w.st[7][k], yz = w.st[8][k], zz = w.st[9][k];
@@ -128,30 +152,26 @@ __device__ __forceinline__ void adj_p2c_pair(AdjWarp& w, int k, const AdjTarget&
     jx = -s * x.ax + k1 * rx + cc * qax - dd * ra * qx;
     jy = -s * x.ay + k1 * ry + cc * qay - dd * ra * qy;
     jz = -s * x.az + k1 * rz + cc * qaz - dd * ra * qz;
-    c[3] = -bb * ra;
+    c[3] += -bb * ra;
     const double h = -dd * ra;
-    c[4] = h * 0.5 * rx * rx + cc * ra * 0.5 + cc * x.ax * rx;
-    c[5] = h * 0.5 * ry * ry + cc * ra * 0.5 + cc * x.ay * ry;
-    c[6] = h * 0.5 * rz * rz + cc * ra * 0.5 + cc * x.az * rz;
-    c[7] = h * rx * ry + cc * (x.ax * ry + x.ay * rx);
-    c[8] = h * rx * rz + cc * (x.ax * rz + x.az * rx);
-    c[9] = h * ry * rz + cc * (x.ay * rz + x.az * ry);
+    c[4] += h * 0.5 * rx * rx + cc * ra * 0.5 + cc * x.ax * rx;
+    c[5] += h * 0.5 * ry * ry + cc * ra * 0.5 + cc * x.ay * ry;
+    c[6] += h * 0.5 * rz * rz + cc * ra * 0.5 + cc * x.az * rz;
+    c[7] += h * rx * ry + cc * (x.ax * ry + x.ay * rx);
+    c[8] += h * rx * rz + cc * (x.ax * rz + x.az * rx);
+    c[9] += h * ry * rz + cc * (x.ay * rz + x.az * ry);
   }
-  gx += jx;
-  gy += jy;
-  gz += jz;
-  c[0] = -jx;
-  c[1] = -jy;
-  c[2] = -jz;
-#pragma unroll
-  for (int q = 0; q < 10; q++) w.acc[q][k] += c[q];
+  c[0] -= jx;
+  c[1] -= jy;
+  c[2] -= jz;
+  return true;
 }
 
-// One P2P pair (target, staged source k): T = b I + (b'/r) d d^T with
-// d = x_k - x_i; the target gets -m_k T abar_i, the source +m_k T abar_i and
-// mbar_k += b d.abar_i.
-__device__ __forceinline__ void adj_p2p_pair(AdjWarp& w, int k, const AdjTarget& x, double& gx, double& gy,
-                                             double& gz) {
+// P2P terms of one (target, staged source k) pair: T = b I + (b'/r) d d^T
+// with d = x_k - x_i; the target gets -m_k T abar_i (returned as s), the
+// source +m_k T abar_i and mbar_k += b d.abar_i (added to c[0..3]).
+__device__ __forceinline__ void adj_p2p_terms(const AdjWarp& w, int k, const AdjTgt& x, double& gx, double& gy,
+                                              double& gz, double c[4]) {
   const double dx = w.st[0][k] - x.x, dy = w.st[1][k] - x.y, dz = w.st[2][k] - x.z;
   const double r2 = dx * dx + dy * dy + dz * dz;
   if (r2 == 0.0) return;
@@ -165,35 +185,66 @@ __device__ __forceinline__ void adj_p2p_pair(AdjWarp& w, int k, const AdjTarget&
   gx -= sx;
   gy -= sy;
   gz -= sz;
-  w.acc[0][k] += sx;
-  w.acc[1][k] += sy;
-  w.acc[2][k] += sz;
-  w.acc[3][k] += bb * da;
+  c[0] += sx;
+  c[1] += sy;
+  c[2] += sz;
+  c[3] += bb * da;
 }
 
-// The rotation over the n staged slots of a chunk (see AdjWarp); kP2C picks
-// the pair kind.  Every lane runs the same number of steps.
+// The rotation over the n staged slots of a chunk (see AdjWarp), with the
+// lane's one or two targets; kP2C picks the pair kind.  Every lane runs the
+// same number of steps.
 template <bool kP2C>
-__device__ __forceinline__ void adj_rotate(AdjWarp& w, int n, const AdjTarget& x, double& gx, double& gy,
-                                           double& gz, unsigned* status) {
+__device__ __forceinline__ void adj_rotate(AdjWarp& w, int n, const AdjTarget& x, double g[6], unsigned* status) {
   const int mg = (x.grp < x.G && x.grp < n) ? (n - x.grp + x.G - 1) / x.G : 0;  // this group's slots
   const int mmax = (n + x.G - 1) / x.G;
-  const int L = max(x.nt, mmax);
+  const int L = max(x.h, mmax);
   for (int st = 0; st < L; st++) {
-    const int local = (st + x.t) % L;
+    const int local = (st + x.tl) % L;
     if (x.act && local < mg) {
       const int k = x.grp + x.G * local;
-      if (kP2C) adj_p2c_pair(w, k, x, gx, gy, gz, status);
-      else adj_p2p_pair(w, k, x, gx, gy, gz);
+      if (kP2C) {
+        double c[10] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        double jx, jy, jz;
+        if (adj_p2c_terms(w, k, x.a, jx, jy, jz, c, status)) {
+          g[0] += jx;
+          g[1] += jy;
+          g[2] += jz;
+        }
+        if (x.two && adj_p2c_terms(w, k, x.b, jx, jy, jz, c, status)) {
+          g[3] += jx;
+          g[4] += jy;
+          g[5] += jz;
+        }
+#pragma unroll
+        for (int q = 0; q < 10; q++) w.acc[q][k] += c[q];
+      } else {
+        double c[4] = {0.0, 0.0, 0.0, 0.0};
+        adj_p2p_terms(w, k, x.a, g[0], g[1], g[2], c);
+        if (x.two) adj_p2p_terms(w, k, x.b, g[3], g[4], g[5], c);
+#pragma unroll
+        for (int q = 0; q < 4; q++) w.acc[q][k] += c[q];
+      }
     }
     __syncwarp();
   }
 }
 
-__global__ void __launch_bounds__(kAdjWarps * 32) adjoint_lists(AdjParams A) {
+__device__ __forceinline__ AdjTgt adj_load_target(const AdjParams& A, int i) {
+  AdjTgt t;
+  t.x = A.p.x[i]; t.y = A.p.y[i]; t.z = A.p.z[i]; t.s = A.p.soft[i];
+  t.ax = A.cax[i]; t.ay = A.cay[i]; t.az = A.caz[i];
+  return t;
+}
+
+#ifndef PT_ADJ_MINB
+#define PT_ADJ_MINB 1
+#endif
+__global__ void __launch_bounds__(kAdjWarps * 32, PT_ADJ_MINB) adjoint_lists(AdjParams A) {
   __shared__ AdjWarp warps[kAdjWarps];
   AdjWarp& w = warps[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
+  ADJ_T0
   while (true) {
     unsigned bi = 0;
     if (lane == 0) bi = atomicAdd(A.work, 1u);
@@ -211,17 +262,19 @@ __global__ void __launch_bounds__(kAdjWarps * 32) adjoint_lists(AdjParams A) {
       const int t0 = tbase + tc, nt = min(32, ntot - tc);
       AdjTarget x;
       x.nt = nt;
-      x.t = lane % nt;
-      x.grp = lane / nt;
-      x.G = 32 / nt;
+      x.h = PT_ADJ_TWO ? (nt + 1) >> 1 : nt;
+      x.G = 32 / x.h;
+      x.grp = lane / x.h;
+      x.tl = lane % x.h;
       x.act = x.grp < x.G;
-      x.x = x.y = x.z = x.s = x.ax = x.ay = x.az = 0.0;
-      if (x.act) {
-        const int i = t0 + x.t;
-        x.x = A.p.x[i]; x.y = A.p.y[i]; x.z = A.p.z[i]; x.s = A.p.soft[i];
-        x.ax = A.cax[i]; x.ay = A.cay[i]; x.az = A.caz[i];
-      }
-      double gx = 0.0, gy = 0.0, gz = 0.0;
+      x.t1 = PT_ADJ_TWO ? 2 * x.tl : x.tl;
+      x.t2 = PT_ADJ_TWO ? min(x.t1 + 1, nt) : nt;
+      x.two = x.act && x.t2 < nt;
+      x.a = x.b = AdjTgt{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      if (x.act) x.a = adj_load_target(A, t0 + x.t1);
+      if (x.two) x.b = adj_load_target(A, t0 + x.t2);
+      double g[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // target-side sums of the lane's targets
+      ADJ_MARK(0);
       // P2C: the list's nodes, 32 at a time
       for (int64_t win = e0; win < e1; win += 32) {
         const int64_t e = win + lane;
@@ -256,7 +309,7 @@ __global__ void __launch_bounds__(kAdjWarps * 32) adjoint_lists(AdjParams A) {
 #pragma unroll
         for (int q = 0; q < 10; q++) w.acc[q][lane] = 0.0;
         __syncwarp();
-        adj_rotate<true>(w, n, x, gx, gy, gz, A.status);
+        adj_rotate<true>(w, n, x, g, A.status);
         if (lane < n) {
           double* na = A.nadj + 10 * (int64_t)w.sidx[lane];
 #pragma unroll
@@ -264,6 +317,7 @@ __global__ void __launch_bounds__(kAdjWarps * 32) adjoint_lists(AdjParams A) {
         }
         __syncwarp();
       }
+      ADJ_MARK(1);
       // P2P: the listed leaves' particles, 32 at a time
       for (int64_t win = e0; win < e1; win += 32) {
         const int64_t e = win + lane;
@@ -309,7 +363,7 @@ __global__ void __launch_bounds__(kAdjWarps * 32) adjoint_lists(AdjParams A) {
 #pragma unroll
           for (int r = 0; r < 4; r++) w.acc[r][lane] = 0.0;
           __syncwarp();
-          adj_rotate<false>(w, n, x, gx, gy, gz, A.status);
+          adj_rotate<false>(w, n, x, g, A.status);
           if (lane < n) {
             const int j = w.sidx[lane];
             atomicAdd(&A.gx[j], w.acc[0][lane]);
@@ -320,17 +374,27 @@ __global__ void __launch_bounds__(kAdjWarps * 32) adjoint_lists(AdjParams A) {
           __syncwarp();
         }
       }
-      // the target-side sums of the G groups
-      w.acc[0][lane] = gx;
-      w.acc[1][lane] = gy;
-      w.acc[2][lane] = gz;
+      ADJ_MARK(2);
+      // the target-side sums of the G groups: slot (group, target) rows in
+      // the staging area (G n_t <= 64 slots)
+      double* red = &w.st[0][0];
+      __syncwarp();
+      if (x.act) {
+        const int s1 = 3 * (x.grp * nt + x.t1);
+        red[s1] = g[0]; red[s1 + 1] = g[1]; red[s1 + 2] = g[2];
+        if (x.two) {
+          const int s2 = 3 * (x.grp * nt + x.t2);
+          red[s2] = g[3]; red[s2 + 1] = g[4]; red[s2 + 2] = g[5];
+        }
+      }
       __syncwarp();
       if (lane < nt) {
         double sx = 0.0, sy = 0.0, sz = 0.0;
-        for (int g = 0; g < x.G; g++) {
-          sx += w.acc[0][g * nt + lane];
-          sy += w.acc[1][g * nt + lane];
-          sz += w.acc[2][g * nt + lane];
+        for (int gg = 0; gg < x.G; gg++) {
+          const int sl = 3 * (gg * nt + lane);
+          sx += red[sl];
+          sy += red[sl + 1];
+          sz += red[sl + 2];
         }
         const int i = t0 + lane;
         atomicAdd(&A.gx[i], sx);
@@ -338,9 +402,18 @@ __global__ void __launch_bounds__(kAdjWarps * 32) adjoint_lists(AdjParams A) {
         atomicAdd(&A.gz[i], sz);
       }
       __syncwarp();
+      ADJ_MARK(3);
     }
   }
 }
+
+#if PT_PROF
+extern "C" int pt_debug_prof_adj(unsigned long long* out) {
+  if (cudaMemcpyFromSymbol(out, g_prof_adj, sizeof(g_prof_adj)) != cudaSuccess) return -1;
+  unsigned long long z[8] = {};
+  return cudaMemcpyToSymbol(g_prof_adj, z, sizeof(z)) == cudaSuccess ? 0 : -1;
+}
+#endif
 
 // Node adjoints -> particles through the closed-form upward pass.
 __global__ void __launch_bounds__(kAdjWarps * 32) adjoint_upward(AdjParams A) {

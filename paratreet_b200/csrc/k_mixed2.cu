@@ -31,6 +31,7 @@
 
 namespace pt {
 
+
 // Phase timers of a diagnostic build (PT_PROF=1): lane 0 adds the clock
 // cycles since the previous mark to a per-warp slot in shared memory; the
 // slots are summed into g_prof when the warp exits.
@@ -163,6 +164,7 @@ __global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravPa
   unsigned max_len = 0;
   Region rpc{0, 0}, rpp{0, 0};
   bool pool_ok = true;
+  const int nn32 = (int)min(P.nnodes, (int64_t)INT_MAX);  // node indices are 32-bit
   PROF_START(w);
   while (true) {
     const unsigned bi = grab_bucket(P.work, P.smq, lane);
@@ -192,7 +194,7 @@ __global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravPa
     const double blo[3] = {g.lo[0], g.lo[1], g.lo[2]}, bhi[3] = {g.hi[0], g.hi[1], g.hi[2]};
     const int ntot = P.walk[tnode].pcount;
     unsigned long long pc0 = rpc.cur, pp0 = rpp.cur;  // the bucket's lists start here (moved on overflow)
-    unsigned long long opens = 0;
+    unsigned opens32 = 0;  // internal children classified (fits 32 bits per bucket)
     int sp = 0;
     int nexp = 1, pop = -1;
     bool ok = true, fits = true;
@@ -209,7 +211,7 @@ __global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravPa
       double gap2 = -1.0;
       WalkRec r;
       if (node >= 0) {
-        if (node >= P.nnodes) {
+        if (node >= nn32) {
           atomicOr(P.status, kErrCapacity);
         } else {
           if (node == 0) {
@@ -231,8 +233,7 @@ __global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravPa
           else cls = classify_node_gap_nooff(r, blo, bhi, g, gap2);
         }
       }
-      opens += (unsigned long long)__popc(__ballot_sync(kFull, node >= 0 && node < P.nnodes &&
-                                                                    r.type == kTypeInternal));
+      opens32 += __popc(__ballot_sync(kFull, node >= 0 && node < nn32 && r.type == kTypeInternal));
       bool near = false;
       if (cls == kClsQuad) {
         // a target may be inside twoh of the centre (SPLINEQ's softened
@@ -292,7 +293,7 @@ __global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravPa
     }
     max_len = max(max_len, max(npc, npp));
     c_pc += (unsigned long long)npc * (unsigned long long)ntot;
-    c_open += opens;
+    c_open += opens32;
     if (P.bucket_work && lane == 0) {  // eval_p2p adds the P2P pairs
       unsigned long long wk = (unsigned long long)npc * (unsigned long long)ntot;
       if (P.accumulate) wk += P.bucket_work[b];
@@ -506,13 +507,31 @@ __device__ __forceinline__ bool next_bucket(const TravParams& P, int lane, int64
 
 // FP32 offset of a node's centre of mass (plus the replica offset) from the
 // bucket's, computed in FP64 as the walk computes it.
+
+// 256-bit loads (sm_100): half a 64-byte walk record, or a whole 32-byte
+// FP32 node record, with one instruction (the read-only path: these kernels
+// never write the node arrays)
+__device__ __forceinline__ double4 ld_nc_d4(const void* p) {
+  double4 v;
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ void ld_nc_f8(const void* p, float4& a, float4& b) {
+  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+      : "l"(p));
+}
+
 __device__ __forceinline__ float4 node_offset(const WalkRec* __restrict__ walk, int node, const TravParams& P,
                                               const BucketGeom& g) {
-  const double2* r = reinterpret_cast<const double2*>(walk + node);
-  const double2 c01 = r[0];
-  const double c2 = r[1].x;
-  return make_float4((float)((c01.x + P.ox) - g.cm[0]), (float)((c01.y + P.oy) - g.cm[1]),
-                     (float)((c2 + P.oz) - g.cm[2]), 0.f);
+  const double4 c = ld_nc_d4(walk + node);  // cm x, y, z, orsq | reach
+  return make_float4((float)((c.x + P.ox) - g.cm[0]), (float)((c.y + P.oy) - g.cm[1]),
+                     (float)((c.z + P.oz) - g.cm[2]), 0.f);
+}
+
+// The FP32 node record (mass, soft, xx, xy), (xz, yy, yz, zz).
+__device__ __forceinline__ void load_quadf(const QuadRecF* __restrict__ q, int node, float4& r0, float4& r1) {
+  ld_nc_f8(q + node, r0, r1);
 }
 
 struct P2cTerm {
@@ -605,8 +624,8 @@ __device__ __forceinline__ void ev_p2c_specials(const EvalWarpC& w, const TravPa
     const int e = w.spec[j];
     const int node = e & 0x3fffffff;
     const float4 o = node_offset(P.walk, node, P, w.geom);
-    const float4* rec = reinterpret_cast<const float4*>(P.quadf + node);
-    const float4 r0 = rec[0], r1 = rec[1];  // (mass, soft, xx, xy), (xz, yy, yz, zz)
+    float4 r0, r1;  // (mass, soft, xx, xy), (xz, yy, yz, zz)
+    load_quadf(P.quadf, node, r0, r1);
     const bool mono = e < 0;
     const float4 q0 = mono ? make_float4(0.f, 0.f, 0.f, 0.f) : make_float4(r0.z, r0.w, r1.x, r1.y);
     const float2 q1 = mono ? make_float2(0.f, 0.f) : make_float2(r1.z, r1.w);
@@ -676,10 +695,8 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c(TravParams
             spec[h] = (e & 0xc0000000) != 0;
             if (!spec[h]) {
               const int node = e & 0x3fffffff;
-              const float4* rec = reinterpret_cast<const float4*>(P.quadf + node);
               o[h] = node_offset(P.walk, node, P, w.geom);
-              r0[h] = rec[0];  // mass, soft, xx, xy
-              r1[h] = rec[1];  // xz, yy, yz, zz
+              load_quadf(P.quadf, node, r0[h], r1[h]);  // (mass, soft, xx, xy), (xz, yy, yz, zz)
             }
           }
         }
@@ -843,10 +860,8 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c2(TravParam
             spec[h] = (e & 0xc0000000) != 0;
             if (!spec[h]) {
               const int node = e & 0x3fffffff;
-              const float4* rec = reinterpret_cast<const float4*>(P.quadf + node);
               o[h] = node_offset(P.walk, node, P, w.geom);
-              r0[h] = rec[0];  // mass, soft, xx, xy
-              r1[h] = rec[1];  // xz, yy, yz, zz
+              load_quadf(P.quadf, node, r0[h], r1[h]);  // (mass, soft, xx, xy), (xz, yy, yz, zz)
             }
           }
         }
@@ -876,8 +891,8 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2c2(TravParam
             const int e = w.spec[j];
             const int node = e & 0x3fffffff;
             const float4 of = node_offset(P.walk, node, P, w.geom);
-            const float4* rec = reinterpret_cast<const float4*>(P.quadf + node);
-            const float4 q0r = rec[0], q1r = rec[1];
+            float4 q0r, q1r;
+            load_quadf(P.quadf, node, q0r, q1r);
             const bool mono = e < 0;
             const float4 q0 = mono ? make_float4(0.f, 0.f, 0.f, 0.f) : make_float4(q0r.z, q0r.w, q1r.x, q1r.y);
             const float2 q1 = mono ? make_float2(0.f, 0.f) : make_float2(q1r.z, q1r.w);
@@ -988,6 +1003,14 @@ __device__ __forceinline__ void ev_near_source(float m, float dx, float dy, floa
   }
 }
 
+// First particle and particle count of a leaf (WalkRec pstart, pcount).
+__device__ __forceinline__ void leaf_range(const WalkRec* __restrict__ walk, int nd, int& pstart, int& pcount) {
+  float4 a, b;  // the record's second half: soft_max, first_child, type, count, pstart, pcount, pad
+  ld_nc_f8(reinterpret_cast<const char*>(walk + nd) + 32, a, b);
+  pstart = __float_as_int(b.y);
+  pcount = __float_as_int(b.z);
+}
+
 // Leaf of chunk positions 2 lane and 2 lane + 1 (chunk start cs): the leaf
 // covering position cs plus the leaves that start in (cs, q] -- one bit per
 // start position, OR-reduced over the warp, counted with popc.  preA / preB =
@@ -1016,14 +1039,12 @@ __device__ __forceinline__ void ev_p2p_leaves(EvalWarp& w, int nleaves, const Tr
   int s0a = 0, s0b = 0, na = 0, nb = 0;
   if (lane < nleaves) {
     const int nd = w.lsel[lane];
-    s0a = P.walk[nd].pstart;
-    na = P.walk[nd].pcount;
+    leaf_range(P.walk, nd, s0a, na);
     w.lof[lane] = node_offset(P.walk, nd, P, w.geom);
   }
   if (lane + 32 < nleaves) {
     const int nd = w.lsel[lane + 32];
-    s0b = P.walk[nd].pstart;
-    nb = P.walk[nd].pcount;
+    leaf_range(P.walk, nd, s0b, nb);
     w.lof[lane + 32] = node_offset(P.walk, nd, P, w.geom);
   }
   int inca = na, incb = nb;
@@ -1196,8 +1217,15 @@ __device__ __noinline__ unsigned long long mark_near_leaves(const WalkRec* __res
     unsigned cnt = 0;
     if (k < count) {  // the walk wrote the entries with bit 31 clear: only near leaves are stored
       const int e = list[k];
-      cnt = (unsigned)walk[e].pcount;
-      if (p2p_leaf_near(walk, e, g->lo, g->hi, g->soft_max, ox, oy, oz)) list[k] = e | (int)0x80000000;
+      // p2p_leaf_near on the whole record, read with two 256-bit loads
+      const double4 c = ld_nc_d4(walk + e);  // cm x, y, z, reach
+      float4 a, b;                           // soft_max, first_child, type, count, pstart, pcount, pad
+      ld_nc_f8(reinterpret_cast<const char*>(walk + e) + 32, a, b);
+      cnt = (unsigned)__float_as_int(b.z);
+      const double smax = __hiloint2double(__float_as_int(a.y), __float_as_int(a.x));
+      const double gap2 = box_gap2_exact(g->lo, g->hi, __dadd_rn(c.x, ox), __dadd_rn(c.y, oy), __dadd_rn(c.z, oz));
+      const double reach = c.w + smax + g->soft_max;
+      if (!(gap2 > reach * reach)) list[k] = e | (int)0x80000000;
     }
     nsrc += __reduce_add_sync(kFull, cnt);
   }
