@@ -74,13 +74,14 @@ __device__ __forceinline__ void spline_b_db(double r2, double ir, double twoh, d
 }
 
 // Work layout of adjoint_lists: one warp per bucket, the bucket's n_t targets
-// replicated over G = floor(32 / n_t) lane groups (as the evaluation kernels
-// do).  A chunk of up to 32 list nodes, or of 32 source particles of the
-// listed leaves, is staged in shared memory with one adjoint accumulator row
-// per staged slot; group g takes the slots g, g + G, ...  Inside a group, at
-// step s lane t handles its group's slot number (s + t) mod L (L = max(n_t,
-// the group's slots)), so no two lanes touch one slot in a step and each
-// (target, slot) pair is visited once; a __syncwarp separates the steps.  The
+// two per lane in groups of h = ceil(n_t / 2) lanes, replicated over
+// G = floor(32 / h) lane groups (as the evaluation kernels do).  A chunk of up
+// to 32 list nodes, or of 32 source particles of the listed leaves, is staged
+// in shared memory with one adjoint accumulator row per staged slot; group g
+// takes the slots g, g + G, ...  Inside a group, at step s lane t handles its
+// group's slot number (s + t) mod L (L = max(h, the group's slots)), so no two
+// lanes touch one slot in a step and each (target, slot) pair is visited once;
+// a __syncwarp separates the steps.  The
 // target-side terms stay in registers; the source-side ones are added to the
 // slot's row and flushed with one atomic add per slot and value after the
 // chunk.  Atomic adds make the last bits of the results order-dependent.
@@ -92,19 +93,15 @@ struct AdjWarp {
   int32_t lincl[32];   // P2P: inclusive prefix of their particle counts
 };
 
-#ifndef PT_ADJ_TWO
-#define PT_ADJ_TWO 0
-#endif
-
 // One target of a lane: position, softening and cotangent.
 struct AdjTgt {
   double x, y, z, s, ax, ay, az;
 };
 
-// The lane's targets: with two targets per lane (PT_ADJ_TWO), lane l of
-// group l / h holds targets 2 (l mod h) and 2 (l mod h) + 1 (h = ceil(n_t / 2),
-// t2 == n_t when there is none), so every staged slot is read, and its row
-// updated, once for two pairs; otherwise h = n_t and t2 == n_t.
+// The lane's targets: lane l of group l / h holds targets 2 (l mod h) and
+// 2 (l mod h) + 1 (h = ceil(n_t / 2), t2 == n_t when there is none), so every
+// staged slot is read, and its row updated, once for two pairs (Hernquist
+// N = 262,144, theta 0.6: 13.4 -> 11.8 ms against one target per lane).
 struct AdjTarget {
   int t1, t2, tl, h, grp, G, nt;
   bool act, two;
@@ -237,8 +234,10 @@ __device__ __forceinline__ AdjTgt adj_load_target(const AdjParams& A, int i) {
   return t;
 }
 
+// CTAs per SM of adjoint_lists: 5 (96 registers, a little spilled) measured
+// faster than the 4 that 124 registers allow
 #ifndef PT_ADJ_MINB
-#define PT_ADJ_MINB 1
+#define PT_ADJ_MINB 5
 #endif
 __global__ void __launch_bounds__(kAdjWarps * 32, PT_ADJ_MINB) adjoint_lists(AdjParams A) {
   __shared__ AdjWarp warps[kAdjWarps];
@@ -262,13 +261,13 @@ __global__ void __launch_bounds__(kAdjWarps * 32, PT_ADJ_MINB) adjoint_lists(Adj
       const int t0 = tbase + tc, nt = min(32, ntot - tc);
       AdjTarget x;
       x.nt = nt;
-      x.h = PT_ADJ_TWO ? (nt + 1) >> 1 : nt;
+      x.h = (nt + 1) >> 1;
       x.G = 32 / x.h;
       x.grp = lane / x.h;
       x.tl = lane % x.h;
       x.act = x.grp < x.G;
-      x.t1 = PT_ADJ_TWO ? 2 * x.tl : x.tl;
-      x.t2 = PT_ADJ_TWO ? min(x.t1 + 1, nt) : nt;
+      x.t1 = 2 * x.tl;
+      x.t2 = min(x.t1 + 1, nt);
       x.two = x.act && x.t2 < nt;
       x.a = x.b = AdjTgt{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
       if (x.act) x.a = adj_load_target(A, t0 + x.t1);

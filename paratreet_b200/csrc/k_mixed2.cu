@@ -318,9 +318,10 @@ constexpr int kEvWarps = 4;
 #ifndef PT_P2C_MINB
 #define PT_P2C_MINB 7
 #endif
-// CTAs per SM of eval_p2p (64 registers; 7 measured 0.5 ms slower)
+// CTAs per SM of eval_p2p (72 registers; with the 256-bit leaf-record loads
+// 7 measured 0.3 ms faster than 8 at 64 registers, which spills more)
 #ifndef PT_P2P_MINB
-#define PT_P2P_MINB 8
+#define PT_P2P_MINB 7
 #endif
 
 // Per-warp shared memory of eval_p2p ...
@@ -511,6 +512,9 @@ __device__ __forceinline__ bool next_bucket(const TravParams& P, int lane, int64
 // 256-bit loads (sm_100): half a 64-byte walk record, or a whole 32-byte
 // FP32 node record, with one instruction (the read-only path: these kernels
 // never write the node arrays)
+// (a 256-bit load needs a 32-byte aligned address: the arrays come from
+// cudaMalloc, and their records are 64 and 32 bytes long)
+static_assert(sizeof(WalkRec) == 64 && sizeof(QuadRecF) == 32, "records of 64 and 32 bytes");
 __device__ __forceinline__ double4 ld_nc_d4(const void* p) {
   double4 v;
   asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w) : "l"(p));
