@@ -194,7 +194,10 @@ __global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravPa
     const double blo[3] = {g.lo[0], g.lo[1], g.lo[2]}, bhi[3] = {g.hi[0], g.hi[1], g.hi[2]};
     const int ntot = P.walk[tnode].pcount;
     unsigned long long pc0 = rpc.cur, pp0 = rpp.cur;  // the bucket's lists start here (moved on overflow)
-    unsigned opens32 = 0;  // internal children classified (fits 32 bits per bucket)
+    // internal children classified (fits 32 bits per bucket): those accepted as
+    // P2C nodes plus those opened, counted from the two ballots the step takes
+    // anyway (one ballot fewer per step: 1.1 ms at N = 2^24)
+    unsigned opens32 = 0;
     int sp = 0;
     int nexp = 1, pop = -1;
     bool ok = true, fits = true;
@@ -233,7 +236,6 @@ __global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravPa
           else cls = classify_node_gap_nooff(r, blo, bhi, g, gap2);
         }
       }
-      opens32 += __popc(__ballot_sync(kFull, node >= 0 && node < nn32 && r.type == kTypeInternal));
       bool near = false;
       if (cls == kClsQuad) {
         // a target may be inside twoh of the centre (SPLINEQ's softened
@@ -248,6 +250,7 @@ __global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravPa
         const bool pc = (cls == kClsQuad || cls == kClsMono);
         const unsigned m = __ballot_sync(kFull, pc);
         const int n = __popc(m);
+        opens32 += n;  // internal children: accepted (P2C) here, opened below
         if (n && fits) {
           fits = make_room(n, rpc, pc0, L.pc_pool, L.cursor + 0, L.cap_pc, L.region, lane);
           if (fits && pc)
@@ -267,6 +270,7 @@ __global__ void __launch_bounds__(kWlWarps * 32, PT_WALK_MINB) walk_lists(TravPa
       {
         const bool op = (cls == kClsOpen);
         const unsigned m = __ballot_sync(kFull, op);
+        opens32 += __popc(m);
         if (sp + __popc(m) > kWlStack) {
           ok = false;
           break;
