@@ -354,9 +354,9 @@ def main():
 # proportion to the interactions, which grow with N in the same proportion at
 # fixed theta, so the per-particle figure scales to the bench size.
 TRAVERSE_MIXED_DRAM_PER_PARTICLE = {
-    "walk_lists": (67293696 + 893227520) / 2097152.0,
-    "eval_p2c2": (899478528 + 78930944) / 2097152.0,
-    "eval_p2p": (413271808 + 84599296) / 2097152.0,
+    "walk_lists": (67588352 + 893458432) / 2097152.0,
+    "eval_p2c2": (900244480 + 80266240) / 2097152.0,
+    "eval_p2p": (414259968 + 85849856) / 2097152.0,
 }
 TRAVERSE_MIXED_DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of each kernel at "
                               "N = 2^21, scaled by N (profiles/traversal_kernels_plummer_2m.md)")
