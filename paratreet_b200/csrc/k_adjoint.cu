@@ -235,7 +235,8 @@ __device__ __forceinline__ AdjTgt adj_load_target(const AdjParams& A, int i) {
 }
 
 // CTAs per SM of adjoint_lists: 5 (96 registers, a little spilled) measured
-// faster than the 4 that 124 registers allow
+// faster than the 4 that 124 registers allow (13.0 -> 11.7 ms); 6 and 7 spill
+// far more (14.4 and 15.8 ms)
 #ifndef PT_ADJ_MINB
 #define PT_ADJ_MINB 5
 #endif
