@@ -132,7 +132,7 @@ def adjoint_at(g, coords):
     return np.array([g["g" + c][i] for i, c in coords])
 
 
-def judge(fd, g, coords):
+def assess(fd, g, coords):
     """Errors of the adjoint gradient g against the finite differences: the
     plain relative error, and the slack |fd - g| - (1e-6 |g| + 3 eta), which
     must not be positive."""
@@ -172,8 +172,8 @@ def test_gradient_workload_hernquist_262k():
     with GravitySimulation(max_particles_per_leaf=16, theta=THETA, max_timestep=DT, precision="fp64_lists",
                            integrator="kdk") as f:
         fd = fd_check(lambda q: gpu_chain(f, q, K), p, y, coords, ad, h_mass=1e-10)
-    rep_d, rel_d, slack_d, ok, is_m = judge(fd, ad, coords)
-    rep_m, rel_m, _, _, _ = judge(fd, am, coords)
+    rep_d, rel_d, slack_d, ok, is_m = assess(fd, ad, coords)
+    rep_m, rel_m, _, _, _ = assess(fd, am, coords)
     print("gradient workload:", {"fp64_chain_vs_fd": rep_d, "fp32_interaction_chain_vs_fd_of_fp64_chain": rep_m,
                                  "loss": {"fp64": loss_d, "mixed": loss_m}})
     assert abs(loss_m - loss_d) / loss_d < 1e-4
@@ -234,8 +234,8 @@ def test_chain_gradient_against_oracle_fd_small_n():
         _, gm = s.chain_grad(steps, DT, y, ckpt_every=3)
     ad, am = adjoint_at(gd, coords), adjoint_at(gm, coords)
     ref = fd_check(lambda q: oracle_chain(q, steps, DT, THETA, bucket), p, y, coords, ad, h_mass=1e-6)
-    rep_d, rel_d, slack_d, ok, is_m = judge(ref, ad, coords)
-    rep_m, rel_m, _, _, _ = judge(ref, am, coords)
+    rep_d, rel_d, slack_d, ok, is_m = assess(ref, ad, coords)
+    rep_m, rel_m, _, _, _ = assess(ref, am, coords)
     print("oracle FD gradient, N=2000 K=8:", {"fp64_chain": rep_d, "fp32_interaction_chain": rep_m})
     assert rep_d["valid_positions"] >= 40 and rep_d["valid_masses"] >= 10, rep_d["lists_changed"]
     assert slack_d[ok].max() <= 0.0, rep_d
