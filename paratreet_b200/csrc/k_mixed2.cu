@@ -1011,14 +1011,6 @@ __device__ __forceinline__ void ev_near_source(float m, float dx, float dy, floa
   }
 }
 
-// First particle and particle count of a leaf (WalkRec pstart, pcount).
-__device__ __forceinline__ void leaf_range(const WalkRec* __restrict__ walk, int nd, int& pstart, int& pcount) {
-  float4 a, b;  // the record's second half: soft_max, first_child, type, count, pstart, pcount, pad
-  ld_nc_f8(reinterpret_cast<const char*>(walk + nd) + 32, a, b);
-  pstart = __float_as_int(b.y);
-  pcount = __float_as_int(b.z);
-}
-
 // Leaf of chunk positions 2 lane and 2 lane + 1 (chunk start cs): the leaf
 // covering position cs plus the leaves that start in (cs, q] -- one bit per
 // start position, OR-reduced over the warp, counted with popc.  preA / preB =
@@ -1042,18 +1034,18 @@ __device__ __forceinline__ void chunk_leaves(int cs, int preA, int preB, int lan
 // per chunk as 32 interleaved pairs px = (x_a, x_b, y_a, y_b), pz = (z_a,
 // z_b, m_a, m_b), relative to the bucket, and evaluated with packed FP32.
 template <bool kFar, bool kTwo, class Tgt>
-__device__ __forceinline__ void ev_p2p_leaves(EvalWarp& w, int nleaves, const TravParams& P, const Tgt& x,
-                                              int lane, Kahan4& K) {
+__device__ __forceinline__ void ev_p2p_leaves(EvalWarp& w, int base, int nleaves, const TravParams& P,
+                                              const Tgt& x, int lane, Kahan4& K) {
   int s0a = 0, s0b = 0, na = 0, nb = 0;
+  // the block pass left each leaf's first particle in ps0, its particle
+  // count in lsel and its offset in lof, from index base on
   if (lane < nleaves) {
-    const int nd = w.lsel[lane];
-    leaf_range(P.walk, nd, s0a, na);
-    w.lof[lane] = node_offset(P.walk, nd, P, w.geom);
+    s0a = w.ps0[base + lane];
+    na = w.lsel[base + lane];
   }
   if (lane + 32 < nleaves) {
-    const int nd = w.lsel[lane + 32];
-    leaf_range(P.walk, nd, s0b, nb);
-    w.lof[lane + 32] = node_offset(P.walk, nd, P, w.geom);
+    s0b = w.ps0[base + lane + 32];
+    nb = w.lsel[base + lane + 32];
   }
   int inca = na, incb = nb;
   for (int o = 1; o < 32; o <<= 1) {
@@ -1069,8 +1061,8 @@ __device__ __forceinline__ void ev_p2p_leaves(EvalWarp& w, int nleaves, const Tr
   // block: never reached); ps0 becomes source index - stream position
   const int preA = (lane < nleaves) ? inca - na : INT_MAX;
   const int preB = (lane + 32 < nleaves) ? tota + incb - nb : INT_MAX;
-  if (lane < nleaves) w.ps0[lane] = s0a - preA;
-  if (lane + 32 < nleaves) w.ps0[lane + 32] = s0b - preB;
+  if (lane < nleaves) w.ps0[base + lane] = s0a - preA;
+  if (lane + 32 < nleaves) w.ps0[base + lane + 32] = s0b - preB;
   // a leaf node always holds a particle: two leaves never start together
   if (__any_sync(kFull, (lane < nleaves && na == 0) || (lane + 32 < nleaves && nb == 0)) && lane == 0)
     atomicOr(P.status, kErrCapacity);
@@ -1099,14 +1091,14 @@ __device__ __forceinline__ void ev_p2p_leaves(EvalWarp& w, int nleaves, const Tr
       float4 oa = make_float4(0.f, 0.f, 0.f, 0.f), ob = oa;
       float sa = 0.f, sb = 0.f;
       if (q0 < total) {
-        oa = w.lof[lo];
-        const int j = w.ps0[lo] + q0;
+        oa = w.lof[base + lo];
+        const int j = w.ps0[base + lo] + q0;
         ra = P.srcf[j];
         if (!kFar) sa = P.softf[j];
       }
       if (q0 + 1 < total) {
-        ob = w.lof[lo1];
-        const int j = w.ps0[lo1] + q0 + 1;
+        ob = w.lof[base + lo1];
+        const int j = w.ps0[base + lo1] + q0 + 1;
         rb = P.srcf[j];
         if (!kFar) sb = P.softf[j];
       }
@@ -1210,61 +1202,66 @@ __device__ __forceinline__ void ev_p2p_leaves(EvalWarp& w, int nleaves, const Tr
   __syncwarp();
 }
 
-// Marks the leaves of a bucket's P2P list that may hold a softened pair
-// (bit 31 of the entry, p2p_leaf_near: the same exact test for every form)
-// and returns the source particles of all its leaves.  Out of line, so that
-// its FP64 temporaries do not add to the evaluation loops' registers (a
-// separate kernel between the walk and the evaluations measured 0.6 ms
-// slower at N = 2^24).
-__device__ __noinline__ unsigned long long mark_near_leaves(const WalkRec* __restrict__ walk, const BucketGeom* g,
-                                                            double ox, double oy, double oz,
-                                                            int32_t* __restrict__ list, int count, int lane) {
-  unsigned long long nsrc = 0;
-  for (int k0 = 0; k0 < count; k0 += 32) {
-    const int k = k0 + lane;
-    unsigned cnt = 0;
-    if (k < count) {  // the walk wrote the entries with bit 31 clear: only near leaves are stored
-      const int e = list[k];
-      // p2p_leaf_near on the whole record, read with two 256-bit loads
-      const double4 c = ld_nc_d4(walk + e);  // cm x, y, z, reach
-      float4 a, b;                           // soft_max, first_child, type, count, pstart, pcount, pad
-      ld_nc_f8(reinterpret_cast<const char*>(walk + e) + 32, a, b);
-      cnt = (unsigned)__float_as_int(b.z);
-      const double smax = __hiloint2double(__float_as_int(a.y), __float_as_int(a.x));
-      const double gap2 = box_gap2_exact(g->lo, g->hi, __dadd_rn(c.x, ox), __dadd_rn(c.y, oy), __dadd_rn(c.z, oz));
-      const double reach = c.w + smax + g->soft_max;
-      if (!(gap2 > reach * reach)) list[k] = e | (int)0x80000000;
-    }
-    nsrc += __reduce_add_sync(kFull, cnt);
-  }
-  __syncwarp();  // the marked entries are read back by other lanes
-  return nsrc;
-}
-
-// The bucket's P2P list in blocks of 64 entries: far leaves, then near ones.
+// The bucket's P2P list in blocks of 64 entries, each leaf record read once:
+// the near test (p2p_leaf_near's, on the whole record read with two 256-bit
+// loads), the particle range and the FP32 offset go to shared memory with the
+// far leaves first, and the far and near leaves are then evaluated from there
+// (a separate marking pass over the list read every record twice: 0.6 ms at
+// N = 2^24).  Returns the source particles of the listed leaves, as the
+// reference counts P2P work (n_src * n_tgt per leaf(), src/Traverser.h:27).
 template <bool kTwo, class Tgt>
-__device__ __forceinline__ void ev_p2p_blocks(EvalWarp& w, const TravParams& P, const ListParams& L, const Tgt& x,
-                                              int64_t start, int count, int lane, Kahan4& K) {
+__device__ __forceinline__ unsigned long long ev_p2p_blocks(EvalWarp& w, const TravParams& P,
+                                                                  const ListParams& L, const Tgt& x, int64_t start,
+                                                                  int count, int lane, Kahan4& K) {
+  unsigned long long nsrc = 0;
+  const unsigned lt = (1u << lane) - 1u;
   for (int blk = 0; blk < count; blk += 64) {
-    const bool va = blk + lane < count, vb = blk + lane + 32 < count;
-    const int ea = va ? L.pp_pool[start + blk + lane] : 0;
-    const int eb = vb ? L.pp_pool[start + blk + lane + 32] : 0;
+    bool v[2], nr[2];
+    int ps[2], pc[2];
+    float4 of[2];
 #pragma unroll
-    for (int kind = 0; kind < 2; kind++) {  // far leaves, then near leaves
-      const bool sa = va && ((ea < 0) == (kind == 1)), sb = vb && ((eb < 0) == (kind == 1));
-      const unsigned ma = __ballot_sync(kFull, sa), mb = __ballot_sync(kFull, sb);
-      const unsigned lt = (1u << lane) - 1u;
-      __syncwarp();
-      if (sa) w.lsel[__popc(ma & lt)] = ea & 0x7fffffff;
-      if (sb) w.lsel[__popc(ma) + __popc(mb & lt)] = eb & 0x7fffffff;
-      __syncwarp();
-      const int n = __popc(ma) + __popc(mb);
-      if (n) {
-        if (kind == 0) ev_p2p_leaves<true, kTwo>(w, n, P, x, lane, K);
-        else ev_p2p_leaves<false, kTwo>(w, n, P, x, lane, K);
+    for (int h = 0; h < 2; h++) {
+      const int q = blk + lane + 32 * h;
+      v[h] = q < count;
+      nr[h] = false;
+      ps[h] = pc[h] = 0;
+      of[h] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (v[h]) {
+        const int e = L.pp_pool[start + q] & 0x7fffffff;
+        const double4 c = ld_nc_d4(P.walk + e);  // cm x, y, z, reach
+        float4 a, b;                             // soft_max, first_child, type, count, pstart, pcount, pad
+        ld_nc_f8(reinterpret_cast<const char*>(P.walk + e) + 32, a, b);
+        ps[h] = __float_as_int(b.y);
+        pc[h] = __float_as_int(b.z);
+        const double smax = __hiloint2double(__float_as_int(a.y), __float_as_int(a.x));
+        const double cx = __dadd_rn(c.x, P.ox), cy = __dadd_rn(c.y, P.oy), cz = __dadd_rn(c.z, P.oz);
+        const double gap2 = box_gap2_exact(w.geom.lo, w.geom.hi, cx, cy, cz);
+        const double reach = c.w + smax + w.geom.soft_max;
+        nr[h] = !(gap2 > reach * reach);
+        of[h] = make_float4((float)((c.x + P.ox) - w.geom.cm[0]), (float)((c.y + P.oy) - w.geom.cm[1]),
+                            (float)((c.z + P.oz) - w.geom.cm[2]), 0.f);
       }
     }
+    nsrc += __reduce_add_sync(kFull, (unsigned)(pc[0] + pc[1]));
+    const unsigned f0 = __ballot_sync(kFull, v[0] && !nr[0]), f1 = __ballot_sync(kFull, v[1] && !nr[1]);
+    const unsigned n0 = __ballot_sync(kFull, v[0] && nr[0]), n1 = __ballot_sync(kFull, v[1] && nr[1]);
+    const int nf = __popc(f0) + __popc(f1), nn = __popc(n0) + __popc(n1);
+    __syncwarp();  // the previous block's readers of lsel / ps0 / lof are done
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      if (v[h]) {
+        const int pos = nr[h] ? nf + (h ? __popc(n0) + __popc(n1 & lt) : __popc(n0 & lt))
+                              : (h ? __popc(f0) + __popc(f1 & lt) : __popc(f0 & lt));
+        w.ps0[pos] = ps[h];
+        w.lsel[pos] = pc[h];
+        w.lof[pos] = of[h];
+      }
+    }
+    __syncwarp();
+    if (nf) ev_p2p_leaves<true, kTwo>(w, 0, nf, P, x, lane, K);
+    if (nn) ev_p2p_leaves<false, kTwo>(w, nf, nn, P, x, lane, K);
   }
+  return nsrc;
 }
 
 template <int kMinBlocks>
@@ -1287,7 +1284,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2p(TravParams
     if (lane == 0) load_bucket_geom(mom, tnode, w.geom);
     __syncwarp();
     const int tbase = P.walk[tnode].pstart, ntot = P.walk[tnode].pcount;
-    const unsigned long long nsrc = mark_near_leaves(P.walk, &w.geom, P.ox, P.oy, P.oz, L.pp_pool + start, count, lane);
+    unsigned long long nsrc = 0;
     PROF_MARK(w, 0);
     for (int tc = 0; tc < ntot; tc += 32) {
       const int t0 = tbase + tc, nt = min(32, ntot - tc);
@@ -1296,7 +1293,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2p(TravParams
         ev_two_zero(w, lane);
         Kahan4 K;
         K.zero();
-        ev_p2p_blocks<true>(w, P, L, x, start, count, lane, K);
+        nsrc = ev_p2p_blocks<true>(w, P, L, x, start, count, lane, K);
         ev_finish2(w, K, x, P, t0, lane);
         PROF_MARK(w, 4);
         continue;
@@ -1304,7 +1301,7 @@ __global__ void __launch_bounds__(kEvWarps * 32, kMinBlocks) eval_p2p(TravParams
       const EvTarget x = ev_target(P.p, w.geom, t0, nt, lane);
       Kahan4 K;
       K.zero();
-      ev_p2p_blocks<false>(w, P, L, x, start, count, lane, K);
+      nsrc = ev_p2p_blocks<false>(w, P, L, x, start, count, lane, K);
       ev_finish(w, K, 0.f, x, P, t0, lane, false, false);
       PROF_MARK(w, 4);
     }
