@@ -350,13 +350,13 @@ def main():
 # traversal, Plummer sphere, bucket 32, theta 0.7, eps 1e-3: ncu
 # dram__bytes_read.sum + dram__bytes_write.sum of one launch of each kernel on
 # the N = 2^21 pass, divided by N (profiles/traversal_kernels_plummer_2m.md
-# holds the command and the figures).  Every kernel reads and writes in
+# holds the commands and the figures).  Every kernel reads and writes in
 # proportion to the interactions, which grow with N in the same proportion at
 # fixed theta, so the per-particle figure scales to the bench size.
 TRAVERSE_MIXED_DRAM_PER_PARTICLE = {
     "walk_lists": (67588352 + 893458432) / 2097152.0,
     "eval_p2c2": (900244480 + 80266240) / 2097152.0,
-    "eval_p2p": (414259968 + 85849856) / 2097152.0,
+    "eval_p2p": (413512448 + 60272640) / 2097152.0,
 }
 TRAVERSE_MIXED_DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of each kernel at "
                               "N = 2^21, scaled by N (profiles/traversal_kernels_plummer_2m.md)")
