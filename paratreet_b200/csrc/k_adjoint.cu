@@ -91,6 +91,7 @@ struct AdjWarp {
   int32_t sidx[32];    // the slot's node or particle index
   int32_t lnode[32];   // P2P: the window's leaves
   int32_t lincl[32];   // P2P: inclusive prefix of their particle counts
+  int32_t lpst[32];    // P2P: their first particles
 };
 
 // One target of a lane: position, softening and cotangent.
@@ -330,7 +331,11 @@ __global__ void __launch_bounds__(kAdjWarps * 32, PT_ADJ_MINB) adjoint_lists(Adj
         const unsigned m = __ballot_sync(kAdjFull, sel);
         const int nl = __popc(m);
         if (nl == 0) continue;
-        const int cnt = sel ? A.walk[node].pcount : 0;
+        int cnt = 0, pst = 0;
+        if (sel) {
+          cnt = A.walk[node].pcount;
+          pst = A.walk[node].pstart;
+        }
         int inc = cnt;
         for (int o = 1; o < 32; o <<= 1) {
           const int y = __shfl_up_sync(kAdjFull, inc, o);
@@ -342,6 +347,7 @@ __global__ void __launch_bounds__(kAdjWarps * 32, PT_ADJ_MINB) adjoint_lists(Adj
           const int k = __popc(m & ((1u << lane) - 1u));
           w.lnode[k] = node;
           w.lincl[k] = inc;
+          w.lpst[k] = pst;
         }
         __syncwarp();
         for (int cs = 0; cs < total; cs += 32) {
@@ -355,7 +361,7 @@ __global__ void __launch_bounds__(kAdjWarps * 32, PT_ADJ_MINB) adjoint_lists(Adj
               else lo = mid + 1;
             }
             const int first = (lo == 0) ? 0 : w.lincl[lo - 1];
-            const int j = A.walk[w.lnode[lo]].pstart + (q - first);
+            const int j = w.lpst[lo] + (q - first);
             w.sidx[lane] = j;
             w.st[0][lane] = A.p.x[j]; w.st[1][lane] = A.p.y[j]; w.st[2][lane] = A.p.z[j];
             w.st[3][lane] = A.p.m[j]; w.st[4][lane] = A.p.soft[j];
